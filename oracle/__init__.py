@@ -1,0 +1,140 @@
+"""CPU oracle for the MRRR path (TEST INFRASTRUCTURE ONLY).
+
+Loads two shared libraries built by ``oracle/Makefile``:
+
+* ``_build/libmr3_oracle.so`` -- the C restatement in ``mr3_oracle.c`` of the
+  reference's ``mrrr()`` (SRC/mrrr.c:87-296) and of the LAPACK kernels it calls;
+* ``_ref/libmrrr_ref.so`` -- the reference's own C sources linked against
+  scipy's bundled LAPACK (present only where the reference was built).
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline legs of
+``bench.py`` import this package, and only as the checker.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "libmr3_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libmrrr_ref.so")
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_pi = C.POINTER(C.c_int)
+_pd = C.POINTER(C.c_double)
+
+_libs: dict[str, C.CDLL] = {}
+
+
+def build(force: bool = False) -> None:
+    """Compile the oracle (and, where the reference sources exist, the reference)."""
+    if force or not os.path.exists(ORACLE_SO):
+        subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+
+
+def _mrrr_sig(fn):
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_char_p, C.c_char_p, _pi, _pd, _pd, _pd, _pd, _pi, _pi, _pi,
+                   _pi, _pd, _pd, _pi, _pi]
+    return fn
+
+
+def lib() -> C.CDLL:
+    """The oracle library (restatement)."""
+    if "oracle" not in _libs:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        L = C.CDLL(ORACLE_SO)
+        _mrrr_sig(L.or_mrrr)
+        L.or_dlaneg.restype = C.c_int
+        L.or_dlaneg.argtypes = [C.c_int, _dp, _dp, C.c_double, C.c_double, C.c_int]
+        L.or_log.restype = C.c_double
+        L.or_log.argtypes = [C.c_double]
+        L.or_count_bisect.restype = C.c_int
+        L.or_count_bisect.argtypes = [C.c_int, _dp, _dp, C.c_double, C.c_double]
+        L.or_count_ijob1.restype = C.c_int
+        L.or_count_ijob1.argtypes = [C.c_int, _dp, _dp, C.c_double, C.c_double]
+        L.or_dlarrb.restype = None
+        L.or_dlarrb.argtypes = [C.c_int, _dp, _dp, C.c_int, C.c_int, C.c_double, C.c_double,
+                                C.c_int, _dp, _dp, _dp, _dp, _ip, C.c_double, C.c_double,
+                                C.c_int, _pi]
+        L.or_dlar1v.restype = None
+        L.or_dlar1v.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, _dp, _dp, _dp, _dp,
+                                C.c_double, C.c_double, _dp, C.c_int, _pi, _pd, _pd, _pi,
+                                _ip, _pd, _pd, _pd, _dp]
+        L.or_dlarrf.restype = None
+        L.or_dlarrf.argtypes = [C.c_int, _dp, _dp, _dp, C.c_int, C.c_int, _dp, _dp, _dp,
+                                C.c_double, C.c_double, C.c_double, C.c_double, _pd, _dp,
+                                _dp, _dp, _pi]
+        L.or_dlarnv2.restype = None
+        L.or_dlarnv2.argtypes = [_ip, C.c_int, _dp]
+        L.or_dlarrr.restype = C.c_int
+        L.or_dlarrr.argtypes = [C.c_int, _dp, _dp]
+        _libs["oracle"] = L
+    return _libs["oracle"]
+
+
+def ref_lib() -> C.CDLL | None:
+    """The reference library built from the reference's own sources, if built."""
+    if "ref" not in _libs:
+        if not os.path.exists(REF_SO):
+            return None
+        os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+        L = C.CDLL(REF_SO)
+        _mrrr_sig(L.mrrr)
+        _libs["ref"] = L
+    return _libs["ref"]
+
+
+def _call(fn, jobz, rng, D, E, vl=0.0, vu=0.0, il=1, iu=1, tryrac=0, ldz=None):
+    D = np.array(D, dtype=np.float64, copy=True)
+    E = np.array(E, dtype=np.float64, copy=True)
+    n = D.shape[0]
+    if E.shape[0] < n:
+        E = np.concatenate([E, np.zeros(n - E.shape[0])])
+    ldz = n if ldz is None else ldz
+    want_z = jobz[0] in "Vv"
+    W = np.zeros(max(n, 1))
+    nz = max(n, 1)
+    if want_z and rng[0] in "Ii":
+        nz = iu - il + 1
+    Z = np.zeros((nz if want_z else 1) * (ldz if want_z else 1))
+    Zs = np.zeros(2 * max(n, 1), dtype=np.int32)
+    n_ = C.c_int(n)
+    vl_ = C.c_double(vl)
+    vu_ = C.c_double(vu)
+    il_ = C.c_int(il)
+    iu_ = C.c_int(iu)
+    tr_ = C.c_int(tryrac)
+    m_ = C.c_int(0)
+    ldz_ = C.c_int(ldz)
+    info = fn(jobz.encode(), rng.encode(), C.byref(n_), D.ctypes.data_as(_pd),
+              E.ctypes.data_as(_pd), C.byref(vl_), C.byref(vu_), C.byref(il_), C.byref(iu_),
+              C.byref(tr_), C.byref(m_), W.ctypes.data_as(_pd), Z.ctypes.data_as(_pd),
+              C.byref(ldz_), Zs.ctypes.data_as(_pi))
+    m = m_.value
+    out = dict(info=info, m=m, W=W[:m].copy(), D=D, E=E, vl=vl_.value, vu=vu_.value,
+               il=il_.value, iu=iu_.value, tryrac=tr_.value)
+    if want_z:
+        out["Z"] = Z[: ldz * m].reshape(m, ldz).T[:n].copy() if m > 0 else np.zeros((n, 0))
+        out["Zsupp"] = Zs[: 2 * m].copy()
+    return out
+
+
+def mrrr(jobz, rng, D, E, vl=0.0, vu=0.0, il=1, iu=1, tryrac=0, ldz=None):
+    """Oracle solve with the reference's argument contract; returns a dict."""
+    return _call(lib().or_mrrr, jobz, rng, D, E, vl, vu, il, iu, tryrac, ldz)
+
+
+def ref_mrrr(jobz, rng, D, E, vl=0.0, vu=0.0, il=1, iu=1, tryrac=0, ldz=None,
+             threads: int = 2):
+    """The reference's own mrrr() (needs the _ref build)."""
+    L = ref_lib()
+    if L is None:
+        raise RuntimeError("reference library not built (oracle/_ref)")
+    os.environ["PMR_NUM_THREADS"] = str(threads)
+    return _call(L.mrrr, jobz, rng, D, E, vl, vu, il, iu, tryrac, ldz)

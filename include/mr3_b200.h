@@ -1,0 +1,71 @@
+/*
+ * mr3_b200.h -- public C ABI of the B200 MRRR tridiagonal eigensolver.
+ *
+ * Drop-in replacement for the tridiagonal entry points of MR3-SMP.  All
+ * arguments keep the reference's meaning; host pointers throughout.
+ */
+#ifndef MR3_B200_H
+#define MR3_B200_H
+
+#include "mr3_cuda.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Replaces int mrrr(...) of INCLUDE/mrrr.h:62-65 (implementation
+ * SRC/mrrr.c:87-296); same argument contract (INCLUDE/mrrr.h:67-149):
+ *   jobz  "N" eigenvalues, "V" eigenpairs, "C" count only (first char, any case)
+ *   range "A" all, "V" (vl,vu], "I" il..iu (1-based)
+ *   D, E  n doubles each (E[n-1] arbitrary); overwritten with the root
+ *         representation L D L^T of each block and its shift, as the
+ *         reference does
+ *   vl, vu, il, iu  refined on output; tryrac reset to 0 if relative
+ *         accuracy cannot be guaranteed
+ *   m     number of eigenpairs; W[0..m-1] ascending
+ *   Z     column j at Z[j*ldz], rows 0..n-1 written; Zsupp[2j], Zsupp[2j+1]
+ *         its 1-based support
+ * Returns 0 on success, 1 for a bad argument, 2 on an internal failure. */
+int mrrr(char *jobz, char *range, int *n, double *D, double *E, double *vl,
+         double *vu, int *il, int *iu, int *tryrac, int *m, double *W,
+         double *Z, int *ldz, int *Zsupp);
+
+/* Replaces the Fortran binding mrrr_ of SRC/mrrr.c:630-637. */
+void mrrr_(char *jobz, char *range, int *n, double *D, double *E, double *vl,
+           double *vu, int *il, int *iu, int *tryrac, int *m, double *W,
+           double *Z, int *ldz, int *Zsupp, int *info);
+
+/* One problem of a batched call with host arrays (no counterpart in the
+ * reference, which has no batch API; each entry means what the arguments of
+ * mrrr() mean). */
+typedef struct mr3_host_prob {
+  char    jobz, range;
+  int     n, il, iu, tryrac, ldz;
+  double  vl, vu;
+  double *D, *E;       /* in/out, n each */
+  double *W;           /* out, n */
+  double *Z;           /* out, ldz*m (jobz 'V') */
+  int    *Zsupp;       /* out, 2*m  (jobz 'V') */
+  int     m, info;     /* out */
+  double  vl_out, vu_out;
+  int     il_out, iu_out, tryrac_out;
+} mr3_host_prob;
+
+/* Solves all problems in one batched device pass (arrays in host memory).
+ * Returns 0 if every problem succeeded, else the largest info. */
+int mr3_batched(int nprob, mr3_host_prob *probs);
+
+/* Same with arrays already resident in device memory on `stream`
+ * (a cudaStream_t or NULL). */
+int mr3_batched_device(int nprob, mr3_cuda_prob *probs, void *stream);
+
+/* Kernels launched by the calling thread's last solve (diagnostics). */
+long long mr3_last_launches(void);
+
+/* Text of the last CUDA error seen by the calling thread's last solve. */
+const char *mr3_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

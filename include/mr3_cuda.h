@@ -1,0 +1,89 @@
+/*
+ * mr3_cuda.h -- C ABI of the CUDA layer of the B200 MRRR solver.
+ *
+ * The host library (mrrr(), the batched and serving APIs in mr3_b200.h) calls
+ * only these functions.  No CUDA or torch types cross this boundary: streams
+ * are passed as void*, buffers as plain device pointers.
+ *
+ * This layer replaces the reference's eigenvalue stage and task runtime:
+ *   mrrr_val()  SRC/mrrr_val.c:110-639      (scaling, splitting, bisection,
+ *                                             root representation, refinement)
+ *   mrrr_vec()  SRC/mrrr_vec.c:75-143       (representation tree and the
+ *               SRC/process_cluster.c        pthread task queue; here a
+ *               SRC/process_singleton.c      device work queue drained level by
+ *               SRC/process_refinement.c     level)
+ *   and the post-processing of mrrr() in SRC/mrrr.c:257-285.
+ */
+#ifndef MR3_CUDA_H
+#define MR3_CUDA_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Job and range codes (first character of the reference's jobz/range). */
+enum { MR3_JOB_N = 0, MR3_JOB_V = 1, MR3_JOB_C = 2 };
+enum { MR3_RANGE_A = 1, MR3_RANGE_V = 2, MR3_RANGE_I = 3 };
+
+/* Status codes, the reference's return values (INCLUDE/mrrr.h:133-137). */
+enum { MR3_OK = 0, MR3_EARG = 1, MR3_EMISC = 2 };
+
+/* One tridiagonal problem whose arrays are resident on the device.
+ * Inputs mirror the arguments of mrrr() (INCLUDE/mrrr.h:62-65); D and E are
+ * overwritten with the root representation as the reference does. */
+typedef struct mr3_cuda_prob {
+  int     n;            /* order */
+  int     jobz;         /* MR3_JOB_* */
+  int     range;        /* MR3_RANGE_* */
+  int     il, iu;       /* 1-based index range (range I) */
+  int     tryrac;       /* try high relative accuracy */
+  int     ldz;          /* leading dimension of Z (>= n when jobz = V) */
+  double  vl, vu;       /* value range (vl, vu] (range V) */
+  double *D, *E;        /* device, n each (in/out) */
+  double *W;            /* device, n: first m entries ascending */
+  double *Z;            /* device, ldz*m (jobz = V), column-major */
+  int    *Zsupp;        /* device, 2*m (jobz = V), 1-based supports */
+  /* outputs */
+  int     m, info, il_out, iu_out, tryrac_out;
+  double  vl_out, vu_out;
+} mr3_cuda_prob;
+
+typedef struct mr3_cuda_ctx mr3_cuda_ctx;
+
+/* Per-device solver context with a grow-only workspace.  One context serves
+ * one host thread at a time. */
+int  mr3_cuda_ctx_create(int device, mr3_cuda_ctx **out);
+void mr3_cuda_ctx_destroy(mr3_cuda_ctx *ctx);
+
+/* Solve nprob problems in one batched pass on `stream` (a cudaStream_t, or
+ * NULL for the context's own stream).  Returns MR3_OK when the launch
+ * sequence ran; per-problem outcomes are in probs[i].info and .m.  The call
+ * returns after the results (m, info, ...) have been copied to probs. */
+int  mr3_cuda_solve(mr3_cuda_ctx *ctx, int nprob, mr3_cuda_prob *probs, void *stream);
+
+/* Grow-only device buffer `slot` (0..MR3_CUDA_WS_SLOTS-1) of this context,
+ * at least `bytes` long and 256-byte aligned; NULL on allocation failure.
+ * Its contents do not survive a call that grows it. */
+#define MR3_CUDA_WS_SLOTS 8
+void *mr3_cuda_ws(mr3_cuda_ctx *ctx, int slot, size_t bytes);
+
+/* Copies on the context's stream; dir 0 = host to device, 1 = device to host.
+ * mr3_cuda_copy2d copies `height` rows of `width` bytes between pitched
+ * buffers (used for column-major Z with different leading dimensions). */
+int  mr3_cuda_copy(mr3_cuda_ctx *ctx, void *dst, const void *src, size_t bytes, int dir);
+int  mr3_cuda_copy2d(mr3_cuda_ctx *ctx, void *dst, size_t dpitch, const void *src,
+                     size_t spitch, size_t width, size_t height, int dir);
+int  mr3_cuda_sync(mr3_cuda_ctx *ctx);
+
+/* Number of kernels launched by the last mr3_cuda_solve on this context. */
+long long mr3_cuda_last_launches(const mr3_cuda_ctx *ctx);
+
+/* Last CUDA error text of this context (empty if none). */
+const char *mr3_cuda_last_error(const mr3_cuda_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

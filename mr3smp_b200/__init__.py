@@ -1,0 +1,194 @@
+"""B200-native MRRR tridiagonal eigensolver (drop-in for MR3-SMP's ``mrrr``).
+
+Python mirror of the reference's entry point ``mrrr(jobz, range, n, D, E, vl,
+vu, il, iu, tryrac, m, W, Z, ldz, Zsupp)`` (INCLUDE/mrrr.h:62-65), backed by
+the in-tree shared library ``lib/libmr3b200.so`` (C host library + sm_100a
+kernels).  There is no CPU fallback: if the library cannot be loaded, every
+call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build as _build
+
+__all__ = ["mrrr", "mrrr_batched", "mrrr_batched_device", "lib", "last_launches", "MR3Error"]
+
+LIB_PATH = _build.LIB
+_pd = C.POINTER(C.c_double)
+_pi = C.POINTER(C.c_int)
+
+
+class MR3Error(RuntimeError):
+    """Raised when the native library is missing or a call fails."""
+
+
+class HostProb(C.Structure):
+    """Mirror of ``mr3_host_prob`` in include/mr3_b200.h."""
+    _fields_ = [("jobz", C.c_char), ("range", C.c_char), ("n", C.c_int), ("il", C.c_int),
+                ("iu", C.c_int), ("tryrac", C.c_int), ("ldz", C.c_int), ("vl", C.c_double),
+                ("vu", C.c_double), ("D", _pd), ("E", _pd), ("W", _pd), ("Z", _pd),
+                ("Zsupp", _pi), ("m", C.c_int), ("info", C.c_int), ("vl_out", C.c_double),
+                ("vu_out", C.c_double), ("il_out", C.c_int), ("iu_out", C.c_int),
+                ("tryrac_out", C.c_int)]
+
+
+class CudaProb(C.Structure):
+    """Mirror of ``mr3_cuda_prob`` in include/mr3_cuda.h (device pointers)."""
+    _fields_ = [("n", C.c_int), ("jobz", C.c_int), ("range", C.c_int), ("il", C.c_int),
+                ("iu", C.c_int), ("tryrac", C.c_int), ("ldz", C.c_int), ("vl", C.c_double),
+                ("vu", C.c_double), ("D", C.c_void_p), ("E", C.c_void_p), ("W", C.c_void_p),
+                ("Z", C.c_void_p), ("Zsupp", C.c_void_p), ("m", C.c_int), ("info", C.c_int),
+                ("il_out", C.c_int), ("iu_out", C.c_int), ("tryrac_out", C.c_int),
+                ("vl_out", C.c_double), ("vu_out", C.c_double)]
+
+
+_lib: C.CDLL | None = None
+
+
+def lib() -> C.CDLL:
+    """The loaded native library (raises MR3Error if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise MR3Error(f"native library missing: {LIB_PATH} (run python -m mr3smp_b200.build)")
+        L = C.CDLL(LIB_PATH)
+        L.mrrr.restype = C.c_int
+        L.mrrr.argtypes = [C.c_char_p, C.c_char_p, _pi, _pd, _pd, _pd, _pd, _pi, _pi, _pi, _pi,
+                           _pd, _pd, _pi, _pi]
+        L.mr3_batched.restype = C.c_int
+        L.mr3_batched.argtypes = [C.c_int, C.POINTER(HostProb)]
+        L.mr3_batched_device.restype = C.c_int
+        L.mr3_batched_device.argtypes = [C.c_int, C.POINTER(CudaProb), C.c_void_p]
+        L.mr3_last_launches.restype = C.c_longlong
+        L.mr3_last_error.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def last_launches() -> int:
+    """Kernels launched by this thread's last solve."""
+    return int(lib().mr3_last_launches())
+
+
+def last_error() -> str:
+    return lib().mr3_last_error().decode()
+
+
+def _ncols(jobz: str, rng: str, n: int, il: int, iu: int) -> int:
+    if jobz[0] not in "Vv":
+        return 1
+    if rng[0] in "Ii":
+        return max(iu - il + 1, 1)
+    return max(n, 1)
+
+
+def mrrr(jobz: str, rng: str, D, E, vl: float = 0.0, vu: float = 0.0, il: int = 1,
+         iu: int = 1, tryrac: int = 0, ldz: int | None = None) -> dict:
+    """Solve one tridiagonal problem through the C ABI ``mrrr()``.
+
+    Arguments mean what they mean for the reference.  Returns a dict with
+    ``info`` (return code), ``m``, ``W`` (m,), ``Z`` (n, m), ``Zsupp`` (2m,),
+    the overwritten ``D``/``E`` and the refined ``vl, vu, il, iu, tryrac``.
+    """
+    L = lib()
+    D = np.array(D, dtype=np.float64, copy=True)
+    E = np.array(E, dtype=np.float64, copy=True)
+    n = int(D.shape[0])
+    if E.shape[0] < n:
+        E = np.concatenate([E, np.zeros(n - E.shape[0])])
+    ldz = n if ldz is None else int(ldz)
+    want_z = jobz[0] in "Vv"
+    W = np.zeros(max(n, 1))
+    Z = np.zeros(_ncols(jobz, rng, n, il, iu) * (ldz if want_z else 1))
+    Zs = np.zeros(2 * max(n, 1), dtype=np.int32)
+    n_, vl_, vu_ = C.c_int(n), C.c_double(vl), C.c_double(vu)
+    il_, iu_, tr_, m_, ldz_ = C.c_int(il), C.c_int(iu), C.c_int(tryrac), C.c_int(0), C.c_int(ldz)
+    info = L.mrrr(jobz.encode(), rng.encode(), C.byref(n_), D.ctypes.data_as(_pd),
+                  E.ctypes.data_as(_pd), C.byref(vl_), C.byref(vu_), C.byref(il_), C.byref(iu_),
+                  C.byref(tr_), C.byref(m_), W.ctypes.data_as(_pd), Z.ctypes.data_as(_pd),
+                  C.byref(ldz_), Zs.ctypes.data_as(_pi))
+    m = m_.value if info == 0 else 0
+    out = dict(info=info, m=m, W=W[:m].copy(), D=D, E=E, vl=vl_.value, vu=vu_.value,
+               il=il_.value, iu=iu_.value, tryrac=tr_.value)
+    if want_z:
+        out["Z"] = Z[: ldz * m].reshape(m, ldz).T[:n].copy() if m > 0 else np.zeros((n, 0))
+        out["Zsupp"] = Zs[: 2 * m].copy()
+    return out
+
+
+def mrrr_batched(problems: list[dict]) -> list[dict]:
+    """Solve a list of problems in one batched device pass (host arrays).
+
+    Each problem is a dict with keys ``jobz, range, D, E`` and optionally
+    ``vl, vu, il, iu, tryrac``.  Returns one result dict per problem, as
+    :func:`mrrr` does.
+    """
+    L = lib()
+    P = len(problems)
+    arr = (HostProb * P)()
+    keep = []
+    for k, pb in enumerate(problems):
+        D = np.array(pb["D"], dtype=np.float64, copy=True)
+        n = int(D.shape[0])
+        E = np.array(pb["E"], dtype=np.float64, copy=True)
+        if E.shape[0] < n:
+            E = np.concatenate([E, np.zeros(n - E.shape[0])])
+        jz, rg = pb["jobz"], pb["range"]
+        il, iu = int(pb.get("il", 1)), int(pb.get("iu", 1))
+        want_z = jz[0] in "Vv"
+        W = np.zeros(max(n, 1))
+        Z = np.zeros(_ncols(jz, rg, n, il, iu) * (n if want_z else 1))
+        Zs = np.zeros(2 * max(n, 1), dtype=np.int32)
+        keep.append((D, E, W, Z, Zs, n, jz))
+        h = arr[k]
+        h.jobz, h.range, h.n, h.il, h.iu = jz[0].encode(), rg[0].encode(), n, il, iu
+        h.tryrac, h.ldz = int(pb.get("tryrac", 0)), n
+        h.vl, h.vu = float(pb.get("vl", 0.0)), float(pb.get("vu", 0.0))
+        h.D, h.E, h.W = D.ctypes.data_as(_pd), E.ctypes.data_as(_pd), W.ctypes.data_as(_pd)
+        h.Z, h.Zsupp = Z.ctypes.data_as(_pd), Zs.ctypes.data_as(_pi)
+    L.mr3_batched(P, arr)
+    res = []
+    for k in range(P):
+        h = arr[k]
+        D, E, W, Z, Zs, n, jz = keep[k]
+        m = h.m if h.info == 0 else 0
+        out = dict(info=h.info, m=m, W=W[:m].copy(), D=D, E=E, vl=h.vl_out, vu=h.vu_out,
+                   il=h.il_out, iu=h.iu_out, tryrac=h.tryrac_out)
+        if jz[0] in "Vv":
+            out["Z"] = Z[: n * m].reshape(m, n).T.copy() if m > 0 else np.zeros((n, 0))
+            out["Zsupp"] = Zs[: 2 * m].copy()
+        res.append(out)
+    return res
+
+
+_JOB = {"N": 0, "V": 1, "C": 2}
+_RANGE = {"A": 1, "V": 2, "I": 3}
+
+
+def mrrr_batched_device(problems: list[dict], stream: int | None = None) -> tuple[int, list]:
+    """Batched solve on device-resident torch tensors (float64 / int32).
+
+    Each problem dict holds ``jobz, range`` and CUDA tensors ``D, E, W`` (n),
+    ``Z`` (m_max*n, column-major, ldz = n) and ``Zsupp`` (2*m_max) for jobz V.
+    Returns (rc, list of CudaProb results).
+    """
+    L = lib()
+    P = len(problems)
+    arr = (CudaProb * P)()
+    for k, pb in enumerate(problems):
+        q = arr[k]
+        q.n = int(pb["D"].numel())
+        q.jobz = _JOB[pb["jobz"][0].upper()]
+        q.range = _RANGE[pb["range"][0].upper()]
+        q.il, q.iu, q.tryrac = int(pb.get("il", 1)), int(pb.get("iu", 1)), int(pb.get("tryrac", 0))
+        q.vl, q.vu = float(pb.get("vl", 0.0)), float(pb.get("vu", 0.0))
+        q.ldz = q.n
+        q.D, q.E, q.W = pb["D"].data_ptr(), pb["E"].data_ptr(), pb["W"].data_ptr()
+        q.Z = pb["Z"].data_ptr() if pb.get("Z") is not None else None
+        q.Zsupp = pb["Zsupp"].data_ptr() if pb.get("Zsupp") is not None else None
+    rc = L.mr3_batched_device(P, arr, C.c_void_p(stream) if stream else None)
+    return rc, [arr[k] for k in range(P)]

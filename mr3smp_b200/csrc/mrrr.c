@@ -1,0 +1,249 @@
+/*
+ * mrrr.c -- C host library: the reference-compatible entry points.
+ *
+ * mrrr()/mrrr_() keep the argument contract of INCLUDE/mrrr.h:62-149 and the
+ * argument checks of SRC/mrrr.c:119-138.  The solve itself runs on the GPU
+ * through the C ABI of mr3_cuda.h; there is no CPU path.  Calls are reentrant:
+ * each calling thread borrows a solver context from a small pool.
+ */
+#include <pthread.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "mr3_b200.h"
+
+#define POOL_MAX 64
+
+typedef struct {
+  mr3_cuda_ctx *ctx;
+  int busy;
+} pool_slot;
+
+static pool_slot g_pool[POOL_MAX];
+static pthread_mutex_t g_pool_mu = PTHREAD_MUTEX_INITIALIZER;
+static __thread long long t_launches;
+static __thread char t_err[256];
+
+static int device_id(void)
+{
+  const char *s = getenv("MR3_DEVICE");
+  return s ? atoi(s) : 0;
+}
+
+static int pool_acquire(void)
+{
+  int i, slot = -1;
+  pthread_mutex_lock(&g_pool_mu);
+  for (i = 0; i < POOL_MAX; i++) {
+    if (g_pool[i].ctx && !g_pool[i].busy) { slot = i; break; }
+  }
+  if (slot < 0) {
+    for (i = 0; i < POOL_MAX; i++) {
+      if (!g_pool[i].ctx) {
+        if (mr3_cuda_ctx_create(device_id(), &g_pool[i].ctx) == MR3_OK) slot = i;
+        break;
+      }
+    }
+  }
+  if (slot >= 0) g_pool[slot].busy = 1;
+  pthread_mutex_unlock(&g_pool_mu);
+  return slot;
+}
+
+static void pool_release(int slot)
+{
+  const char *e = mr3_cuda_last_error(g_pool[slot].ctx);
+  t_launches = mr3_cuda_last_launches(g_pool[slot].ctx);
+  strncpy(t_err, e ? e : "", sizeof(t_err) - 1);
+  t_err[sizeof(t_err) - 1] = 0;
+  pthread_mutex_lock(&g_pool_mu);
+  g_pool[slot].busy = 0;
+  pthread_mutex_unlock(&g_pool_mu);
+}
+
+long long mr3_last_launches(void) { return t_launches; }
+const char *mr3_last_error(void) { return t_err; }
+
+static int job_code(char c)
+{
+  if (c == 'N' || c == 'n') return MR3_JOB_N;
+  if (c == 'V' || c == 'v') return MR3_JOB_V;
+  if (c == 'C' || c == 'c') return MR3_JOB_C;
+  return -1;
+}
+
+static int range_code(char c)
+{
+  if (c == 'A' || c == 'a') return MR3_RANGE_A;
+  if (c == 'V' || c == 'v') return MR3_RANGE_V;
+  if (c == 'I' || c == 'i') return MR3_RANGE_I;
+  return -1;
+}
+
+/* Number of eigenvector columns to reserve on the device for one problem. */
+static int ncols_of(const mr3_host_prob *h, int jz, int rg)
+{
+  if (jz != MR3_JOB_V) return 0;
+  if (rg == MR3_RANGE_I) return h->iu - h->il + 1;
+  return h->n;
+}
+
+static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+int mr3_batched(int nprob, mr3_host_prob *hp)
+{
+  int i, slot, rc = MR3_OK, worst = 0;
+  mr3_cuda_ctx *ctx;
+  mr3_cuda_prob *dp;
+  size_t nrow = 0, nz = 0, nzs = 0;
+  char *base;
+  double *dD, *dE, *dW, *dZ;
+  int *dZs;
+  if (nprob <= 0) return 0;
+  dp = (mr3_cuda_prob *)calloc((size_t)nprob, sizeof(mr3_cuda_prob));
+  if (!dp) return MR3_EMISC;
+  for (i = 0; i < nprob; i++) {
+    mr3_host_prob *h = &hp[i];
+    int jz = job_code(h->jobz), rg = range_code(h->range);
+    int ok = jz >= 0 && rg >= 0 && h->n > 0;
+    if (ok && rg == MR3_RANGE_V) ok = h->vu > h->vl;
+    if (ok && rg == MR3_RANGE_I) ok = h->il >= 1 && h->il <= h->n && h->iu >= h->il && h->iu <= h->n;
+    if (ok && jz == MR3_JOB_V) ok = h->ldz >= h->n;
+    dp[i].jobz = ok ? jz : -1;
+    dp[i].range = ok ? rg : -1;
+    if (!ok) continue;
+    nrow += align_up((size_t)h->n, 32);
+    nz += (size_t)h->n * (size_t)ncols_of(h, jz, rg);
+    nzs += align_up(2 * (size_t)h->n, 64);
+  }
+  slot = pool_acquire();
+  if (slot < 0) { free(dp); return MR3_EMISC; }
+  ctx = g_pool[slot].ctx;
+  base = (char *)mr3_cuda_ws(ctx, 0, 3 * nrow * sizeof(double) + nzs * sizeof(int) + 1024);
+  dZ = (double *)mr3_cuda_ws(ctx, 1, nz * sizeof(double) + 256);
+  if (!base || !dZ) { rc = MR3_EMISC; goto done; }
+  dD = (double *)base;
+  dE = dD + nrow;
+  dW = dE + nrow;
+  dZs = (int *)(dW + nrow);
+  {
+    size_t orow = 0, oz = 0, ozs = 0;
+    for (i = 0; i < nprob; i++) {
+      mr3_host_prob *h = &hp[i];
+      mr3_cuda_prob *q = &dp[i];
+      q->n = h->n;
+      q->il = h->il; q->iu = h->iu; q->tryrac = h->tryrac;
+      q->vl = h->vl; q->vu = h->vu;
+      if (q->jobz < 0) continue;
+      q->D = dD + orow; q->E = dE + orow; q->W = dW + orow;
+      q->ldz = h->n;
+      q->Z = (q->jobz == MR3_JOB_V) ? dZ + oz : NULL;
+      q->Zsupp = (q->jobz == MR3_JOB_V) ? dZs + ozs : NULL;
+      orow += align_up((size_t)h->n, 32);
+      oz += (size_t)h->n * (size_t)ncols_of(h, q->jobz, q->range);
+      ozs += align_up(2 * (size_t)h->n, 64);
+      if (mr3_cuda_copy(ctx, q->D, h->D, (size_t)h->n * sizeof(double), 0) != MR3_OK ||
+          mr3_cuda_copy(ctx, q->E, h->E, (size_t)h->n * sizeof(double), 0) != MR3_OK) {
+        rc = MR3_EMISC;
+        goto done;
+      }
+    }
+  }
+  if (mr3_cuda_solve(ctx, nprob, dp, NULL) != MR3_OK) { rc = MR3_EMISC; goto done; }
+  for (i = 0; i < nprob; i++) {
+    mr3_host_prob *h = &hp[i];
+    mr3_cuda_prob *q = &dp[i];
+    h->m = 0;
+    if (q->jobz < 0) { h->info = MR3_EARG; continue; }
+    h->info = q->info;
+    h->m = q->m;
+    h->vl_out = q->vl_out; h->vu_out = q->vu_out;
+    h->il_out = q->il_out; h->iu_out = q->iu_out;
+    h->tryrac_out = q->tryrac_out;
+    if (q->info != MR3_OK || q->jobz == MR3_JOB_C) continue;
+    if (h->n == 1) {   /* 1x1: nothing was overwritten on the device */
+      if (q->m > 0) {
+        mr3_cuda_copy(ctx, h->W, q->W, sizeof(double), 1);
+        if (q->jobz == MR3_JOB_V) {
+          mr3_cuda_copy(ctx, h->Z, q->Z, sizeof(double), 1);
+          mr3_cuda_copy(ctx, h->Zsupp, q->Zsupp, 2 * sizeof(int), 1);
+        }
+      }
+      continue;
+    }
+    mr3_cuda_copy(ctx, h->W, q->W, (size_t)q->m * sizeof(double), 1);
+    mr3_cuda_copy(ctx, h->D, q->D, (size_t)h->n * sizeof(double), 1);
+    mr3_cuda_copy(ctx, h->E, q->E, (size_t)h->n * sizeof(double), 1);
+    if (q->jobz == MR3_JOB_V && q->m > 0) {
+      mr3_cuda_copy2d(ctx, h->Z, (size_t)h->ldz * sizeof(double), q->Z,
+                      (size_t)q->ldz * sizeof(double), (size_t)h->n * sizeof(double),
+                      (size_t)q->m, 1);
+      mr3_cuda_copy(ctx, h->Zsupp, q->Zsupp, 2 * (size_t)q->m * sizeof(int), 1);
+    }
+  }
+  if (mr3_cuda_sync(ctx) != MR3_OK) rc = MR3_EMISC;
+done:
+  pool_release(slot);
+  for (i = 0; i < nprob; i++) {
+    if (rc != MR3_OK && hp[i].info == MR3_OK) hp[i].info = MR3_EMISC;
+    if (hp[i].info > worst) worst = hp[i].info;
+  }
+  free(dp);
+  return worst;
+}
+
+int mr3_batched_device(int nprob, mr3_cuda_prob *probs, void *stream)
+{
+  int i, rc, worst = 0, slot = pool_acquire();
+  if (slot < 0) return MR3_EMISC;
+  rc = mr3_cuda_solve(g_pool[slot].ctx, nprob, probs, stream);
+  pool_release(slot);
+  if (rc != MR3_OK) return rc;
+  for (i = 0; i < nprob; i++)
+    if (probs[i].info > worst) worst = probs[i].info;
+  return worst;
+}
+
+int mrrr(char *jobz, char *range, int *np, double *D, double *E, double *vl,
+         double *vu, int *il, int *iu, int *tryrac, int *m, double *W,
+         double *Z, int *ldz, int *Zsupp)
+{
+  int n = *np, jz = job_code(jobz[0]), rg = range_code(range[0]);
+  mr3_host_prob h;
+  /* argument checks of SRC/mrrr.c:119-126 */
+  if (jz < 0 || rg < 0) return 1;
+  if (n <= 0) return 1;
+  if (rg == MR3_RANGE_V) {
+    if (*vu <= *vl) return 1;
+  } else if (rg == MR3_RANGE_I) {
+    if (*il < 1 || *il > n || *iu < *il || *iu > n) return 1;
+  }
+  /* counting with range A or I needs no work (SRC/mrrr.c:130-138) */
+  if (jz == MR3_JOB_C) {
+    if (rg == MR3_RANGE_A) { *m = n; return 0; }
+    if (rg == MR3_RANGE_I) { *m = *iu - *il + 1; return 0; }
+  }
+  if (jz == MR3_JOB_V && *ldz < n) return 1;
+  memset(&h, 0, sizeof(h));
+  h.jobz = jobz[0]; h.range = range[0]; h.n = n;
+  h.il = *il; h.iu = *iu; h.tryrac = *tryrac; h.ldz = (jz == MR3_JOB_V) ? *ldz : n;
+  h.vl = *vl; h.vu = *vu;
+  h.D = D; h.E = E; h.W = W; h.Z = Z; h.Zsupp = Zsupp;
+  mr3_batched(1, &h);
+  if (h.info != MR3_OK) return h.info;
+  *m = h.m;
+  if (n > 1) {
+    *vl = h.vl_out; *vu = h.vu_out;
+    *il = h.il_out; *iu = h.iu_out;
+    *tryrac = h.tryrac_out;
+  }
+  return 0;
+}
+
+void mrrr_(char *jobz, char *range, int *n, double *D, double *E, double *vl,
+           double *vu, int *il, int *iu, int *tryrac, int *m, double *W,
+           double *Z, int *ldz, int *Zsupp, int *info)
+{
+  *info = mrrr(jobz, range, n, D, E, vl, vu, il, iu, tryrac, m, W, Z, ldz, Zsupp);
+}

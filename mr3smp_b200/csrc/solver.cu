@@ -1,0 +1,1978 @@
+// solver.cu -- batched MRRR tridiagonal eigensolver for sm_100a.
+//
+// One pass solves a whole batch: every kernel runs over all problems, blocks,
+// eigenvalues or clusters of the batch at once.  The algorithm is the one of
+// MR3-SMP (SRC/mrrr.c, SRC/mrrr_val.c, SRC/mrrr_vec.c,
+// SRC/process_{cluster,singleton,refinement}.c) executed in one fixed,
+// order-independent way, so the output does not depend on how the GPU
+// schedules the work:
+//   - bisection (dlarrd) and root refinement (dlarrb) are not chunked: one
+//     thread per eigenvalue gives exactly the unchunked sequential result;
+//   - the eigenvalue stage always bisects (the reference's choice once
+//     nthreads > 12*m/n, SRC/mrrr_val.c:281-285); there is no dqds;
+//   - every singleton is its own task and cluster refinement is never split;
+//     a cluster is classified completely before its singletons run.
+// The pthread task queue becomes a device work queue drained level by level:
+// a level's clusters compute their child representations and refine their
+// eigenvalues; a classification kernel appends child clusters and singleton
+// tasks to device queues with atomics; persistent warps pull singleton tasks.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "mr3_cuda.h"
+#include "mr3_device.cuh"
+
+#define MR3_THREADS 256
+
+// ------------------------------------------------------------------------
+// Device-side records
+// ------------------------------------------------------------------------
+struct ProbDev {
+  // inputs
+  int n, off, jobz, range, il, iu, tryrac, ldz;
+  double vl, vu;
+  double *Z;
+  int *Zsupp;
+  // state and outputs
+  int status, m, nvals, nsplit, irange, nwl, nwu, il_out, iu_out, tryrac_out, trivial;
+  double scale, pivmin, spdiam, tnorm, gl, gu, wl, wu, wlu, wul, vl_out, vu_out, split;
+};
+
+struct BlockDev {
+  int prob, ibgn, iend, nbl;    // global rows
+  int ilow, iupp, mbl, wbgn;    // block-local indices, global W slot
+  int irange, nab1, nab2, itmax2, nwl, nwu, none;
+  double bgl, bgu;              // fudged block bounds of mrrr_val (gl, gu)
+  double gl3, gu3, atoli;       // dlarrd bisection start and abstol
+  double wlu, wul;              // dlarrd discard thresholds
+  double sigma, spdiam, bl_spdiam;
+};
+
+struct ClusterDev {
+  int begin, end, depth, blk;   // W slots (global), depth, block
+  double bl_spdiam, lgap;
+  long long par_off;            // -1: parent is the block's root; else offset in previous arena
+  long long own_off;            // this cluster's slot in the current arena (depth >= 1)
+  double par_sigma, sigma;
+};
+
+struct SngDev {
+  int slot, cl;
+  double lgap;
+};
+
+struct WTask {
+  int first, count;
+};
+
+// Clusters of one level and their arena need (one record per level parity).
+struct LevelCounters {
+  int n_cl, err;
+  unsigned long long arena_need;
+};
+
+// Singleton queue of the level being processed.
+struct SngCounters {
+  int n_sng, n_wt, wt_next, n_unit;
+};
+
+struct Tol {
+  double rtol1, rtol2, bsrtol, rqtol;
+};
+
+// ------------------------------------------------------------------------
+// Small helpers
+// ------------------------------------------------------------------------
+__device__ __forceinline__ double warp_min(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Inclusive scan of ints over a 256-thread CTA; returns the exclusive prefix
+// and stores the total in *total.
+__device__ int cta_exscan(int v, int *sh, int *total) {
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sh[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int t = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    sh[lane] = t;
+  }
+  __syncthreads();
+  int base = (wid > 0) ? sh[wid - 1] : 0;
+  *total = sh[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return base + x - v;
+}
+
+__device__ __forceinline__ void set_status(ProbDev *p, int s) { atomicMax(&p->status, s); }
+
+// ------------------------------------------------------------------------
+// Stage A0: per-problem prologue (SRC/mrrr.c:206-243, SRC/mrrr_val.c:167-329)
+// ------------------------------------------------------------------------
+__global__ void k_gather(ProbDev *probs, const double *const *Din, const double *const *Ein,
+                         double *D, double *E, int *prob_of_slot, int *iblk) {
+  ProbDev *p = &probs[blockIdx.x];
+  const double *di = Din[blockIdx.x], *ei = Ein[blockIdx.x];
+  for (int i = threadIdx.x; i < p->n; i += blockDim.x) {
+    D[p->off + i] = di[i];
+    E[p->off + i] = ei[i];
+    prob_of_slot[p->off + i] = blockIdx.x;
+    iblk[p->off + i] = -1;
+  }
+}
+
+__global__ void __launch_bounds__(MR3_THREADS)
+k_prologue(ProbDev *probs, BlockDev *blocks, int *blk_of_row, double *D, double *E, double *E2,
+           double2 *gers, double2 *TP, double2 *TPc, Tol tol) {
+  __shared__ double sred[32];
+  __shared__ int sint[64];
+  __shared__ int sflag;
+  ProbDev *p = &probs[blockIdx.x];
+  const int n = p->n, off = p->off, tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, wid = tid >> 5;
+  double *d = D + off, *e = E + off, *e2 = E2 + off;
+  if (p->trivial) return;   // handled on the host side (n == 1 or counting only)
+
+  // ---- scale_matrix (SRC/mrrr.c:325-365): dlanst('M') by a max-reduction
+  double tn = 0.0;
+  for (int i = tid; i < n; i += nt) {
+    tn = fmax(tn, fabs(d[i]));
+    if (i < n - 1) tn = fmax(tn, fabs(e[i]));
+  }
+  tn = warp_max(tn);
+  if (lane == 0) sred[wid] = tn;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (nt >> 5); w++) t = fmax(t, sred[w]);
+    double smlnum = MR3_SAFMIN / MR3_EPS, bignum = 1.0 / smlnum;
+    double rmin = sqrt(smlnum), rmax = fmin(sqrt(bignum), 1.0 / sqrt(sqrt(MR3_SAFMIN)));
+    double scale = 1.0;
+    if (t > 0 && t < rmin) scale = rmin / t;
+    else if (t > rmax) scale = rmax / t;
+    p->scale = scale;
+    if (scale != 1.0 && p->range == MR3_RANGE_V) { p->vl *= scale; p->vu *= scale; }
+  }
+  __syncthreads();
+  const double scale = p->scale;
+  if (scale != 1.0) {
+    for (int i = tid; i < n; i += nt) {
+      d[i] *= scale;
+      if (i < n - 1) e[i] *= scale;
+    }
+  }
+  __syncthreads();
+
+  // ---- dlarrr (SRC/LAPACK/odrrr.f): the sequential test is an AND of
+  // independent per-row conditions, so it is evaluated in parallel.
+  if (tid == 0) sflag = 0;
+  __syncthreads();
+  int tryrac = p->tryrac;
+  if (tryrac) {
+    // fail if some sqrt|d(i)| < rmin, or od(i-1) + od(i) >= 0.999 with
+    // od(i) = |e(i-1)| / (sqrt|d(i-1)| sqrt|d(i)|) and od(0) = 0
+    const double rmin = sqrt(MR3_SAFMIN / MR3_EPS);
+    int bad = 0;
+    for (int i = tid; i < n; i += nt) {
+      double t2 = sqrt(fabs(d[i]));
+      if (t2 < rmin) bad = 1;
+      if (i >= 1) {
+        double t1 = sqrt(fabs(d[i - 1]));
+        double od = fabs(e[i - 1]) / (t1 * t2);
+        double odp = (i >= 2) ? fabs(e[i - 2]) / (sqrt(fabs(d[i - 2])) * t1) : 0.0;
+        if (odp + od >= 0.999) bad = 1;
+      }
+    }
+    if (bad) atomicOr(&sflag, 1);
+    __syncthreads();
+    tryrac = (sflag == 0);
+  }
+  if (tid == 0) {
+    p->tryrac_out = tryrac;
+    p->split = tryrac ? MR3_EPS : -MR3_EPS;
+  }
+  if (tryrac) {   // Dcopy, E2copy for refine_to_highrac (SRC/mrrr.c:217-222)
+    for (int i = tid; i < n; i += nt) {
+      double e2c = (i >= 1) ? e[i - 1] * e[i - 1] : 0.0;
+      TPc[off + i] = make_double2(d[i], e2c);
+    }
+  }
+  __syncthreads();
+
+  // ---- E2, Gershgorin discs, pivmin, spdiam (SRC/mrrr_val.c:213-241)
+  for (int i = tid; i < n; i += nt) e2[i] = e[i] * e[i];
+  __syncthreads();
+  if (tid == 0) e[n - 1] = 0.0;
+  __syncthreads();
+  double gl = d[0], gu = d[0], emax = 0.0;
+  for (int i = tid; i < n; i += nt) {
+    double eabs = fabs(e[i]);
+    double eold = (i > 0) ? fabs(e[i - 1]) : 0.0;
+    double t1 = eabs + eold;
+    double lo = d[i] - t1, hi = d[i] + t1;
+    gers[off + i] = make_double2(lo, hi);
+    gl = fmin(gl, lo);
+    gu = fmax(gu, hi);
+    emax = fmax(emax, eabs);
+  }
+  gl = warp_min(gl);
+  gu = warp_max(gu);
+  emax = warp_max(emax);
+  __shared__ double sgl[8], sgu[8], sem[8];
+  if (lane == 0) { sgl[wid] = gl; sgu[wid] = gu; sem[wid] = emax; }
+  __syncthreads();
+  if (tid == 0) {
+    for (int w = 1; w < (nt >> 5); w++) {
+      sgl[0] = fmin(sgl[0], sgl[w]);
+      sgu[0] = fmax(sgu[0], sgu[w]);
+      sem[0] = fmax(sem[0], sem[w]);
+    }
+    double pivmin = MR3_SAFMIN * fmax(1.0, sem[0] * sem[0]);
+    double g0 = sgl[0], g1 = sgu[0];
+    p->pivmin = pivmin;
+    p->spdiam = g1 - g0;
+    double tnorm = fmax(fabs(g0), fabs(g1));
+    p->tnorm = tnorm;
+    g0 = g0 - 2 * tnorm * MR3_EPS * n - 4 * pivmin;
+    g1 = g1 + 2 * tnorm * MR3_EPS * n + 4 * pivmin;
+    p->gl = g0;
+    p->gu = g1;
+    int irange = p->range;
+    if (irange == MR3_RANGE_I && p->il == 1 && p->iu == n) irange = MR3_RANGE_A;
+    if (irange == MR3_RANGE_V && p->vl < g0 && p->vu >= g1) irange = MR3_RANGE_A;
+    p->irange = irange;
+  }
+  __syncthreads();
+
+  // ---- dlarra splitting (SRC/LAPACK/odrra.f:98-125) and the block list
+  const double split = p->split, spd = p->spdiam;
+  int chunk = (n + nt - 1) / nt;
+  int c0 = tid * chunk, c1 = min(n, c0 + chunk);
+  int cnt = 0;
+  for (int i = c0; i < c1; i++) {
+    if (i < n - 1) {
+      double eabs = fabs(e[i]);
+      bool sp = (split < 0.0) ? (eabs <= fabs(split) * spd)
+                              : (eabs <= split * sqrt(fabs(d[i])) * sqrt(fabs(d[i + 1])));
+      if (sp) { e[i] = 0.0; e2[i] = 0.0; cnt++; }
+    }
+  }
+  __syncthreads();
+  int total;
+  int base = cta_exscan(cnt, sint, &total);
+  // splits are recognised again by e[i] == 0.0 && e2[i] == 0.0 only where we
+  // set them; recount with the same predicate outcome stored in a flag pass.
+  int b = base;
+  for (int i = c0; i < c1; i++) {
+    blk_of_row[off + i] = off + b;
+    if (i < n - 1) {
+      double eabs = fabs(e[i]);
+      // after zeroing, a split row has e[i] == 0 exactly; rows that were
+      // already zero also satisfy the split test, so the test is repeated on
+      // the stored value, which gives the same decision.
+      bool sp = (split < 0.0) ? (eabs <= fabs(split) * spd)
+                              : (eabs <= split * sqrt(fabs(d[i])) * sqrt(fabs(d[i + 1])));
+      if (sp) {
+        blocks[off + b].iend = off + i;
+        blocks[off + b + 1].ibgn = off + i + 1;
+        b++;
+      }
+    }
+  }
+  if (tid == 0) {
+    blocks[off].ibgn = off;
+    blocks[off + total].iend = off + n - 1;
+    p->nsplit = total + 1;
+  }
+  __syncthreads();
+  for (int bb = tid; bb <= total; bb += nt) {
+    BlockDev *B = &blocks[off + bb];
+    B->prob = blockIdx.x;
+    B->nbl = B->iend - B->ibgn + 1;
+  }
+  // packed T rows for the Sturm counts: (d[j], e2[j-1])
+  for (int i = tid; i < n; i += nt) TP[off + i] = make_double2(d[i], (i > 0) ? e2[i - 1] : 0.0);
+  __syncthreads();
+
+  // ---- number of wanted eigenvalues (SRC/mrrr_val.c:252-270)
+  const int irange = p->irange;
+  const double pivmin = p->pivmin;
+  if (irange == MR3_RANGE_A) {
+    if (tid == 0) { p->il_out = 1; p->iu_out = n; }
+  } else if (irange == MR3_RANGE_V) {
+    if (tid == 0) p->il_out = dv_count_ijob1(n, TP + off, pivmin, p->vl) + 1;
+    if (tid == 32) p->iu_out = dv_count_ijob1(n, TP + off, pivmin, p->vu);
+  } else {
+    if (tid == 0) { p->il_out = p->il; p->iu_out = p->iu; }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    p->nvals = p->iu_out - p->il_out + 1;
+    p->m = p->nvals;
+    if (irange == MR3_RANGE_V) { p->wl = p->vl; p->wu = p->vu; p->vl_out = p->vl; p->vu_out = p->vu; }
+    if (irange == MR3_RANGE_A) { p->wl = p->gl; p->wu = p->gu; p->vl_out = p->gl; p->vu_out = p->gu; }
+  }
+  if (p->jobz == MR3_JOB_C) return;
+  // ---- range I: the interval holding eigenvalues il..iu (SRC/mrrr_val.c:295-319)
+  if (irange == MR3_RANGE_I && (tid == 0 || tid == 32)) {
+    int itmax = (int)((dv_log(p->tnorm + pivmin) - dv_log(pivmin)) / dv_log(2.0) + 2);
+    double atoli = 2 * (2 * MR3_SAFMIN + 2 * pivmin);
+    double a = p->gl, bq = p->gu;
+    int na = -1, nb = n + 1;
+    if (tid == 0) {
+      dv_ijob3(n, TP + off, pivmin, atoli, tol.rqtol, itmax, p->il - 1, p->gl, &a, &bq, &na, &nb);
+      p->wl = a; p->wlu = bq; p->nwl = na; p->vl_out = a;
+    } else {
+      dv_ijob3(n, TP + off, pivmin, atoli, tol.rqtol, itmax, p->iu, p->gu, &a, &bq, &na, &nb);
+      p->wul = a; p->wu = bq; p->nwu = nb; p->vu_out = bq;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+// Stage A1: per-block setup (SRC/mrrr_val.c:340-412 and the set-up part of
+// dlarrd, SRC/LAPACK/odrrd.f:283-450).  One warp per block.
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(MR3_THREADS)
+k_blocks(ProbDev *probs, BlockDev *blocks, const double *D, double *E, const double2 *gers,
+         const double2 *TP, Tol tol) {
+  ProbDev *p = &probs[blockIdx.x];
+  if (p->trivial || p->jobz == MR3_JOB_C) return;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const double pivmin = p->pivmin, tnorm = p->tnorm, wl = p->wl, wu = p->wu;
+  const int irange = p->irange;
+  for (int b = wid; b < p->nsplit; b += nw) {
+    BlockDev *B = &blocks[p->off + b];
+    const int ibgn = B->ibgn, iend = B->iend, nbl = B->nbl;
+    if (nbl == 1) {
+      if (lane == 0) {
+        double dv = D[ibgn];
+        bool take = (irange == MR3_RANGE_A) || (irange == MR3_RANGE_V && dv > wl && dv <= wu) ||
+                    (irange == MR3_RANGE_I && (dv + pivmin) > wl && (dv - pivmin) <= wu);
+        B->mbl = take ? 1 : 0;
+        B->ilow = 1; B->iupp = take ? 1 : 0;
+        B->nab1 = 0; B->nab2 = 0; B->none = 1;
+        B->sigma = 0.0;
+        E[iend] = 0.0;
+      }
+      continue;
+    }
+    double bgl = D[ibgn], bgu = D[ibgn];
+    for (int i = ibgn + lane; i <= iend; i += 32) {
+      double2 g = gers[i];
+      bgl = fmin(bgl, g.x);
+      bgu = fmax(bgu, g.y);
+    }
+    bgl = warp_min(bgl);
+    bgu = warp_max(bgu);
+    const double bglf = bgl - 2 * tnorm * MR3_EPS * nbl - 4 * pivmin;
+    const double bguf = bgu + 2 * tnorm * MR3_EPS * nbl + 4 * pivmin;
+    int ilow = 1, iupp = nbl;
+    if (irange != MR3_RANGE_A) {
+      int c = 0;
+      if (lane == 0) c = dv_count_ijob1(nbl, TP + ibgn, pivmin, fmax(wl, bglf)) + 1;
+      if (lane == 1) c = dv_count_ijob1(nbl, TP + ibgn, pivmin, fmin(wu, bguf));
+      ilow = __shfl_sync(0xffffffffu, c, 0);
+      iupp = __shfl_sync(0xffffffffu, c, 1);
+    }
+    const int mbl = iupp - ilow + 1;
+    if (lane == 0) {
+      B->bgl = bglf; B->bgu = bguf; B->spdiam = bguf - bglf;
+      B->ilow = ilow; B->iupp = iupp; B->mbl = mbl;
+      B->none = 1; B->nab1 = 0; B->nab2 = 0;
+      if (mbl < 0) set_status(p, MR3_EMISC);
+      if (mbl <= 0) E[iend] = 0.0;
+    }
+    if (mbl <= 0) continue;
+    // dlarrd("I","B") set-up on this block
+    const int brange = (ilow == 1 && iupp == nbl) ? MR3_RANGE_A : MR3_RANGE_I;
+    const double tnb = fmax(fabs(bgl), fabs(bgu));
+    const double gl2 = bgl - 2.0 * tnb * MR3_EPS * nbl - 2.0 * 2.0 * pivmin;
+    const double gu2 = bgu + 2.0 * tnb * MR3_EPS * nbl + 2.0 * 2.0 * pivmin;
+    const double atoli = 2.0 * 2.0 * MR3_SAFMIN + 2.0 * 2.0 * pivmin;
+    double wlb = gl2, wub = gu2, wlub = 0.0, wulb = 0.0;
+    int bad = 0;
+    if (brange == MR3_RANGE_I) {
+      int itmax = dv_itmax(tnb + pivmin, pivmin);
+      double a = gl2, bq = gu2;
+      int na = -1, nb = nbl + 1;
+      if (lane == 0) {
+        dv_ijob3(nbl, TP + ibgn, pivmin, atoli, tol.bsrtol, itmax, ilow - 1, gl2, &a, &bq, &na, &nb);
+      } else if (lane == 1) {
+        dv_ijob3(nbl, TP + ibgn, pivmin, atoli, tol.bsrtol, itmax, iupp, gu2, &a, &bq, &na, &nb);
+      }
+      double a0 = __shfl_sync(0xffffffffu, a, 0), b0 = __shfl_sync(0xffffffffu, bq, 0);
+      double a1 = __shfl_sync(0xffffffffu, a, 1), b1 = __shfl_sync(0xffffffffu, bq, 1);
+      int nwl = __shfl_sync(0xffffffffu, na, 0), nwu = __shfl_sync(0xffffffffu, nb, 1);
+      wlb = a0; wlub = b0; wulb = a1; wub = b1;
+      if (nwl < 0 || nwl >= nbl || nwu < 1 || nwu > nbl) bad = 1;
+    }
+    double gl3 = bgl - 2.0 * tnb * MR3_EPS * nbl - 2.0 * pivmin;
+    double gu3 = bgu + 2.0 * tnb * MR3_EPS * nbl + 2.0 * pivmin;
+    int none = 0, nwlb = 0, nwub = 0;
+    if (brange == MR3_RANGE_I) {
+      if (gu3 < wlb) { none = 1; nwlb = nbl; nwub = nbl; }
+      else {
+        gl3 = fmax(gl3, wlb);
+        gu3 = fmin(gu3, wub);
+        if (gl3 >= gu3) none = 1;
+      }
+    }
+    int nab1 = 0, nab2 = 0;
+    if (!none) {
+      int c = 0;
+      if (lane == 0) c = dv_count_ijob1(nbl, TP + ibgn, pivmin, gl3);
+      if (lane == 1) c = dv_count_ijob1(nbl, TP + ibgn, pivmin, gu3);
+      nab1 = __shfl_sync(0xffffffffu, c, 0);
+      nab2 = __shfl_sync(0xffffffffu, c, 1);
+      nwlb = nab1; nwub = nab2;
+    }
+    if (lane == 0) {
+      B->irange = brange;
+      B->gl3 = gl3; B->gu3 = gu3; B->atoli = atoli;
+      B->wlu = wlub; B->wul = wulb;
+      B->none = none; B->nab1 = nab1; B->nab2 = nab2; B->nwl = nwlb; B->nwu = nwub;
+      B->itmax2 = none ? 0 : dv_itmax(gu3 - gl3 + pivmin, pivmin);
+      if (bad) set_status(p, MR3_EMISC);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+// Stage A2: initial approximations by bisection, one thread per eigenvalue
+// (dlarrd/dlaebz IJOB=2, SRC/LAPACK/odrrd.f:450-520).  Thread k of a block
+// bisects eigenvalue nab1+1+k; a block never has more than nbl of them.
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(128)
+k_bisect(int N, const ProbDev *probs, const BlockDev *blocks, const int *blk_of_row,
+         const double2 *TP, double *Wt, double *Et, int *It, Tol tol) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= N) return;
+  const BlockDev *B = &blocks[blk_of_row[g]];
+  const ProbDev *p = &probs[B->prob];
+  if (p->trivial || p->jobz == MR3_JOB_C || p->status) return;
+  int k = g - B->ibgn;
+  if (B->nbl < 2 || B->mbl <= 0 || B->none || k >= B->nab2 - B->nab1) return;
+  int j = B->nab1 + 1 + k;
+  double a = B->gl3, b = B->gu3;
+  dv_bisect_one(B->nbl, TP + B->ibgn, p->pivmin, B->atoli, tol.bsrtol, B->itmax2, j, &a, &b,
+                B->nab1, B->nab2);
+  Wt[g] = 0.5 * (a + b);
+  Et[g] = 0.5 * fabs(a - b);
+  It[g] = j;
+}
+
+// ------------------------------------------------------------------------
+// Stage A3: per problem, place each block's approximations in W after the
+// dlarrd discard of range I (SRC/LAPACK/odrrd.f:520-640).
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(MR3_THREADS)
+k_compact(ProbDev *probs, BlockDev *blocks, const double *D, double *Wt, double *Et, int *It,
+          double *W, double *Werr, int *Windex, int *iblk, double *Wcopy) {
+  __shared__ int sint[64];
+  ProbDev *p = &probs[blockIdx.x];
+  if (p->trivial || p->jobz == MR3_JOB_C) return;
+  const int tid = threadIdx.x, nt = blockDim.x, off = p->off, ns = p->nsplit;
+  // W slot of each block: exclusive prefix of mbl over the blocks
+  int chunk = (ns + nt - 1) / nt, c0 = tid * chunk, c1 = min(ns, c0 + chunk), s = 0;
+  for (int b = c0; b < c1; b++) s += max(blocks[off + b].mbl, 0);
+  int total, base = cta_exscan(s, sint, &total);
+  for (int b = c0; b < c1; b++) {
+    blocks[off + b].wbgn = off + base;
+    base += max(blocks[off + b].mbl, 0);
+  }
+  if (tid == 0) p->m = total;
+  __syncthreads();
+  const int lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
+  for (int b = wid; b < ns; b += nw) {
+    BlockDev *B = &blocks[off + b];
+    const int mbl = B->mbl, wb = B->wbgn, ib = B->ibgn;
+    if (mbl <= 0) continue;
+    if (B->nbl == 1) {
+      if (lane == 0) {
+        W[wb] = D[ib]; Werr[wb] = 0.0; Windex[wb] = 1; iblk[wb] = off + b; Wcopy[wb] = D[ib];
+      }
+      continue;
+    }
+    int mcnt = B->nab2 - B->nab1;
+    if (B->irange == MR3_RANGE_I && lane == 0) {
+      // discard surplus values from both ends, in place on the row scratch
+      double *w = Wt + ib, *we = Et + ib;
+      int *ix = It + ib;
+      int idiscl = B->ilow - 1 - B->nwl, idiscu = B->nwu - B->iupp, im;
+      if (idiscl > 0) {
+        im = 0;
+        for (int je = 0; je < mcnt; je++) {
+          if (w[je] <= B->wlu && idiscl > 0) idiscl--;
+          else { w[im] = w[je]; we[im] = we[je]; ix[im] = ix[je]; im++; }
+        }
+        mcnt = im;
+      }
+      if (idiscu > 0) {
+        im = mcnt;
+        for (int je = mcnt - 1; je >= 0; je--) {
+          if (w[je] >= B->wul && idiscu > 0) idiscu--;
+          else { im--; w[im] = w[je]; we[im] = we[je]; ix[im] = ix[je]; }
+        }
+        int jee = 0;
+        for (int je = im; je < mcnt; je++) { w[jee] = w[je]; we[jee] = we[je]; ix[jee] = ix[je]; jee++; }
+        mcnt = mcnt - im;
+      }
+      if (idiscl > 0 || idiscu > 0) {
+        // kill-off path of dlarrd (bad arithmetic): mark by index = 0
+        if (idiscl > 0) {
+          double wkill = 0.0;
+          for (int jd = 0; jd < idiscl; jd++) {
+            int iw = -1;
+            for (int je = 0; je < mcnt; je++)
+              if (ix[je] != 0 && (iw == -1 || w[je] < wkill)) { iw = je; wkill = w[je]; }
+            if (iw >= 0) ix[iw] = 0;
+          }
+        }
+        if (idiscu > 0) {
+          double wkill = 0.0;
+          for (int jd = 0; jd < idiscu; jd++) {
+            int iw = -1;
+            for (int je = 0; je < mcnt; je++)
+              if (ix[je] != 0 && (iw == -1 || w[je] >= wkill)) { iw = je; wkill = w[je]; }
+            if (iw >= 0) ix[iw] = 0;
+          }
+        }
+        im = 0;
+        for (int je = 0; je < mcnt; je++)
+          if (ix[je] != 0) { w[im] = w[je]; we[im] = we[je]; ix[im] = ix[je]; im++; }
+        mcnt = im;
+      }
+      B->nab2 = B->nab1 + mcnt;   // remember the kept count
+    }
+    __syncwarp();
+    mcnt = B->nab2 - B->nab1;
+    if (mcnt != mbl) {
+      if (lane == 0) set_status(p, MR3_EMISC);
+      continue;
+    }
+    for (int k = lane; k < mbl; k += 32) {
+      W[wb + k] = Wt[ib + k];
+      Werr[wb + k] = Et[ib + k];
+      Windex[wb + k] = It[ib + k];
+      iblk[wb + k] = off + b;
+      Wcopy[wb + k] = Wt[ib + k];
+    }
+  }
+}
+
+// Gaps after the initial approximations (SRC/mrrr_val.c:431-435).
+__global__ void k_gaps_init(int N, const ProbDev *probs, const BlockDev *blocks, const int *iblk,
+                            const double *W, const double *Werr, double *Wgap) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= N || iblk[s] < 0) return;
+  const BlockDev *B = &blocks[iblk[s]];
+  if (B->nbl < 2) return;
+  const ProbDev *p = &probs[B->prob];
+  int wend = B->wbgn + B->mbl - 1;
+  if (s < wend) Wgap[s] = fmax(0.0, (W[s + 1] - Werr[s + 1]) - (W[s] + Werr[s]));
+  else Wgap[s] = fmax(0.0, p->wu - (W[s] + Werr[s]));
+}
+
+// ------------------------------------------------------------------------
+// Stage A4: root representation L D L^T = T - sigma I of each block
+// (compute_root_rrr, bisection branch, SRC/mrrr_val.c:717-948).
+// One warp per block; the factorisation tries are serial on lane 0.
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(MR3_THREADS)
+k_root(ProbDev *probs, BlockDev *blocks, double *D, double *E, const double2 *TP, double *Dt,
+       double *Lt, const double *W, const double *Werr, const double *Wgap, double2 *RP,
+       double2 *RQ) {
+  ProbDev *p = &probs[blockIdx.x];
+  if (p->trivial || p->jobz == MR3_JOB_C || p->status) return;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const double pivmin = p->pivmin, vlp = p->vl_out, vup = p->vu_out;
+  for (int b = wid; b < p->nsplit; b += nw) {
+    BlockDev *B = &blocks[p->off + b];
+    const int nbl = B->nbl, mbl = B->mbl, ibgn = B->ibgn, iend = B->iend;
+    if (nbl < 2 || mbl <= 0) continue;
+    const int wbgn = B->wbgn, wend = wbgn + mbl - 1;
+    const double gl = B->bgl, gu = B->bgu;
+    double isleft = fmax(gl, (W[wbgn] - Werr[wbgn]) - 100.0 * MR3_EPS * fabs(W[wbgn] - Werr[wbgn]));
+    double isright = fmin(gu, (W[wend] + Werr[wend]) + 100.0 * MR3_EPS * fabs(W[wend] - Werr[wend]));
+    double spdiam = gu - gl;
+    double tmp0 = fmin(isright, vup) - fmax(isleft, vlp);
+    double s1 = fmax(isleft, vlp) + 0.25 * tmp0;
+    double s2 = fmin(isright, vup) - 0.25 * tmp0;
+    int cnt = 0;
+    if (mbl > 1 && lane < 2) {   // dlarrc('T'): lane 0 counts at s1, lane 1 at s2
+      const double x = (lane == 0) ? s1 : s2;
+      const double2 *tp = TP + ibgn;
+      double piv = tp[0].x - x;
+      cnt = (piv <= 0.0);
+      for (int i = 0; i < nbl - 1; i++) {
+        double ee = E[ibgn + i];
+        double t = ee * ee;
+        piv = (tp[i + 1].x - x) - t / piv;
+        cnt += (piv <= 0.0);
+      }
+    }
+    int lcnt = __shfl_sync(0xffffffffu, cnt, 0), rcnt = __shfl_sync(0xffffffffu, cnt, 1);
+    int ok = 1;
+    double sigma = 0.0;
+    if (lane == 0) {
+      int sgndef;
+      if (mbl == 1) { sigma = gl; sgndef = 1; }
+      else if ((lcnt - B->ilow) >= (B->iupp - rcnt)) { sigma = fmax(isleft, vlp); sgndef = 1; }
+      else { sigma = fmin(isright, vup); sgndef = -1; }
+      double tau;
+      if (mbl > 1) {
+        double clwdth = W[wend] + Werr[wend] - W[wbgn] - Werr[wbgn];
+        double avgap = fabs(clwdth / (double)(wend - wbgn));
+        if (sgndef > 0) { tau = fmax(Wgap[wbgn], avgap); tau *= 0.5; tau = fmax(tau, Werr[wbgn]); }
+        else { tau = fmax(Wgap[wend - 1], avgap); tau *= 0.5; tau = fmax(tau, Werr[wend]); }
+      } else {
+        tau = Werr[wbgn];
+      }
+      ok = 0;
+      for (int jtry = 0; jtry < MR3_MAX_TRY_ROOT; jtry++) {
+        double dpiv = D[ibgn] - sigma;
+        Dt[ibgn] = dpiv;
+        double dmax = fabs(dpiv);
+        for (int i = 0; i < nbl - 1; i++) {
+          int j = ibgn + i;
+          double ej = E[j];
+          double inv = 1.0 / dpiv;
+          double t0 = ej * inv;
+          Lt[j] = t0;
+          dpiv = (D[j + 1] - sigma) - t0 * ej;
+          Dt[j + 1] = dpiv;
+          dmax = fmax(dmax, fabs(dpiv));
+        }
+        bool norep = dmax > MR3_MAX_GROWTH * spdiam;
+        if (!norep) { ok = 1; break; }
+        if (jtry == MR3_MAX_TRY_ROOT - 2) {
+          if (sgndef == 1) sigma = gl - 2.0 * spdiam * MR3_EPS * nbl - 2.0 * 2.0 * pivmin;
+          else sigma = gu + 2.0 * spdiam * MR3_EPS * nbl + 2.0 * 2.0 * pivmin;
+        } else if (jtry == MR3_MAX_TRY_ROOT - 1) {
+          break;
+        } else {
+          sigma -= sgndef * tau;
+          tau *= 2.0;
+        }
+      }
+      if (!ok) set_status(p, MR3_EMISC);
+      B->sigma = sigma;
+      B->spdiam = spdiam;
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    sigma = __shfl_sync(0xffffffffu, sigma, 0);
+    __syncwarp();
+    if (!ok) continue;
+    // store the root, perturb it by 8*eps relative noise from dlarnv(2) with
+    // seed (1,1,1,1) (SRC/mrrr_val.c:927-941), and pack its rows
+    const unsigned long long seed = (1ULL << 36) | (1ULL << 24) | (1ULL << 12) | 1ULL;
+    for (int i = lane; i < nbl; i += 32) {
+      double dv = Dt[ibgn + i];
+      double lv = (i < nbl - 1) ? Lt[ibgn + i] : sigma;
+      if (mbl > 1) {
+        if (i < nbl - 1) {
+          dv *= 1.0 + MR3_EPS * 8.0 * dv_lcg_uniform(seed, (unsigned long long)(i + 1));
+          lv *= 1.0 + MR3_EPS * 8.0 * dv_lcg_uniform(seed, (unsigned long long)(i + 1 + nbl));
+        } else {
+          dv *= 1.0 + MR3_EPS * 8.0 * dv_lcg_uniform(seed, (unsigned long long)(2 * nbl));
+        }
+      }
+      D[ibgn + i] = dv;
+      E[ibgn + i] = lv;
+      if (i < nbl - 1) {
+        double ld = dv * lv;
+        RP[ibgn + i] = make_double2(dv, ld * lv);
+        RQ[ibgn + i] = make_double2(lv, ld);
+      } else {
+        RP[ibgn + i] = make_double2(dv, 0.0);
+        RQ[ibgn + i] = make_double2(sigma, 0.0);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+// Stage A5: refine the approximations w.r.t. the root representation
+// (refine_eigval_approx, unchunked dlarrb, SRC/mrrr_val.c:992-1082).
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(128)
+k_refine_root(int N, const ProbDev *probs, const BlockDev *blocks, const int *iblk,
+              const double2 *RP, double *W, double *Werr, const double *Wgap, Tol tol) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= N || iblk[s] < 0) return;
+  const BlockDev *B = &blocks[iblk[s]];
+  const ProbDev *p = &probs[B->prob];
+  if (p->status || B->nbl < 2) return;
+  const bool onlyW = (p->jobz == MR3_JOB_N);   // rtol1 = rtol2 = 4 eps (SRC/mrrr.c:230-232)
+  const int II = s - B->wbgn + 1;
+  const int i = B->ilow + II - 1;
+  double w = W[s] - B->sigma;
+  double werr = Werr[s] + fabs(w) * MR3_EPS;
+  const double rgap = Wgap[s];
+  const double lgap = (II > 1) ? Wgap[s - 1] : rgap;
+  const int maxitr = dv_itmax(B->spdiam + p->pivmin, p->pivmin);
+  const double rtol1 = onlyW ? 4.0 * MR3_EPS : tol.rtol1;
+  const double rtol2 = onlyW ? 4.0 * MR3_EPS : tol.rtol2;
+  dv_dlarrb_one(B->nbl, RP + B->ibgn, i, II == 1, II > 1, rgap, lgap, rtol1, rtol2, p->pivmin,
+                maxitr, B->nbl, &w, &werr);
+  W[s] = w;
+  Werr[s] = werr;
+}
+
+// Final gaps of the root refinement (dlarrb loop 111) and the last gap of the
+// block (SRC/mrrr_val.c:1080-1082).
+__global__ void k_gaps_root(int N, const ProbDev *probs, const BlockDev *blocks, const int *iblk,
+                            const double *W, const double *Werr, double *Wgap) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= N || iblk[s] < 0) return;
+  const BlockDev *B = &blocks[iblk[s]];
+  const ProbDev *p = &probs[B->prob];
+  if (p->status || B->nbl < 2) return;
+  int wend = B->wbgn + B->mbl - 1;
+  if (s < wend) Wgap[s] = fmax(0.0, W[s + 1] - Werr[s + 1] - W[s] - Werr[s]);
+  else Wgap[s] = fmax(0.0, (p->vu_out - B->sigma) - (W[s] + Werr[s]));
+}
+
+// ------------------------------------------------------------------------
+// Range I: drop surplus eigenvalues found near wl/wu
+// (SRC/mrrr_val.c:515-626).  One thread per problem; runs only when the
+// blocks together produced more than nvals values.
+// ------------------------------------------------------------------------
+__global__ void k_discard(ProbDev *probs, int nprob, BlockDev *blocks, double *W, double *Werr,
+                          double *Wgap, int *Windex, int *iblk, double *Wcopy) {
+  int pi = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pi >= nprob) return;
+  ProbDev *p = &probs[pi];
+  if (p->trivial || p->jobz == MR3_JOB_C || p->status) return;
+  int mp = p->m;
+  if (!(mp > p->nvals && p->irange == MR3_RANGE_I)) {
+    if (mp < p->nvals) set_status(p, MR3_EMISC);
+    return;
+  }
+  const int o = p->off;
+  double *w = W + o, *we = Werr + o, *wg = Wgap + o, *wc = Wcopy + o;
+  int *wi = Windex + o, *ib = iblk + o;
+  int idiscl = p->il_out - 1 - p->nwl, idiscu = p->nwu - p->iu_out, im;
+#define MOVE(dst, src) { w[dst] = w[src]; wc[dst] = wc[src]; we[dst] = we[src]; wg[dst] = wg[src]; \
+                         wi[dst] = wi[src]; ib[dst] = ib[src]; }
+  if (idiscl > 0) {
+    im = 0;
+    for (int je = 0; je < mp; je++) {
+      if (wc[je] < p->wlu && idiscl > 0) idiscl--;
+      else { MOVE(im, je); im++; }
+    }
+    mp = im;
+  }
+  if (idiscu > 0) {
+    im = mp;
+    for (int je = mp - 1; je >= 0; je--) {
+      if (wc[je] > p->wul && idiscu > 0) idiscu--;
+      else { im--; MOVE(im, je); }
+    }
+    int jee = 0;
+    for (int je = im; je < mp; je++) { MOVE(jee, je); jee++; }
+    mp -= im;
+  }
+  if (idiscl > 0 || idiscu > 0) {
+    if (idiscl > 0) {
+      double wkill = p->wu;
+      for (int jd = 0; jd < idiscl; jd++) {
+        int iw = -1;
+        for (int je = 0; je < mp; je++)
+          if (ib[je] >= 0 && (wc[je] < wkill || iw == -1)) { iw = je; wkill = wc[je]; }
+        if (iw >= 0) ib[iw] = -2;
+      }
+    }
+    if (idiscu > 0) {
+      double wkill = p->wl;
+      for (int jd = 0; jd < idiscu; jd++) {
+        int iw = -1;
+        for (int je = 0; je < mp; je++)
+          if (ib[je] >= 0 && (wc[je] > wkill || iw == -1)) { iw = je; wkill = wc[je]; }
+        if (iw >= 0) ib[iw] = -2;
+      }
+    }
+    im = 0;
+    for (int je = 0; je < mp; je++)
+      if (ib[je] >= 0) { MOVE(im, je); im++; }
+    mp = im;
+  }
+#undef MOVE
+  for (int je = mp; je < p->m; je++) ib[je] = -1;
+  p->m = mp;
+  if (mp < p->nvals) set_status(p, MR3_EMISC);
+  // block W ranges after the removal: recomputed from iblk (SRC/mrrr_vec.c:335-338)
+  for (int b = 0; b < p->nsplit; b++) blocks[o + b].mbl = 0;
+  for (int je = 0; je < mp; je++) {
+    BlockDev *B = &blocks[ib[je]];
+    if (B->mbl == 0) B->wbgn = o + je;
+    B->mbl++;
+  }
+}
+
+// ------------------------------------------------------------------------
+// Eigenvalues only: W += sigma of the block (SRC/mrrr.c:262-269).
+// ------------------------------------------------------------------------
+__global__ void k_shift_w(int N, const ProbDev *probs, const BlockDev *blocks, const int *iblk,
+                          const double *E, double *W) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= N || iblk[s] < 0) return;
+  const BlockDev *B = &blocks[iblk[s]];
+  const ProbDev *p = &probs[B->prob];
+  if (p->status || p->jobz != MR3_JOB_N) return;
+  W[s] += E[B->iend];
+}
+
+// refine_to_highrac (SRC/mrrr.c:452-520): dlarrj on the scaled input T,
+// one thread per eigenvalue.
+__global__ void k_highrac(int N, const ProbDev *probs, const BlockDev *blocks, const int *iblk,
+                          const int *Windex, const double2 *TPc, double *W, double *Werr) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= N || iblk[s] < 0) return;
+  const BlockDev *B = &blocks[iblk[s]];
+  const ProbDev *p = &probs[B->prob];
+  if (p->status || !p->tryrac_out || p->jobz == MR3_JOB_C) return;
+  // ilow = smallest local index of the block's values; values are stored in
+  // increasing local index, so it is the index of the first one.
+  const int i = Windex[B->wbgn] + (s - B->wbgn);
+  const int maxitr = dv_itmax(p->spdiam + p->pivmin, p->pivmin);
+  double w = W[s], we = Werr[s];
+  dv_dlarrj_one(B->nbl, TPc + B->ibgn, i, 4.0 * MR3_EPS, maxitr, &w, &we);
+  W[s] = w;
+  Werr[s] = we;
+}
+
+__global__ void k_invscale(int N, const ProbDev *probs, const BlockDev *blocks, const int *iblk,
+                           double *W) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= N || iblk[s] < 0) return;
+  const ProbDev *p = &probs[blocks[iblk[s]].prob];
+  if (p->status || p->scale == 1.0) return;
+  W[s] = (1.0 / p->scale) * W[s];
+}
+
+// ------------------------------------------------------------------------
+// Sorting: per-problem bottom-up merge sort of (key, sec, idx) by the
+// lexicographic order, one element per thread and pass.
+// ------------------------------------------------------------------------
+struct SortRec {
+  double key;
+  long long sec;
+  int idx, pad;
+};
+__device__ __forceinline__ bool rec_less(const SortRec &a, const SortRec &b) {
+  if (a.key < b.key) return true;
+  if (a.key > b.key) return false;
+  if (a.sec != b.sec) return a.sec < b.sec;
+  return a.idx < b.idx;
+}
+__global__ void k_merge_pass(int N, const ProbDev *probs, const int *prob_of_slot, const SortRec *in,
+                             SortRec *out, int width, int want_job, const int *flag) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= N) return;
+  int pi = prob_of_slot[s];
+  if (pi < 0) return;
+  const ProbDev *p = &probs[pi];
+  if (p->trivial || p->status || p->jobz != want_job) return;
+  if (flag && !flag[pi]) return;
+  int m = p->m, o = p->off, k = s - o;
+  if (k >= m) return;
+  int run0 = (k / (2 * width)) * (2 * width);
+  int a0 = run0, a1 = min(run0 + width, m), b1 = min(run0 + 2 * width, m);
+  SortRec r = in[s];
+  int pos;
+  if (k < a1) {   // element of run A: count run-B elements smaller
+    int lo = a1, hi = b1;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (rec_less(in[o + mid], r)) lo = mid + 1; else hi = mid;
+    }
+    pos = run0 + (k - a0) + (lo - a1);
+  } else {        // element of run B: count run-A elements smaller
+    int lo = a0, hi = a1;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (rec_less(in[o + mid], r)) lo = mid + 1; else hi = mid;
+    }
+    pos = run0 + (k - a1) + (lo - a0);
+  }
+  out[o + pos] = r;
+}
+
+// Keys of init_zindex (SRC/mrrr_vec.c:380-416): the running maximum of
+// W + sigma inside each block; one warp per block.
+__global__ void k_zkeys(ProbDev *probs, const BlockDev *blocks, const double *W, const double *E,
+                        const int *Windex, SortRec *rec) {
+  ProbDev *p = &probs[blockIdx.x];
+  if (p->trivial || p->status || p->jobz != MR3_JOB_V) return;
+  const int o = p->off;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const double ninf = -__longlong_as_double(0x7ff0000000000000LL);
+  for (int b = wid; b < p->nsplit; b += nw) {
+    const BlockDev *B = &blocks[o + b];
+    if (B->mbl <= 0) continue;
+    const double sigma = E[B->iend];
+    double run = ninf;
+    for (int c = 0; c < B->mbl; c += 32) {
+      const int k = c + lane;
+      double v = (k < B->mbl) ? W[B->wbgn + k] + sigma : ninf;
+      for (int sh = 1; sh < 32; sh <<= 1) {
+        double u = __shfl_up_sync(0xffffffffu, v, sh);
+        if (lane >= sh) v = fmax(v, u);
+      }
+      v = fmax(v, run);
+      if (k < B->mbl) {
+        const int s = B->wbgn + k;
+        rec[s].key = v;
+        rec[s].sec = ((long long)Windex[s] << 32) | (long long)b;
+        rec[s].idx = s - o;
+      }
+      run = __shfl_sync(0xffffffffu, v, 31);
+    }
+  }
+}
+
+// Keys for the final ascending sort of eigenvalues-only results (qsort in
+// SRC/mrrr.c:284) and of the bubble fix-up of sort_eigenpairs
+// (SRC/mrrr.c:560-585), which yields the stable order by value.
+__global__ void k_wkeys(int N, const ProbDev *probs, const int *prob_of_slot, const double *Wv,
+                        SortRec *rec, int want_job, const int *flag) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= N) return;
+  int pi = prob_of_slot[s];
+  if (pi < 0) return;
+  const ProbDev *p = &probs[pi];
+  if (p->trivial || p->status || p->jobz != want_job) return;
+  if (flag && !flag[pi]) return;
+  int k = s - p->off;
+  if (k >= p->m) return;
+  rec[s].key = Wv[s];
+  rec[s].sec = 0;
+  rec[s].idx = k;
+}
+
+__global__ void k_zindex_from_sorted(int N, const ProbDev *probs, const int *prob_of_slot,
+                                     const SortRec *rec, int *Zindex) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= N) return;
+  int pi = prob_of_slot[s];
+  if (pi < 0) return;
+  const ProbDev *p = &probs[pi];
+  int k = s - p->off;
+  if (k >= p->m || p->jobz != MR3_JOB_V || p->status) return;
+  Zindex[p->off + rec[s].idx] = k;
+}
+
+// ------------------------------------------------------------------------
+// Stage B, level 0: one cluster per block (init_workQ, SRC/mrrr_vec.c:304-374,
+// and the depth-0 branch of refine_eigvals, SRC/process_cluster.c:278-297).
+// ------------------------------------------------------------------------
+__global__ void k_level0(ProbDev *probs, BlockDev *blocks, const double *E, const double2 *gers,
+                         double *W, const double *Werr, double *Wsh, ClusterDev *cl,
+                         LevelCounters *lc, SngCounters *sc, int *unit_list) {
+  ProbDev *p = &probs[blockIdx.x];
+  if (p->trivial || p->status || p->jobz != MR3_JOB_V) return;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int b = wid; b < p->nsplit; b += nw) {
+    BlockDev *B = &blocks[p->off + b];
+    if (B->mbl <= 0) continue;
+    if (B->nbl == 1) {   // the eigenvector of a 1x1 block is a unit vector
+      if (lane == 0) unit_list[atomicAdd(&sc->n_unit, 1)] = B->wbgn;
+      continue;
+    }
+    const double sigma = E[B->iend];
+    const int wb = B->wbgn, we = wb + B->mbl - 1;
+    const double lgap = fmax(0.0, (W[wb] + sigma) - Werr[wb] - p->vl_out);
+    // spectral diameter of the block as refine_eigvals computes it at depth 0:
+    // discs of its first row and of rows bl_begin+1 .. bl_end-1
+    double gl = gers[B->ibgn].x, gu = gers[B->ibgn].y;
+    for (int i = B->ibgn + 1 + lane; i < B->iend; i += 32) {
+      gl = fmin(gl, gers[i].x);
+      gu = fmax(gu, gers[i].y);
+    }
+    gl = warp_min(gl);
+    gu = warp_max(gu);
+    __syncwarp();
+    for (int s = wb + lane; s <= we; s += 32) {
+      Wsh[s] = W[s];
+      W[s] = W[s] + sigma;
+    }
+    if (lane == 0) {
+      B->bl_spdiam = gu - gl;
+      int c = atomicAdd(&lc->n_cl, 1);
+      ClusterDev C;
+      C.begin = wb; C.end = we; C.depth = 0; C.blk = p->off + b;
+      C.bl_spdiam = gu - gl; C.lgap = lgap; C.par_off = -1; C.own_off = -1;
+      C.par_sigma = sigma; C.sigma = sigma;
+      cl[c] = C;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+// Child representation of each cluster of depth >= 1
+// (compute_new_rrr, SRC/process_cluster.c:105-235).  One warp per cluster.
+// ------------------------------------------------------------------------
+__device__ __forceinline__ void rrr_ptrs(const ClusterDev &C, const BlockDev &B, const double2 *RP,
+                                         const double2 *RQ, const double *arena,
+                                         const double2 **P, const double2 **Q) {
+  if (C.par_off < 0) { *P = RP + B.ibgn; *Q = RQ + B.ibgn; }
+  else {
+    *P = reinterpret_cast<const double2 *>(arena + C.par_off);
+    *Q = reinterpret_cast<const double2 *>(arena + C.par_off + 2 * (long long)B.nbl);
+  }
+}
+
+__global__ void __launch_bounds__(MR3_THREADS)
+k_newrrr(int ncl, ClusterDev *cl, const ProbDev *probs, const BlockDev *blocks,
+         const double2 *RP, const double2 *RQ, const double *arena_prev, double *arena_cur,
+         double *Wsh, double *Werr, double *Wgap, const int *Windex, int *cl_of_slot,
+         int *lvl_of_slot, int level, Tol tol) {
+  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (w >= ncl) return;
+  ClusterDev C = cl[w];
+  const BlockDev B = blocks[C.blk];
+  const ProbDev *p = &probs[B.prob];
+  const int nb = B.nbl, cb = C.begin, ce = C.end, csz = ce - cb + 1;
+  const double pivmin = p->pivmin;
+  const double2 *Pp, *Qp;
+  rrr_ptrs(C, B, RP, RQ, arena_prev, &Pp, &Qp);
+  double *slot = arena_cur + C.own_off;
+  double2 *Pn = reinterpret_cast<double2 *>(slot);
+  double2 *Qn = reinterpret_cast<double2 *>(slot + 2 * (long long)nb);
+  double *dplus = slot + 4 * (long long)nb, *lplus = slot + 5 * (long long)nb;
+  double *work = slot + 6 * (long long)nb;
+
+  // refine the extremal eigenvalues to full accuracy (dlarrb, RQtol) -- the
+  // two calls see a zero right gap, so their convergence test is independent
+  // of every other gap and they run side by side on lanes 0 and 1
+  const int maxitr = dv_itmax(C.bl_spdiam + pivmin, pivmin);
+  const int off1 = Windex[cb] - 1;
+  double wv = 0.0, ev = 0.0;
+  if (lane < 2) {
+    int sx = (lane == 0) ? cb : ce;
+    int i = Windex[sx];
+    int II = i - off1;
+    wv = Wsh[sx];
+    ev = Werr[sx];
+    dv_dlarrb_one(nb, Pp, i, 1, II > 1, 0.0, 0.0, tol.rqtol, tol.rqtol, pivmin, maxitr, nb, &wv,
+                  &ev);
+  }
+  double w0 = __shfl_sync(0xffffffffu, wv, 0), e0 = __shfl_sync(0xffffffffu, ev, 0);
+  double w1 = __shfl_sync(0xffffffffu, wv, 1), e1 = __shfl_sync(0xffffffffu, ev, 1);
+  if (lane == 0) {
+    // gap right of the first eigenvalue uses its neighbour before the second call
+    double nw_ = Wsh[cb + 1], ne_ = Werr[cb + 1];
+    Wgap[cb] = fmax(0.0, (nw_ - ne_) - (w0 + e0));
+    Wsh[cb] = w0; Werr[cb] = e0;
+    Wsh[ce] = w1; Werr[ce] = e1;
+  }
+  __syncwarp();
+  double tau = 0.0;
+  if (lane == 0) {
+    tau = dv_dlarrf(nb, Pp, Qp, csz, Wsh + cb, Wgap + cb, Werr + cb, C.bl_spdiam, C.lgap, Wgap[ce],
+                    pivmin, dplus, lplus, work);
+  }
+  tau = __shfl_sync(0xffffffffu, tau, 0);
+  __syncwarp();
+  const double sigma = C.par_sigma + tau;
+  for (int k = cb + lane; k <= ce; k += 32) {
+    double f = 3.0 * MR3_EPS * fabs(Wsh[k]);
+    double x = Wsh[k] - tau;
+    Wsh[k] = x;
+    f += 4.0 * MR3_EPS * fabs(x);
+    Werr[k] += f;
+    cl_of_slot[k] = w;
+    lvl_of_slot[k] = level;
+  }
+  for (int i = lane; i < nb; i += 32) {
+    double dv = dplus[i];
+    if (i < nb - 1) {
+      double lv = lplus[i];
+      double ld = dv * lv;
+      Pn[i] = make_double2(dv, ld * lv);
+      Qn[i] = make_double2(lv, ld);
+    } else {
+      Pn[i] = make_double2(dv, 0.0);
+      Qn[i] = make_double2(sigma, 0.0);
+    }
+  }
+  if (lane == 0) cl[w].sigma = sigma;
+}
+
+// Refinement of a level's clusters w.r.t. their new representation
+// (refine_eigvals without R-tasks, SRC/process_cluster.c:394-428).
+__global__ void __launch_bounds__(128)
+k_refine_cl(int N, const ClusterDev *cl, const ProbDev *probs, const BlockDev *blocks,
+            const double *arena_cur, double *Wsh, double *Werr, const double *Wgap,
+            const int *Windex, const int *cl_of_slot, const int *lvl_of_slot, int level, Tol tol) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= N || lvl_of_slot[s] != level) return;
+  const ClusterDev C = cl[cl_of_slot[s]];
+  const BlockDev &B = blocks[C.blk];
+  const ProbDev *p = &probs[B.prob];
+  const int pidx = Windex[C.begin], i = Windex[s], II = i - (pidx - 1);
+  const double2 *P = reinterpret_cast<const double2 *>(arena_cur + C.own_off);
+  const double rgap = Wgap[s];
+  const double lgap = (II > 1) ? Wgap[s - 1] : rgap;
+  const int maxitr = dv_itmax(C.bl_spdiam + p->pivmin, p->pivmin);
+  double w = Wsh[s], e = Werr[s];
+  dv_dlarrb_one(B.nbl, P, i, i == pidx, II > 1, rgap, lgap, tol.rtol1, tol.rtol2, p->pivmin,
+                maxitr, B.nbl, &w, &e);
+  Wsh[s] = w;
+  Werr[s] = e;
+}
+
+__global__ void k_gaps_cl(int N, const ClusterDev *cl, const double *Wsh, const double *Werr,
+                          double *Wgap, double *W, const int *cl_of_slot, const int *lvl_of_slot,
+                          int level) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= N || lvl_of_slot[s] != level) return;
+  const ClusterDev C = cl[cl_of_slot[s]];
+  if (s < C.end) Wgap[s] = fmax(0.0, Wsh[s + 1] - Werr[s + 1] - Wsh[s] - Werr[s]);
+  W[s] = Wsh[s] + C.sigma;
+}
+
+// ------------------------------------------------------------------------
+// Classification of a cluster's eigenvalues into singletons and child
+// clusters (PMR_create_subtasks, SRC/process_cluster.c:438-629).  One warp
+// per cluster and two passes: count, then write to the device queues.
+// ------------------------------------------------------------------------
+// Children of a segment [first, last] of a depth-0 cluster with more than
+// three members, split where the gap exceeds twice the average gap
+// (SRC/process_cluster.c:542-577).  Returns their number; writes them if out.
+__device__ int split_children(int first, int last, const ClusterDev &parent, double avggap,
+                              const double *Wgap, ClusterDev proto, ClusterDev *out,
+                              long long a_base, int crank, long long slot_sz) {
+  int cnt = 0, cl_first = first;
+  for (int k = first + 1; k < last; k++) {
+    int cl_last;
+    if (k == last - 1) cl_last = last;
+    else if (k != cl_first && Wgap[k] > 2.0 * avggap) cl_last = k;
+    else continue;
+    if (out) {
+      ClusterDev c = proto;
+      c.begin = cl_first; c.end = cl_last;
+      c.lgap = (cl_first == parent.begin) ? parent.lgap : Wgap[cl_first - 1];
+      c.own_off = a_base + (long long)(crank + cnt) * slot_sz;
+      out[crank + cnt] = c;
+    }
+    cnt++;
+    cl_first = k + 1;
+  }
+  return cnt;
+}
+
+__global__ void __launch_bounds__(MR3_THREADS)
+k_classify(int ncl, const ClusterDev *cl, const BlockDev *blocks, const double *Wsh,
+           const double *Wgap, ClusterDev *cl_next, SngDev *sng, WTask *wt,
+           LevelCounters *lcn, SngCounters *sc, int cap) {
+  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (w >= ncl) return;
+  const ClusterDev C = cl[w];
+  const BlockDev &B = blocks[C.blk];
+  const int cb = C.begin, ce = C.end, depth = C.depth, nb = B.nbl;
+  const long long slot_sz = 8LL * nb;
+  const double avggap = C.bl_spdiam / (nb - 1);
+  ClusterDev proto;
+  proto.begin = 0; proto.end = 0; proto.lgap = 0.0;
+  proto.depth = depth + 1; proto.blk = C.blk; proto.bl_spdiam = C.bl_spdiam;
+  proto.par_off = (depth == 0) ? -1 : C.own_off;
+  proto.par_sigma = C.sigma; proto.sigma = 0.0; proto.own_off = 0;
+  int s_base = 0, c_base = 0;
+  long long a_base = 0;
+  for (int pass = 0; pass < 2; pass++) {
+    int ns = 0, nc = 0, prev_end = cb - 1;
+    for (int c0 = cb; c0 <= ce; c0 += 32) {
+      const int s = c0 + lane;
+      bool flag = false;
+      if (s <= ce) flag = (s == ce) || (Wgap[s] >= MR3_MIN_RELGAP * fabs(Wsh[s]));
+      const unsigned bal = __ballot_sync(0xffffffffu, flag);
+      const unsigned below = bal & ((1u << lane) - 1u);
+      const int first = below ? (c0 + 31 - __clz(below)) + 1 : prev_end + 1;
+      int is_sng = 0, nchild = 0;
+      const bool split = flag && depth == 0 && (s - first + 1) > 3;
+      if (flag) {
+        if (s == first) is_sng = 1;
+        else if (split) nchild = split_children(first, s, C, avggap, Wgap, proto, nullptr, 0, 0, 0);
+        else nchild = 1;
+      }
+      int sr = is_sng, cr = nchild;
+      for (int o = 1; o < 32; o <<= 1) {
+        int a = __shfl_up_sync(0xffffffffu, sr, o), b = __shfl_up_sync(0xffffffffu, cr, o);
+        if (lane >= o) { sr += a; cr += b; }
+      }
+      if (pass == 1 && flag) {
+        const int srank = ns + sr - is_sng, crank = nc + cr - nchild;
+        if (is_sng) {
+          SngDev r;
+          r.slot = s; r.cl = w;
+          r.lgap = (s == cb) ? C.lgap : Wgap[s - 1];
+          sng[s_base + srank] = r;
+        } else if (split) {
+          split_children(first, s, C, avggap, Wgap, proto, cl_next + c_base, a_base, crank, slot_sz);
+        } else {
+          ClusterDev c = proto;
+          c.begin = first; c.end = s;
+          c.lgap = (first == cb) ? C.lgap : Wgap[first - 1];
+          c.own_off = a_base + (long long)crank * slot_sz;
+          cl_next[c_base + crank] = c;
+        }
+      }
+      ns += __shfl_sync(0xffffffffu, sr, 31);
+      nc += __shfl_sync(0xffffffffu, cr, 31);
+      prev_end = bal ? (c0 + 31 - __clz(bal)) : prev_end;
+    }
+    if (pass == 0) {
+      int err = 0;
+      if (lane == 0) {
+        s_base = atomicAdd(&sc->n_sng, ns);
+        const int nwt = (ns + 31) / 32;
+        const int t0 = atomicAdd(&sc->n_wt, nwt);
+        c_base = atomicAdd(&lcn->n_cl, nc);
+        a_base = (long long)atomicAdd(&lcn->arena_need, (unsigned long long)(nc * slot_sz));
+        if (s_base + ns > cap || c_base + nc > cap || t0 + nwt > cap) {
+          atomicOr(&lcn->err, 1);
+          err = 1;
+        } else {
+          for (int t = 0; t < nwt; t++) {
+            WTask x;
+            x.first = s_base + 32 * t;
+            x.count = min(32, ns - 32 * t);
+            wt[t0 + t] = x;
+          }
+        }
+      }
+      s_base = __shfl_sync(0xffffffffu, s_base, 0);
+      c_base = __shfl_sync(0xffffffffu, c_base, 0);
+      a_base = __shfl_sync(0xffffffffu, a_base, 0);
+      if (__shfl_sync(0xffffffffu, err, 0)) return;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+// Singletons (PMR_process_s_task, SRC/process_singleton.c:65-317): one lane
+// per eigenvector, 32 eigenvectors of one cluster per warp.  Persistent warps
+// pull warp tasks from a device counter.  Each warp owns a scratch region of
+// 2 x nmax x 32 doubles laid out [array][row][lane] so that the lock-step
+// passes of the twisted factorisation read and write whole 256-byte rows.
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(MR3_THREADS)
+k_singletons(const WTask *wt, const SngDev *sng, const ClusterDev *cl, const ProbDev *probs,
+             const BlockDev *blocks, const double2 *RP, const double2 *RQ, const double *arena,
+             double *W, double *Wsh, double *Werr, double *Wgap, const int *Windex,
+             const int *Zindex, SngCounters *sc, double *scratch, long long nmax) {
+  const int lane = threadIdx.x & 31;
+  const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  double *X = scratch + gw * 2 * nmax * 32 + lane;
+  double *Y = X + nmax * 32;
+  const int nwt = sc->n_wt;
+  for (;;) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(&sc->wt_next, 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= nwt) break;
+    const WTask T = wt[t];
+    const bool active = lane < T.count;
+    const SngDev S = sng[T.first + (active ? lane : 0)];
+    const ClusterDev C = cl[S.cl];
+    const BlockDev &B = blocks[C.blk];
+    const ProbDev *p = &probs[B.prob];
+    const int nb = B.nbl;
+    const double pivmin = p->pivmin;
+    const double2 *P, *Q;
+    if (C.depth == 0) { P = RP + B.ibgn; Q = RQ + B.ibgn; }
+    else {
+      P = reinterpret_cast<const double2 *>(arena + C.own_off);
+      Q = reinterpret_cast<const double2 *>(arena + C.own_off + 2 * (long long)nb);
+    }
+    const double sigma = C.sigma;
+    int r = 0, is1 = 1, is2 = nb;
+    double norminv = 0.0;
+    int zind = 0;
+    if (active) {
+      const int s = S.slot;
+      const double twoeps = 2.0 * MR3_EPS, rqtol = 2.0 * MR3_EPS;
+      const double tolr = 4.0 * dv_log((double)nb) * MR3_EPS;
+      double lambda = Wsh[s], wsh = Wsh[s], werr = Werr[s];
+      double left = lambda - werr, right = lambda + werr;
+      const int iloc = Windex[s];
+      // the reference compares the eigenvalue index with the block's first
+      // and last row (SRC/process_singleton.c:142-157); W slots and rows of a
+      // problem start at the same offset, so the same comparison is s == row
+      double lgap = (s == B.ibgn) ? MR3_EPS * fmax(fabs(left), fabs(right)) : S.lgap;
+      double rgap = (s == B.iend) ? MR3_EPS * fmax(fabs(left), fabs(right)) : Wgap[s];
+      double gap = fmin(lgap, rgap);
+      double gaptol = (s == B.ibgn || s == B.iend) ? 0.0 : gap * MR3_EPS;
+      int supmn = nb, supmx = 1;
+      bool usedBS = false, usedRQ = false, needBS = false, wantNC = true;
+      double bstres = 0.0, bstw = 0.0, resid = 0.0;
+      const int maxitr = dv_itmax(C.bl_spdiam + pivmin, pivmin);
+      dlar1v_out o;
+      for (int k = 1; k <= MR3_MAXITER; k++) {
+        if (needBS) {
+          usedBS = true;
+          int tw = (r < 1 || r > nb) ? nb : r;
+          dv_dlarrb_one(nb, P, iloc, 1, 0, 0.0, 0.0, 0.0, twoeps, pivmin, maxitr, tw, &wsh, &werr);
+          lambda = wsh;
+          r = 0;
+        }
+        wantNC = !usedBS;
+        dv_dlar1v(nb, lambda, P, Q, pivmin, gaptol, wantNC, r, X, Y, 32, &o);
+        r = o.r;
+        resid = o.resid;
+        if (k == 1 || o.resid < bstres) { bstres = o.resid; bstw = lambda; }
+        supmn = min(supmn, o.isupp1);
+        supmx = max(supmx, o.isupp2);
+        if (!usedBS && o.resid > tolr * gap && fabs(o.rqcorr) > rqtol * fabs(lambda)) {
+          int sgndef = (iloc <= o.negcnt) ? -1 : 1;
+          if (o.rqcorr * sgndef >= 0.0 && lambda + o.rqcorr <= right &&
+              lambda + o.rqcorr >= left) {
+            usedRQ = true;
+            if (sgndef == 1) left = lambda; else right = lambda;
+            wsh = 0.5 * (left + right);
+            lambda += o.rqcorr;
+          } else {
+            needBS = true;
+          }
+          if (right - left < rqtol * fabs(lambda)) usedBS = true;
+          else if (k == MR3_MAXITER - 1) needBS = true;
+        } else {
+          break;
+        }
+      }
+      if (usedRQ && usedBS && bstres <= resid) {
+        lambda = bstw;
+        dv_dlar1v(nb, lambda, P, Q, pivmin, gaptol, wantNC, r, X, Y, 32, &o);
+        r = o.r;
+      }
+      (void)supmn; (void)supmx;
+      Wsh[s] = lambda;
+      Werr[s] = werr;
+      Wgap[s] = gap;
+      W[s] = lambda + sigma;
+      is1 = o.isupp1;
+      is2 = o.isupp2;
+      norminv = o.nrminv;
+      zind = Zindex[s];
+      const int bl0 = B.ibgn - p->off;   // block's first row inside the problem
+      p->Zsupp[2 * (size_t)zind] = is1 + bl0;
+      p->Zsupp[2 * (size_t)zind + 1] = is2 + bl0;
+    }
+    __syncwarp();
+    // write the warp's eigenvectors: whole columns, rows spread over lanes
+    const int np = p->n, bl0 = B.ibgn - p->off;
+    const size_t ldz = (size_t)p->ldz;
+    for (int v = 0; v < T.count; v++) {
+      const int rv = __shfl_sync(0xffffffffu, r, v);
+      const int a1 = __shfl_sync(0xffffffffu, is1, v), a2 = __shfl_sync(0xffffffffu, is2, v);
+      const double nv = __shfl_sync(0xffffffffu, norminv, v);
+      const int zc = __shfl_sync(0xffffffffu, zind, v);
+      double *Zc = p->Z + (size_t)zc * ldz;
+      const double *Xv = X - lane + v, *Yv = Y - lane + v;
+      for (int row = lane; row < np; row += 32) {
+        int k = row - bl0 + 1;   // 1-based row inside the block
+        double val = 0.0;
+        if (k >= a1 && k <= a2) val = dv_zget(Xv, Yv, 32, rv, k) * nv;
+        Zc[row] = val;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// Unit vectors of 1x1 blocks (SRC/process_singleton.c:125-133).
+__global__ void k_unitvec(const int *list, const SngCounters *sc, const ProbDev *probs,
+                          const BlockDev *blocks, const int *iblk, const int *Zindex) {
+  int t = blockIdx.x;
+  if (t >= sc->n_unit) return;
+  int s = list[t];
+  const BlockDev &B = blocks[iblk[s]];
+  const ProbDev *p = &probs[B.prob];
+  int zind = Zindex[s];
+  double *Zc = p->Z + (size_t)zind * (size_t)p->ldz;
+  int row0 = B.ibgn - p->off;
+  for (int row = threadIdx.x; row < p->n; row += blockDim.x) Zc[row] = (row == row0) ? 1.0 : 0.0;
+  if (threadIdx.x == 0) {
+    p->Zsupp[2 * (size_t)zind] = row0 + 1;
+    p->Zsupp[2 * (size_t)zind + 1] = row0 + 1;
+  }
+}
+
+// ------------------------------------------------------------------------
+// Output ordering (sort_eigenpairs, SRC/mrrr.c:525-588) and copy-out.
+// ------------------------------------------------------------------------
+__global__ void k_place_w(int N, const ProbDev *probs, const int *prob_of_slot, const double *W,
+                          const int *Zindex, double *Wout) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= N) return;
+  int pi = prob_of_slot[s];
+  if (pi < 0) return;
+  const ProbDev *p = &probs[pi];
+  int k = s - p->off;
+  if (k >= p->m || p->status) return;
+  if (p->jobz == MR3_JOB_V) Wout[p->off + Zindex[s]] = W[s];
+  else Wout[s] = W[s];
+}
+
+__global__ void k_check_sorted(int N, ProbDev *probs, const int *prob_of_slot, const double *Wout,
+                               int *unsorted) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= N) return;
+  int pi = prob_of_slot[s];
+  if (pi < 0) return;
+  const ProbDev *p = &probs[pi];
+  int k = s - p->off;
+  if (k + 1 >= p->m || p->status || p->jobz == MR3_JOB_C) return;
+  if (Wout[s] > Wout[s + 1]) atomicOr(&unsorted[pi], 1);
+}
+
+__global__ void k_scatter(const ProbDev *probs, double *const *Wp, double *const *Dp,
+                          double *const *Ep, const double *Wout, const double *D, const double *E) {
+  const ProbDev *p = &probs[blockIdx.x];
+  if (p->trivial) return;
+  for (int i = threadIdx.x; i < p->n; i += blockDim.x) {
+    if (i < p->m && p->jobz != MR3_JOB_C && !p->status) Wp[blockIdx.x][i] = Wout[p->off + i];
+    Dp[blockIdx.x][i] = D[p->off + i];
+    Ep[blockIdx.x][i] = E[p->off + i];
+  }
+}
+
+__global__ void k_sorted_to_w(int N, const ProbDev *probs, const int *prob_of_slot,
+                              const SortRec *rec, double *Wout, int want_job, const int *flag) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= N) return;
+  int pi = prob_of_slot[s];
+  if (pi < 0) return;
+  const ProbDev *p = &probs[pi];
+  if (p->trivial || p->status || p->jobz != want_job) return;
+  if (flag && !flag[pi]) return;
+  if (s - p->off < p->m) Wout[s] = rec[s].key;
+}
+
+// Apply the permutation of the bubble fix-up to Zsupp (new column k takes
+// old column rec[k].idx); W was already rewritten from the sorted keys.
+__global__ void k_perm_zsupp(int N, const ProbDev *probs, const int *prob_of_slot,
+                             const SortRec *rec, const int *flag, int *tmp2) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= N) return;
+  int pi = prob_of_slot[s];
+  if (pi < 0 || !flag[pi]) return;
+  const ProbDev *p = &probs[pi];
+  int k = s - p->off;
+  if (k >= p->m) return;
+  int src = rec[s].idx;
+  tmp2[2 * (size_t)s] = p->Zsupp[2 * (size_t)src];
+  tmp2[2 * (size_t)s + 1] = p->Zsupp[2 * (size_t)src + 1];
+}
+__global__ void k_perm_zsupp2(int N, const ProbDev *probs, const int *prob_of_slot, const int *flag,
+                              const int *tmp2) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= N) return;
+  int pi = prob_of_slot[s];
+  if (pi < 0 || !flag[pi]) return;
+  const ProbDev *p = &probs[pi];
+  int k = s - p->off;
+  if (k >= p->m) return;
+  p->Zsupp[2 * (size_t)k] = tmp2[2 * (size_t)s];
+  p->Zsupp[2 * (size_t)k + 1] = tmp2[2 * (size_t)s + 1];
+}
+
+// ========================================================================
+// Host side
+// ========================================================================
+struct mr3_cuda_ctx {
+  int device = 0, nsm = 148;
+  cudaStream_t own = nullptr;
+  char err[256] = {0};
+  long long launches = 0;
+  size_t capN = 0, capP = 0, capScratch = 0, capArena[2] = {0, 0};
+  ProbDev *probs = nullptr;
+  BlockDev *blocks = nullptr;
+  int *blk_of_row = nullptr, *Windex = nullptr, *iblk = nullptr, *It = nullptr, *Zindex = nullptr;
+  int *prob_of_slot = nullptr, *cl_of_slot = nullptr, *lvl_of_slot = nullptr, *unit_list = nullptr;
+  int *flag = nullptr, *tmp2 = nullptr;
+  double *D = nullptr, *E = nullptr, *E2 = nullptr, *Wt = nullptr, *Et = nullptr, *W = nullptr;
+  double *Werr = nullptr, *Wgap = nullptr, *Wcopy = nullptr, *Wsh = nullptr, *Dt = nullptr;
+  double *Lt = nullptr, *Wout = nullptr;
+  double2 *gers = nullptr, *TP = nullptr, *TPc = nullptr, *RP = nullptr, *RQ = nullptr;
+  SortRec *rec0 = nullptr, *rec1 = nullptr;
+  ClusterDev *cl[2] = {nullptr, nullptr};
+  SngDev *sng = nullptr;
+  WTask *wt = nullptr;
+  LevelCounters *lc = nullptr;
+  SngCounters *sc = nullptr;
+  double *scratch = nullptr, *arena[2] = {nullptr, nullptr};
+  const double **Din = nullptr, **Ein = nullptr;
+  double **Wp = nullptr, **Dp = nullptr, **Ep = nullptr;
+  // pinned host mirrors
+  ProbDev *h_probs = nullptr;
+  void **h_ptrs = nullptr;
+  LevelCounters *h_lc = nullptr;
+  SngCounters *h_sc = nullptr;
+  int *h_flag = nullptr;
+  double *h_const = nullptr;   // {1.0}
+  int *h_iconst = nullptr;     // {1, 1}
+  void *ws[MR3_CUDA_WS_SLOTS] = {nullptr};
+  size_t ws_cap[MR3_CUDA_WS_SLOTS] = {0};
+};
+
+#define CK(call, what)                                                    \
+  do {                                                                    \
+    cudaError_t e_ = (call);                                              \
+    if (e_ != cudaSuccess) {                                              \
+      snprintf(c->err, sizeof(c->err), "%s: %s", what, cudaGetErrorString(e_)); \
+      return MR3_EMISC;                                                   \
+    }                                                                     \
+  } while (0)
+
+#define LAUNCH(kern, grid, block, ...)                                    \
+  do {                                                                    \
+    if ((grid) > 0) {                                                     \
+      kern<<<(grid), (block), 0, st>>>(__VA_ARGS__);                      \
+      c->launches++;                                                      \
+      CK(cudaGetLastError(), #kern);                                      \
+    }                                                                     \
+  } while (0)
+
+template <typename T>
+static cudaError_t regrow(T **p, size_t count) {
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  return cudaMalloc((void **)p, std::max<size_t>(count, 1) * sizeof(T));
+}
+
+static int ensure_rows(mr3_cuda_ctx *c, size_t N, size_t P) {
+  if (N > c->capN) {
+    size_t n = std::max(N, c->capN + c->capN / 2);
+    CK(regrow(&c->blocks, n), "blocks");
+    CK(regrow(&c->blk_of_row, n), "blk_of_row");
+    CK(regrow(&c->Windex, n), "Windex");
+    CK(regrow(&c->iblk, n), "iblk");
+    CK(regrow(&c->It, n), "It");
+    CK(regrow(&c->Zindex, n), "Zindex");
+    CK(regrow(&c->prob_of_slot, n), "prob_of_slot");
+    CK(regrow(&c->cl_of_slot, n), "cl_of_slot");
+    CK(regrow(&c->lvl_of_slot, n), "lvl_of_slot");
+    CK(regrow(&c->unit_list, n), "unit_list");
+    CK(regrow(&c->tmp2, 2 * n), "tmp2");
+    double **dd[] = {&c->D, &c->E, &c->E2, &c->Wt, &c->Et, &c->W, &c->Werr, &c->Wgap,
+                     &c->Wcopy, &c->Wsh, &c->Dt, &c->Lt, &c->Wout};
+    for (double **q : dd) CK(regrow(q, n), "rows");
+    double2 **d2[] = {&c->gers, &c->TP, &c->TPc, &c->RP, &c->RQ};
+    for (double2 **q : d2) CK(regrow(q, n), "rows2");
+    CK(regrow(&c->rec0, n), "rec0");
+    CK(regrow(&c->rec1, n), "rec1");
+    CK(regrow(&c->cl[0], n), "cl0");
+    CK(regrow(&c->cl[1], n), "cl1");
+    CK(regrow(&c->sng, n), "sng");
+    CK(regrow(&c->wt, n), "wt");
+    c->capN = n;
+  }
+  if (P > c->capP) {
+    size_t p = std::max(P, c->capP + c->capP / 2);
+    CK(regrow(&c->probs, p), "probs");
+    CK(regrow(&c->flag, p), "flag");
+    CK(regrow(&c->Din, p), "Din");
+    CK(regrow(&c->Ein, p), "Ein");
+    CK(regrow(&c->Wp, p), "Wp");
+    CK(regrow(&c->Dp, p), "Dp");
+    CK(regrow(&c->Ep, p), "Ep");
+    if (c->h_probs) cudaFreeHost(c->h_probs);
+    if (c->h_ptrs) cudaFreeHost(c->h_ptrs);
+    if (c->h_flag) cudaFreeHost(c->h_flag);
+    CK(cudaMallocHost((void **)&c->h_probs, p * sizeof(ProbDev)), "h_probs");
+    CK(cudaMallocHost((void **)&c->h_ptrs, 5 * p * sizeof(void *)), "h_ptrs");
+    CK(cudaMallocHost((void **)&c->h_flag, p * sizeof(int)), "h_flag");
+    c->capP = p;
+  }
+  return MR3_OK;
+}
+
+extern "C" int mr3_cuda_ctx_create(int device, mr3_cuda_ctx **out) {
+  *out = nullptr;
+  if (cudaSetDevice(device) != cudaSuccess) return MR3_EMISC;
+  mr3_cuda_ctx *c = new mr3_cuda_ctx();
+  c->device = device;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->nsm = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc((void **)&c->lc, 2 * sizeof(LevelCounters)) != cudaSuccess ||
+      cudaMalloc((void **)&c->sc, sizeof(SngCounters)) != cudaSuccess ||
+      cudaMallocHost((void **)&c->h_lc, 2 * sizeof(LevelCounters)) != cudaSuccess ||
+      cudaMallocHost((void **)&c->h_sc, sizeof(SngCounters)) != cudaSuccess ||
+      cudaMallocHost((void **)&c->h_const, sizeof(double)) != cudaSuccess ||
+      cudaMallocHost((void **)&c->h_iconst, 2 * sizeof(int)) != cudaSuccess) {
+    mr3_cuda_ctx_destroy(c);
+    return MR3_EMISC;
+  }
+  c->h_const[0] = 1.0;
+  c->h_iconst[0] = 1;
+  c->h_iconst[1] = 1;
+  *out = c;
+  return MR3_OK;
+}
+
+extern "C" void mr3_cuda_ctx_destroy(mr3_cuda_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  void *dev[] = {c->probs, c->blocks, c->blk_of_row, c->Windex, c->iblk, c->It, c->Zindex,
+                 c->prob_of_slot, c->cl_of_slot, c->lvl_of_slot, c->unit_list, c->flag, c->tmp2,
+                 c->D, c->E, c->E2, c->Wt, c->Et, c->W, c->Werr, c->Wgap, c->Wcopy, c->Wsh,
+                 c->Dt, c->Lt, c->Wout, c->gers, c->TP, c->TPc, c->RP, c->RQ, c->rec0, c->rec1,
+                 c->cl[0], c->cl[1], c->sng, c->wt, c->lc, c->sc, c->scratch, c->arena[0],
+                 c->arena[1], (void *)c->Din, (void *)c->Ein, c->Wp, c->Dp, c->Ep};
+  for (void *q : dev)
+    if (q) cudaFree(q);
+  for (int i = 0; i < MR3_CUDA_WS_SLOTS; i++)
+    if (c->ws[i]) cudaFree(c->ws[i]);
+  void *host[] = {c->h_probs, c->h_ptrs, c->h_lc, c->h_sc, c->h_flag, c->h_const, c->h_iconst};
+  for (void *q : host)
+    if (q) cudaFreeHost(q);
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+}
+
+extern "C" void *mr3_cuda_ws(mr3_cuda_ctx *c, int slot, size_t bytes) {
+  if (!c || slot < 0 || slot >= MR3_CUDA_WS_SLOTS) return nullptr;
+  if (bytes > c->ws_cap[slot] || !c->ws[slot]) {
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->own);
+    if (c->ws[slot]) cudaFree(c->ws[slot]);
+    c->ws[slot] = nullptr;
+    c->ws_cap[slot] = 0;
+    size_t sz = std::max<size_t>(bytes, 256);
+    if (cudaMalloc(&c->ws[slot], sz) != cudaSuccess) {
+      snprintf(c->err, sizeof(c->err), "workspace of %zu bytes", sz);
+      return nullptr;
+    }
+    c->ws_cap[slot] = sz;
+  }
+  return c->ws[slot];
+}
+
+extern "C" int mr3_cuda_copy(mr3_cuda_ctx *c, void *dst, const void *src, size_t bytes, int dir) {
+  if (!c) return MR3_EMISC;
+  if (bytes == 0) return MR3_OK;
+  CK(cudaMemcpyAsync(dst, src, bytes, dir == 0 ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost,
+                     c->own), "copy");
+  return MR3_OK;
+}
+
+extern "C" int mr3_cuda_copy2d(mr3_cuda_ctx *c, void *dst, size_t dpitch, const void *src,
+                               size_t spitch, size_t width, size_t height, int dir) {
+  if (!c) return MR3_EMISC;
+  if (width == 0 || height == 0) return MR3_OK;
+  CK(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height,
+                       dir == 0 ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost, c->own),
+     "copy2d");
+  return MR3_OK;
+}
+
+extern "C" int mr3_cuda_sync(mr3_cuda_ctx *c) {
+  if (!c) return MR3_EMISC;
+  CK(cudaStreamSynchronize(c->own), "sync");
+  return MR3_OK;
+}
+
+extern "C" long long mr3_cuda_last_launches(const mr3_cuda_ctx *c) { return c ? c->launches : 0; }
+extern "C" const char *mr3_cuda_last_error(const mr3_cuda_ctx *c) { return c ? c->err : ""; }
+
+static int valid_prob(const mr3_cuda_prob &q) {
+  if (q.jobz < MR3_JOB_N || q.jobz > MR3_JOB_C) return 0;
+  if (q.range < MR3_RANGE_A || q.range > MR3_RANGE_I) return 0;
+  if (q.n <= 0) return 0;
+  if (q.range == MR3_RANGE_V && !(q.vu > q.vl)) return 0;
+  if (q.range == MR3_RANGE_I && (q.il < 1 || q.il > q.n || q.iu < q.il || q.iu > q.n)) return 0;
+  if (q.jobz == MR3_JOB_V && q.ldz < q.n) return 0;
+  return 1;
+}
+
+// Sort the records of the problems selected by (want_job, flag) in place in
+// rec0/rec1; returns the buffer holding the result.
+static SortRec *merge_sort(mr3_cuda_ctx *c, cudaStream_t st, int N, int mmax, int want_job,
+                           const int *flag, int *rc) {
+  SortRec *in = c->rec0, *out = c->rec1;
+  *rc = MR3_OK;
+  for (int width = 1; width < mmax; width *= 2) {
+    k_merge_pass<<<(N + 255) / 256, 256, 0, st>>>(N, c->probs, c->prob_of_slot, in, out, width,
+                                                   want_job, flag);
+    c->launches++;
+    if (cudaGetLastError() != cudaSuccess) { *rc = MR3_EMISC; return in; }
+    // elements of unselected problems stay in `in` only; copy them over by
+    // swapping only what was written: every selected element was written.
+    std::swap(in, out);
+  }
+  return in;
+}
+
+extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *stream) {
+  if (!c) return MR3_EMISC;
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->own;
+  c->launches = 0;
+  c->err[0] = 0;
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  if (P <= 0) return MR3_OK;
+
+  // ---- host-side triage: invalid and trivial problems
+  size_t N = 0;
+  int nmaxV = 0, mmax = 0, nlive = 0;
+  bool anyV = false, anyN = false, anyTry = false;
+  std::vector<int> off(P), live(P, 0);
+  for (int i = 0; i < P; i++) {
+    mr3_cuda_prob &q = pr[i];
+    q.m = 0;
+    q.info = MR3_OK;
+    q.il_out = q.il; q.iu_out = q.iu; q.vl_out = q.vl; q.vu_out = q.vu; q.tryrac_out = q.tryrac;
+    off[i] = (int)N;
+    if (!valid_prob(q)) { q.info = MR3_EARG; continue; }
+    if (q.jobz == MR3_JOB_C && q.range != MR3_RANGE_V) {   // SRC/mrrr.c:130-138
+      q.m = (q.range == MR3_RANGE_A) ? q.n : q.iu - q.il + 1;
+      continue;
+    }
+    if (q.n == 1) {   // a 1x1 matrix: its entry is the eigenvalue
+      double d0;
+      CK(cudaMemcpyAsync(&d0, q.D, sizeof(double), cudaMemcpyDeviceToHost, st), "n1 D");
+      CK(cudaStreamSynchronize(st), "n1 sync");
+      bool take = q.range != MR3_RANGE_V || (d0 > q.vl && d0 <= q.vu);
+      q.m = take ? 1 : 0;
+      if (take && q.jobz != MR3_JOB_C) {
+        CK(cudaMemcpyAsync(q.W, q.D, sizeof(double), cudaMemcpyDeviceToDevice, st), "n1 W");
+        if (q.jobz == MR3_JOB_V) {
+          CK(cudaMemcpyAsync(q.Z, c->h_const, sizeof(double), cudaMemcpyHostToDevice, st), "n1 Z");
+          CK(cudaMemcpyAsync(q.Zsupp, c->h_iconst, 2 * sizeof(int), cudaMemcpyHostToDevice, st),
+             "n1 Zsupp");
+        }
+      }
+      continue;
+    }
+    live[i] = 1;
+    nlive++;
+    N += (size_t)q.n;
+    mmax = std::max(mmax, q.n);
+    if (q.jobz == MR3_JOB_V) { anyV = true; nmaxV = std::max(nmaxV, q.n); }
+    if (q.jobz == MR3_JOB_N) anyN = true;
+    if (q.tryrac) anyTry = true;
+  }
+  if (nlive == 0) return cudaStreamSynchronize(st) == cudaSuccess ? MR3_OK : MR3_EMISC;
+
+  // compact the live problems
+  std::vector<int> idx;
+  idx.reserve(nlive);
+  for (int i = 0; i < P; i++)
+    if (live[i]) idx.push_back(i);
+  const int L = nlive;
+  int rc = ensure_rows(c, N, (size_t)L);
+  if (rc != MR3_OK) return rc;
+  const int NN = (int)N;
+  {
+    int o = 0;
+    for (int k = 0; k < L; k++) {
+      const mr3_cuda_prob &q = pr[idx[k]];
+      ProbDev &h = c->h_probs[k];
+      memset(&h, 0, sizeof(ProbDev));
+      h.n = q.n; h.off = o; h.jobz = q.jobz; h.range = q.range; h.il = q.il; h.iu = q.iu;
+      h.tryrac = q.tryrac; h.ldz = q.ldz; h.vl = q.vl; h.vu = q.vu; h.Z = q.Z; h.Zsupp = q.Zsupp;
+      h.scale = 1.0;
+      o += q.n;
+      c->h_ptrs[k] = (void *)q.D;
+      c->h_ptrs[L + k] = (void *)q.E;
+      c->h_ptrs[2 * L + k] = (void *)q.W;
+      c->h_ptrs[3 * L + k] = (void *)q.D;
+      c->h_ptrs[4 * L + k] = (void *)q.E;
+    }
+  }
+  CK(cudaMemcpyAsync(c->probs, c->h_probs, L * sizeof(ProbDev), cudaMemcpyHostToDevice, st), "probs");
+  CK(cudaMemcpyAsync(c->Din, c->h_ptrs, L * sizeof(void *), cudaMemcpyHostToDevice, st), "Din");
+  CK(cudaMemcpyAsync(c->Ein, c->h_ptrs + L, L * sizeof(void *), cudaMemcpyHostToDevice, st), "Ein");
+  CK(cudaMemcpyAsync(c->Wp, c->h_ptrs + 2 * L, L * sizeof(void *), cudaMemcpyHostToDevice, st), "Wp");
+  CK(cudaMemcpyAsync(c->Dp, c->h_ptrs + 3 * L, L * sizeof(void *), cudaMemcpyHostToDevice, st), "Dp");
+  CK(cudaMemcpyAsync(c->Ep, c->h_ptrs + 4 * L, L * sizeof(void *), cudaMemcpyHostToDevice, st), "Ep");
+
+  Tol tol;
+  tol.rtol1 = fmin(sqrt(2.220446049250313e-16), 1e-2 * 1e-3);
+  tol.rtol2 = fmax(fmin(tol.rtol1 * 5.0E-3, 1e-3 * 5.0E-6), 4.0 * 2.220446049250313e-16);
+  tol.bsrtol = fmin(1e-3 * 1.0E-2, sqrt(2.220446049250313e-16));
+  tol.rqtol = 2.0 * 2.220446049250313e-16;
+  const int gN = (NN + 255) / 256, gN128 = (NN + 127) / 128;
+
+  // ---- stage A: eigenvalues
+  LAUNCH(k_gather, L, 256, c->probs, c->Din, c->Ein, c->D, c->E, c->prob_of_slot, c->iblk);
+  LAUNCH(k_prologue, L, MR3_THREADS, c->probs, c->blocks, c->blk_of_row, c->D, c->E, c->E2,
+         c->gers, c->TP, c->TPc, tol);
+  LAUNCH(k_blocks, L, MR3_THREADS, c->probs, c->blocks, c->D, c->E, c->gers, c->TP, tol);
+  LAUNCH(k_bisect, gN128, 128, NN, c->probs, c->blocks, c->blk_of_row, c->TP, c->Wt, c->Et, c->It,
+         tol);
+  LAUNCH(k_compact, L, MR3_THREADS, c->probs, c->blocks, c->D, c->Wt, c->Et, c->It, c->W, c->Werr,
+         c->Windex, c->iblk, c->Wcopy);
+  LAUNCH(k_gaps_init, gN, 256, NN, c->probs, c->blocks, c->iblk, c->W, c->Werr, c->Wgap);
+  LAUNCH(k_root, L, MR3_THREADS, c->probs, c->blocks, c->D, c->E, c->TP, c->Dt, c->Lt, c->W,
+         c->Werr, c->Wgap, c->RP, c->RQ);
+  LAUNCH(k_refine_root, gN128, 128, NN, c->probs, c->blocks, c->iblk, c->RP, c->W, c->Werr,
+         c->Wgap, tol);
+  LAUNCH(k_gaps_root, gN, 256, NN, c->probs, c->blocks, c->iblk, c->W, c->Werr, c->Wgap);
+  LAUNCH(k_discard, (L + 127) / 128, 128, c->probs, L, c->blocks, c->W, c->Werr, c->Wgap,
+         c->Windex, c->iblk, c->Wcopy);
+
+  // ---- stage B: eigenvectors
+  if (anyV) {
+    LAUNCH(k_zkeys, L, MR3_THREADS, c->probs, c->blocks, c->W, c->E, c->Windex, c->rec0);
+    SortRec *sorted = merge_sort(c, st, NN, mmax, MR3_JOB_V, nullptr, &rc);
+    if (rc != MR3_OK) { snprintf(c->err, sizeof(c->err), "merge sort"); return rc; }
+    LAUNCH(k_zindex_from_sorted, gN, 256, NN, c->probs, c->prob_of_slot, sorted, c->Zindex);
+    CK(cudaMemsetAsync(c->lc, 0, 2 * sizeof(LevelCounters), st), "lc");
+    CK(cudaMemsetAsync(c->sc, 0, sizeof(SngCounters), st), "sc");
+    CK(cudaMemsetAsync(c->lvl_of_slot, 0xff, N * sizeof(int), st), "lvl");
+    LAUNCH(k_level0, L, MR3_THREADS, c->probs, c->blocks, c->E, c->gers, c->W, c->Werr, c->Wsh,
+           c->cl[0], &c->lc[0], c->sc, c->unit_list);
+    CK(cudaMemcpyAsync(c->h_lc, c->lc, sizeof(LevelCounters), cudaMemcpyDeviceToHost, st), "lc0");
+    CK(cudaMemcpyAsync(c->h_sc, c->sc, sizeof(SngCounters), cudaMemcpyDeviceToHost, st), "sc0");
+    CK(cudaStreamSynchronize(st), "level0 sync");
+    if (c->h_sc->n_unit > 0)
+      LAUNCH(k_unitvec, c->h_sc->n_unit, 256, c->unit_list, c->sc, c->probs, c->blocks, c->iblk,
+             c->Zindex);
+    // singleton scratch: 2 x nmax x 32 doubles per persistent warp
+    const size_t per_warp = 2ull * (size_t)nmaxV * 32ull;
+    const size_t budget = (size_t)8 << 30;   // bytes
+    size_t nwarps = std::min<size_t>((size_t)c->nsm * 32, std::max<size_t>(c->nsm, budget / (per_warp * 8)));
+    nwarps = (nwarps + 7) / 8 * 8;
+    if (nwarps * per_warp > c->capScratch) {
+      CK(regrow(&c->scratch, nwarps * per_warp), "scratch");
+      c->capScratch = nwarps * per_warp;
+    }
+    int ncl = c->h_lc[0].n_cl;
+    const int DEPTH_CAP = 512;
+    for (int level = 0; ncl > 0; level++) {
+      if (level >= DEPTH_CAP) { snprintf(c->err, sizeof(c->err), "representation tree too deep"); return MR3_EMISC; }
+      const int cur = level & 1, nxt = cur ^ 1;
+      const int gW = (ncl * 32 + MR3_THREADS - 1) / MR3_THREADS;
+      if (level > 0) {
+        LAUNCH(k_newrrr, gW, MR3_THREADS, ncl, c->cl[cur], c->probs, c->blocks, c->RP, c->RQ,
+               c->arena[nxt], c->arena[cur], c->Wsh, c->Werr, c->Wgap, c->Windex, c->cl_of_slot,
+               c->lvl_of_slot, level, tol);
+        LAUNCH(k_refine_cl, gN128, 128, NN, c->cl[cur], c->probs, c->blocks, c->arena[cur], c->Wsh,
+               c->Werr, c->Wgap, c->Windex, c->cl_of_slot, c->lvl_of_slot, level, tol);
+        LAUNCH(k_gaps_cl, gN, 256, NN, c->cl[cur], c->Wsh, c->Werr, c->Wgap, c->W, c->cl_of_slot,
+               c->lvl_of_slot, level);
+      }
+      CK(cudaMemsetAsync(&c->lc[nxt], 0, sizeof(LevelCounters), st), "lcn");
+      CK(cudaMemsetAsync(c->sc, 0, 3 * sizeof(int), st), "scn");
+      LAUNCH(k_classify, gW, MR3_THREADS, ncl, c->cl[cur], c->blocks, c->Wsh, c->Wgap, c->cl[nxt],
+             c->sng, c->wt, &c->lc[nxt], c->sc, NN);
+      CK(cudaMemcpyAsync(c->h_lc, &c->lc[nxt], sizeof(LevelCounters), cudaMemcpyDeviceToHost, st), "lcn d2h");
+      CK(cudaMemcpyAsync(c->h_sc, c->sc, sizeof(SngCounters), cudaMemcpyDeviceToHost, st), "sc d2h");
+      CK(cudaStreamSynchronize(st), "level sync");
+      if (c->h_lc->err) { snprintf(c->err, sizeof(c->err), "queue overflow"); return MR3_EMISC; }
+      if (c->h_sc->n_wt > 0)
+        LAUNCH(k_singletons, (int)(nwarps / 8), MR3_THREADS, c->wt, c->sng, c->cl[cur], c->probs,
+               c->blocks, c->RP, c->RQ, c->arena[cur], c->W, c->Wsh, c->Werr, c->Wgap, c->Windex,
+               c->Zindex, c->sc, c->scratch, (long long)nmaxV);
+      ncl = c->h_lc->n_cl;
+      const size_t need = (size_t)c->h_lc->arena_need;
+      if (ncl > 0 && need > c->capArena[nxt]) {
+        CK(cudaStreamSynchronize(st), "arena sync");
+        size_t nsz = std::max(need, c->capArena[nxt] + c->capArena[nxt] / 2);
+        CK(regrow(&c->arena[nxt], nsz), "arena");
+        c->capArena[nxt] = nsz;
+      }
+    }
+  }
+
+  // ---- post-processing (SRC/mrrr.c:262-285)
+  if (anyN) LAUNCH(k_shift_w, gN, 256, NN, c->probs, c->blocks, c->iblk, c->E, c->W);
+  if (anyTry)
+    LAUNCH(k_highrac, gN128, 128, NN, c->probs, c->blocks, c->iblk, c->Windex, c->TPc, c->W,
+           c->Werr);
+  LAUNCH(k_invscale, gN, 256, NN, c->probs, c->blocks, c->iblk, c->W);
+  if (anyV) {
+    LAUNCH(k_place_w, gN, 256, NN, c->probs, c->prob_of_slot, c->W, c->Zindex, c->Wout);
+    CK(cudaMemsetAsync(c->flag, 0, L * sizeof(int), st), "flag");
+    LAUNCH(k_check_sorted, gN, 256, NN, c->probs, c->prob_of_slot, c->Wout, c->flag);
+    CK(cudaMemcpyAsync(c->h_flag, c->flag, L * sizeof(int), cudaMemcpyDeviceToHost, st), "flag d2h");
+    CK(cudaStreamSynchronize(st), "flag sync");
+    bool anyUnsorted = false;
+    for (int k = 0; k < L; k++) anyUnsorted |= (c->h_flag[k] != 0);
+    if (anyUnsorted) {
+      // bubble fix-up of sort_eigenpairs == stable sort by value of the
+      // columns in output order; permute W, Zsupp and the Z columns
+      LAUNCH(k_wkeys, gN, 256, NN, c->probs, c->prob_of_slot, c->Wout, c->rec0, MR3_JOB_V, c->flag);
+      SortRec *sorted = merge_sort(c, st, NN, mmax, MR3_JOB_V, c->flag, &rc);
+      if (rc != MR3_OK) return rc;
+      LAUNCH(k_sorted_to_w, gN, 256, NN, c->probs, c->prob_of_slot, sorted, c->Wout, MR3_JOB_V, c->flag);
+      LAUNCH(k_perm_zsupp, gN, 256, NN, c->probs, c->prob_of_slot, sorted, c->flag, c->tmp2);
+      LAUNCH(k_perm_zsupp2, gN, 256, NN, c->probs, c->prob_of_slot, c->flag, c->tmp2);
+      std::vector<SortRec> hrec(N);
+      CK(cudaMemcpyAsync(hrec.data(), sorted, N * sizeof(SortRec), cudaMemcpyDeviceToHost, st), "perm d2h");
+      CK(cudaMemcpyAsync(c->h_probs, c->probs, L * sizeof(ProbDev), cudaMemcpyDeviceToHost, st), "probs m");
+      CK(cudaStreamSynchronize(st), "perm sync");
+      for (int k = 0; k < L; k++) {
+        if (!c->h_flag[k]) continue;
+        const ProbDev &h = c->h_probs[k];
+        std::vector<int> moved;
+        for (int j = 0; j < h.m; j++)
+          if (hrec[h.off + j].idx != j) moved.push_back(j);
+        if (moved.empty()) continue;
+        double *tmp = nullptr;
+        size_t colsz = (size_t)h.n;
+        CK(cudaMalloc((void **)&tmp, moved.size() * colsz * sizeof(double)), "perm tmp");
+        for (size_t t = 0; t < moved.size(); t++)
+          CK(cudaMemcpyAsync(tmp + t * colsz, h.Z + (size_t)hrec[h.off + moved[t]].idx * h.ldz,
+                             colsz * sizeof(double), cudaMemcpyDeviceToDevice, st), "perm gather");
+        for (size_t t = 0; t < moved.size(); t++)
+          CK(cudaMemcpyAsync(h.Z + (size_t)moved[t] * h.ldz, tmp + t * colsz,
+                             colsz * sizeof(double), cudaMemcpyDeviceToDevice, st), "perm scatter");
+        CK(cudaStreamSynchronize(st), "perm done");
+        cudaFree(tmp);
+      }
+    }
+  }
+  if (anyN) {
+    LAUNCH(k_wkeys, gN, 256, NN, c->probs, c->prob_of_slot, c->W, c->rec0, MR3_JOB_N, nullptr);
+    SortRec *sorted = merge_sort(c, st, NN, mmax, MR3_JOB_N, nullptr, &rc);
+    if (rc != MR3_OK) return rc;
+    LAUNCH(k_sorted_to_w, gN, 256, NN, c->probs, c->prob_of_slot, sorted, c->Wout, MR3_JOB_N, nullptr);
+  }
+  LAUNCH(k_scatter, L, 256, c->probs, c->Wp, c->Dp, c->Ep, c->Wout, c->D, c->E);
+  CK(cudaMemcpyAsync(c->h_probs, c->probs, L * sizeof(ProbDev), cudaMemcpyDeviceToHost, st), "probs d2h");
+  CK(cudaStreamSynchronize(st), "final sync");
+
+  for (int k = 0; k < L; k++) {
+    const ProbDev &h = c->h_probs[k];
+    mr3_cuda_prob &q = pr[idx[k]];
+    q.info = h.status ? MR3_EMISC : MR3_OK;
+    q.m = h.m;
+    q.tryrac_out = h.tryrac_out;
+    // count-only calls return before the bounds are scaled back (SRC/mrrr.c:250-254)
+    const bool unscale = (h.scale != 1.0) && q.jobz != MR3_JOB_C;
+    const double inv = 1.0 / h.scale;
+    q.vl_out = unscale ? h.vl_out * inv : h.vl_out;
+    q.vu_out = unscale ? h.vu_out * inv : h.vu_out;
+    if (q.jobz == MR3_JOB_C) { q.m = h.nvals; q.vl_out = h.vl; q.vu_out = h.vu; }
+    q.il_out = h.il_out;
+    q.iu_out = h.iu_out;
+  }
+  return MR3_OK;
+}

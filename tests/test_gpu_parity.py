@@ -1,0 +1,53 @@
+"""GPU parity: the CUDA path equals the oracle bit for bit (W, Z, Zsupp, the
+overwritten D/E, m, vl, vu, il, iu, tryrac) and agrees with the reference's
+golden vectors within the stated tolerances."""
+import numpy as np
+import pytest
+
+import mr3smp_b200 as M
+import oracle
+from conftest import EPS, assert_same, load_golden, tnorm
+from mr3smp_b200 import workloads as wl
+from zoo import medium_zoo, small_zoo
+
+pytestmark = pytest.mark.gpu
+CASES, GOLD = load_golden()
+
+
+@pytest.mark.parametrize("case", small_zoo(), ids=lambda c: c[0])
+def test_gpu_equals_oracle_small(case):
+    name, D, E, jz, rg, kw = case
+    g = M.mrrr(jz, rg, D, E, **kw)
+    o = oracle.mrrr(jz, rg, D, E, **kw)
+    assert_same(g, o, name)
+    assert M.last_launches() > 0 or jz == "C" or len(D) == 1
+
+
+@pytest.mark.parametrize("case", medium_zoo(), ids=lambda c: c[0])
+def test_gpu_equals_oracle_medium(case):
+    name, D, E, jz, rg, kw = case
+    g = M.mrrr(jz, rg, D, E, **kw)
+    o = oracle.mrrr(jz, rg, D, E, **kw)
+    assert_same(g, o, name)
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
+def test_gpu_matches_reference_golden(case):
+    name = case["name"]
+    D, E, Wref = GOLD[name + "/D"], GOLD[name + "/E"], GOLD[name + "/W"]
+    r = M.mrrr(case["jobz"], case["range"], D, E, **case["kw"])
+    assert r["info"] == 0
+    assert r["m"] == case["m"]
+    n = len(D)
+    assert np.abs(r["W"] - Wref).max() <= 10 * n * EPS * tnorm(D, E)
+    if case["jobz"] == "V":
+        res, orth = wl.residual_orth(D, E, r["W"], r["Z"])
+        bound = max(10.0, case["ref_orth"]) if name.startswith("w21") else 10.0
+        assert res <= 10.0 and orth <= bound, (res, orth)
+
+
+def test_native_library_is_the_one_loaded():
+    D, E = wl.uniform(64, seed=0)
+    M.mrrr("V", "A", D, E)
+    maps = open("/proc/self/maps").read()
+    assert "libmr3b200.so" in maps

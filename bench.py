@@ -1,0 +1,421 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 MRRR solver on the 4096-problem mixed batch.
+
+Workload (per GPU): 4096 independent symmetric tridiagonals, n log-uniform in
+[32, 4096] from a seed, 25 % of them the 1-2-1 matrix, the rest D, E i.i.d.
+uniform(-1, 1); jobz = V, range = A.  One step solves the whole batch.
+
+  value  eigenpairs/s of the batched device pass, inputs already in HBM
+  e2e    the same through the C ABI (mr3_batched) with pinned host buffers:
+         host-to-device copies of D, E and device-to-host copies of W, Z,
+         Zsupp, D, E inside the timed region
+  percall  eigenpairs/s of one mrrr()-style device call per problem (a
+         stratified sample of the batch), and the batched/per-call ratio
+  roofline  the dominant kernel against the measured FP64 division
+         throughput (every Sturm-count step is one IEEE division)
+  cpu_baseline  the reference's own mrrr() (oracle/_ref) on the host cores,
+         PMR_NUM_THREADS = all cores, on a stratified sample of the batch
+
+``--impl reference`` times only the reference CPU implementation, with the
+same metric.  Under torchrun each rank solves its own batch (weak scaling,
+no collective on the data path); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "eigenpairs/s, 4096-problem mixed batch (jobz=V, range=A)"
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _stratified(ns, count):
+    """Indices of `count` problems spread evenly over the batch sorted by n."""
+    order = np.argsort(np.asarray(ns), kind="stable")
+    if count >= len(order):
+        return [int(i) for i in order]
+    pick = np.linspace(0, len(order) - 1, count).round().astype(int)
+    return [int(order[i]) for i in pick]
+
+
+def _clocks_start(device_index):
+    path = tempfile.mktemp(suffix=".csv")
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    try:
+        proc = subprocess.Popen(["nvidia-smi", "-i", str(device_index), f"--query-gpu={q}",
+                                 "--format=csv,noheader,nounits", "-lms", "200"],
+                                stdout=open(path, "w"), stderr=subprocess.DEVNULL)
+    except Exception:
+        return None, path
+    return proc, path
+
+
+def _clocks_stop(proc, path):
+    if proc is None:
+        return None
+    proc.terminate()
+    try:
+        proc.wait(timeout=5)
+    except Exception:
+        proc.kill()
+    sm, mx, reasons = [], 0.0, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in open(path):
+        f = [x.strip() for x in line.split(",")]
+        if len(f) < 9:
+            continue
+        try:
+            sm.append(float(f[1]))
+            mx = max(mx, float(f[2]))
+        except ValueError:
+            continue
+        for nm, v in zip(names, f[5:9]):
+            if v.lower().startswith("active"):
+                reasons.add(nm)
+    if not sm:
+        return None
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------
+# CPU baseline: the reference's own mrrr() on a bounded sample
+# --------------------------------------------------------------------------
+def cpu_reference(problems, budget_s: float, check: bool = True):
+    """Time the reference mrrr() (oracle/_ref) problem by problem on a
+    stratified sample whose predicted cost is about budget_s seconds.
+    Returns (eigenpairs/s, dict)."""
+    import oracle
+    if oracle.ref_lib() is None:
+        return None, {"unavailable": "reference library oracle/_ref not built"}
+    cores = os.cpu_count() or 1
+    os.environ["PMR_NUM_THREADS"] = str(cores)
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    ns = [len(D) for D, E in problems]
+    # calibrate on one mid-size problem
+    mid = _stratified(ns, 9)[6]
+    t0 = time.perf_counter()
+    oracle.ref_mrrr("V", "A", problems[mid][0], problems[mid][1], threads=cores)
+    dt = max(time.perf_counter() - t0, 1e-4)
+    rate = ns[mid] ** 2 / dt                      # n^2 units per second
+    want = budget_s * rate
+    total = float(sum(n * n for n in ns))
+    count = int(max(8, min(len(ns), round(len(ns) * want / total))))
+    sample = _stratified(ns, count)
+    t0 = time.perf_counter()
+    pairs, bad = 0, 0
+    for i in sample:
+        D, E = problems[i]
+        r = oracle.ref_mrrr("V", "A", D, E, threads=cores)
+        pairs += r["m"]
+        if r["info"] != 0 or r["m"] != len(D):
+            bad += 1
+    el = time.perf_counter() - t0
+    # the reference is checked, not trusted (its asserts are compiled out):
+    # residuals of the sampled results, outside the timed region
+    from mr3smp_b200.workloads import residual_orth
+    worst = 0.0
+    for i in (sample[: min(len(sample), 64)] if check else []):
+        D, E = problems[i]
+        r = oracle.ref_mrrr("V", "A", D, E, threads=cores)
+        if len(D) <= 1500:
+            res, orth = residual_orth(D, E, r["W"], r["Z"])
+            worst = max(worst, res, orth)
+            bad += int(res > 10 or orth > 10)
+    info = {"value": pairs / el, "unit": "eigenpairs/s", "cores": cores, "kind": "reference",
+            "sample": f"{len(sample)} of {len(ns)} problems stratified by n "
+                      f"({pairs} eigenpairs, {el:.1f} s), PMR_NUM_THREADS={cores}",
+            "checked_bad": bad, "checked_worst_resid_orth": worst}
+    return pairs / el, info
+
+
+def run_reference(args):
+    ws, rank, local = _dist()
+    if rank != 0:
+        return 0
+    from mr3smp_b200 import workloads as wl
+    probs = [(D, E) for D, E, _ in wl.mixed_batch(args.count, seed=args.seed)]
+    budget = args.ref_step_seconds
+    for _ in range(args.warmup):
+        cpu_reference(probs, budget / 4, check=False)
+    vals = []
+    info = None
+    for _ in range(args.steps):
+        v, info = cpu_reference(probs, budget, check=False)
+        if v is None:
+            print(json.dumps({"impl": "reference", "unavailable": info["unavailable"]}))
+            return 0
+        vals.append(v)
+    value = float(np.mean(vals))
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "eigenpairs/s",
+           "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+           "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "mixed batch: 4096 tridiagonals, n log-uniform [32,4096], "
+                                  "25% 1-2-1, jobz=V range=A", "problems": args.count,
+                      "seed": args.seed},
+           "cpu_baseline": {**info, "value": value},
+           "e2e": {"value": value, "unit": "eigenpairs/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+# --------------------------------------------------------------------------
+# GPU arm
+# --------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--count", type=int, default=4096)
+    ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--percall-sample", type=int, default=128)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--ref-step-seconds", type=float, default=20.0)
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import mr3smp_b200 as M
+    from mr3smp_b200 import workloads as wl
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
+
+    # workload: this rank's batch
+    batch = wl.mixed_batch(args.count, seed=args.seed + rank)
+    problems = [(D, E) for D, E, _ in batch]
+    ns = [len(D) for D, E in problems]
+    pairs_per_step = int(sum(ns))
+    zbytes = 8 * sum(n * n for n in ns)
+
+    S = M.Solver(local)
+    recs, T = M.device_batch(problems)
+    l2_flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB
+    stream = torch.cuda.current_stream()
+
+    def step():
+        T["D"].copy_(T["D0"])
+        T["E"].copy_(T["E0"])
+        S.solve(recs, stream.cuda_stream)
+        l2_flush.fill_(1.0)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    for q in recs:
+        if q.info != 0 or q.m != q.n:
+            raise SystemExit(f"solve failed: info {q.info} m {q.m} n {q.n}")
+
+    # timed region
+    S.profile(True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    cproc, cpath = _clocks_start(local)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+        launches += S.last_launches() + 2   # solver kernels + the two input copies' kernels
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    clocks = _clocks_stop(cproc, cpath)
+    kern, ctr = S.profile_read()
+    S.profile(False)
+    ms_max = ms
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    ms_per_step = ms_max / args.steps
+    value = ws * pairs_per_step / (ms_per_step * 1e-3)
+
+    # roofline: the dominant kernel, algorithmic divisions per second
+    div_gops = fma_tflops = None
+    L = M.lib()
+    L.mr3_cuda_fp64_peaks.restype = __import__("ctypes").c_int
+    import ctypes
+    a, b = ctypes.c_double(), ctypes.c_double()
+    if L.mr3_cuda_fp64_peaks(local, ctypes.byref(a), ctypes.byref(b)) == 0:
+        fma_tflops, div_gops = a.value, b.value
+    groups = M.Solver.KERNEL_GROUPS
+    # kernel -> counter group; divisions per counted unit
+    kmap = {"k_bisect": (0, [1, 0, 0, 0]), "k_refine_root": (1, [0, 1, 0, 0]),
+            "k_cl_ext": (2, [0, 1, 0, 0]), "k_cl_rrf": (2, [0, 0, 0, 1]),
+            "k_refine_cl": (3, [0, 1, 0, 0]), "k_singletons": (4, [0, 1, 2, 0])}
+    top = max(kern.items(), key=lambda kv: kv[1][0])
+    tname, (tms, tcnt) = top
+    roof = None
+    if tname in kmap:
+        g, w = kmap[tname]
+        divs = sum(ctr[g][k] * w[k] for k in range(4))
+        if tname == "k_cl_ext":
+            divs = ctr[2][1]
+        if tname == "k_cl_rrf":
+            divs = ctr[2][3]
+        avg_ms = tms / max(tcnt, 1)
+        per_launch = divs / max(tcnt, 1)
+        achieved = per_launch / (avg_ms * 1e-3) * 1e-9
+        roof = {"bound": "fp64-div", "kernel": tname, "achieved": achieved,
+                "peak": div_gops, "unit": "Gdiv/s",
+                "frac": (achieved / div_gops) if div_gops else None,
+                "peak_source": "measured in-run (independent IEEE double divisions)",
+                "traffic": None, "avg_launch_ms": avg_ms, "launches": tcnt,
+                "algorithmic_divisions_per_launch": per_launch}
+    hbm = peaks.get("hbm_gbs")
+    roof_hbm = {"bound": "hbm", "what": "Z written per step / step time", "achieved":
+                zbytes / (ms_per_step * 1e-3) * 1e-9, "peak": hbm, "unit": "GB/s",
+                "frac": (zbytes / (ms_per_step * 1e-3) * 1e-9 / hbm) if hbm else None,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs" if hbm else None}
+
+    # per-call comparator on a stratified sample (same device, one call each)
+    percall = None
+    if rank == 0 and args.percall_sample > 0:
+        idx = _stratified(ns, args.percall_sample)
+        sub = [problems[i] for i in idx]
+        precs, PT = M.device_batch(sub)
+        single = []
+        for k in range(len(sub)):
+            one = (M.CudaProb * 1)()
+            one[0] = precs[k]
+            single.append(one)
+        for one in single[:4]:
+            S.solve(one, stream.cuda_stream)
+        PT["D"].copy_(PT["D0"])
+        PT["E"].copy_(PT["E0"])
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for one in single:
+            S.solve(one, stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        pms = e0.elapsed_time(e1)
+        spairs = sum(len(D) for D, E in sub)
+        # the same sample as one batched pass
+        PT["D"].copy_(PT["D0"])
+        PT["E"].copy_(PT["E0"])
+        torch.cuda.synchronize()
+        e0.record(stream)
+        S.solve(precs, stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        bms = e0.elapsed_time(e1)
+        percall = {"value": spairs / (pms * 1e-3), "unit": "eigenpairs/s",
+                   "sample": f"{len(sub)} problems stratified by n ({spairs} eigenpairs)",
+                   "sample_batched_value": spairs / (bms * 1e-3),
+                   "batched_over_percall": value / ws / (spairs / (pms * 1e-3))}
+        del PT, precs, single
+
+    # end to end through the C ABI with pinned host buffers
+    e2e = None
+    if rank == 0 and not args.no_e2e:
+        del T, recs
+        torch.cuda.empty_cache()
+        hp = (M.HostProb * len(problems))()
+        keep = []
+        h2d = d2h = 0
+        for k, (D, E) in enumerate(problems):
+            n = len(D)
+            Dh = torch.empty(n, dtype=torch.float64, pin_memory=True)
+            Eh = torch.empty(n, dtype=torch.float64, pin_memory=True)
+            Wh = torch.empty(n, dtype=torch.float64, pin_memory=True)
+            Zh = torch.empty(n * n, dtype=torch.float64, pin_memory=True)
+            Sh = torch.empty(2 * n, dtype=torch.int32, pin_memory=True)
+            keep.append((Dh, Eh, Wh, Zh, Sh, D, E))
+            h = hp[k]
+            h.jobz, h.range, h.n, h.il, h.iu, h.tryrac, h.ldz = b"V", b"A", n, 1, 1, 0, n
+            h.D = ctypes.cast(Dh.data_ptr(), ctypes.POINTER(ctypes.c_double))
+            h.E = ctypes.cast(Eh.data_ptr(), ctypes.POINTER(ctypes.c_double))
+            h.W = ctypes.cast(Wh.data_ptr(), ctypes.POINTER(ctypes.c_double))
+            h.Z = ctypes.cast(Zh.data_ptr(), ctypes.POINTER(ctypes.c_double))
+            h.Zsupp = ctypes.cast(Sh.data_ptr(), ctypes.POINTER(ctypes.c_int))
+            h2d += 16 * n
+            d2h += 8 * n + 8 * n * n + 8 * n + 16 * n
+        def e2e_step():
+            for Dh, Eh, Wh, Zh, Sh, D, E in keep:
+                Dh.numpy()[:] = D
+                Eh.numpy()[:] = E
+            rc = L.mr3_batched(len(problems), hp)
+            if rc != 0:
+                raise SystemExit(f"mr3_batched failed rc={rc}: {M.last_error()}")
+        e2e_step()   # warm-up (allocates the device workspace)
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        el = (time.perf_counter() - t0) / args.e2e_steps
+        e2e = {"value": ws * pairs_per_step / el, "unit": "eigenpairs/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": el * 1e3, "api": "mr3_batched (C ABI), pinned host buffers",
+               "steps": args.e2e_steps}
+        del keep, hp
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        _, cpu = cpu_reference(problems, args.cpu_seconds)
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    out = {
+        "metric": METRIC, "value": value, "unit": "eigenpairs/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded numpy)",
+        "config": {"workload": "mixed batch: 4096 tridiagonals, n log-uniform [32,4096], "
+                               "25% 1-2-1, D,E uniform(-1,1), jobz=V range=A",
+                   "problems_per_gpu": args.count, "seed": args.seed,
+                   "eigenpairs_per_step_per_gpu": pairs_per_step,
+                   "z_bytes_per_step_per_gpu": zbytes,
+                   "l2": "flushed between steps by a 256 MB write; each step also writes "
+                         f"{zbytes / 1e9:.1f} GB of Z"},
+        "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "roofline": roof,
+        "roofline_hbm": roof_hbm, "fp64_peaks": {"fma_tflops": fma_tflops, "div_gops": div_gops},
+        "percall": percall, "cpu_baseline": cpu,
+        "kernels_ms_per_step": {k: v[0] / args.steps for k, v in
+                                sorted(kern.items(), key=lambda kv: -kv[1][0])},
+        "work_counters": dict(zip(groups, ctr)),
+    }
+    print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

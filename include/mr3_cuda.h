@@ -77,6 +77,25 @@ int  mr3_cuda_copy2d(mr3_cuda_ctx *ctx, void *dst, size_t dpitch, const void *sr
                      size_t spitch, size_t width, size_t height, int dir);
 int  mr3_cuda_sync(mr3_cuda_ctx *ctx);
 
+/* Profiling switch: with on = 1 every kernel launch is bracketed by CUDA
+ * events on the solve's stream and the kernels add their work to device
+ * counters; the accumulators are reset by every call of this function. */
+void mr3_cuda_profile(mr3_cuda_ctx *ctx, int on);
+
+/* Accumulated profile: up to `max` kernels (names as 32-byte strings, total
+ * milliseconds, launch counts) and 24 work counters: counters[4*k + kind] for
+ * kernel group k (bisection, root refinement, child representation, cluster
+ * refinement, singletons, other) and kind (0 Sturm steps on T, 1 Sturm steps
+ * on L D L^T, 2 twisted-factorisation rows, 3 dlarrf rows). */
+int  mr3_cuda_profile_read(mr3_cuda_ctx *ctx, int max, char *names, double *ms,
+                           long long *launches, unsigned long long *counters);
+
+/* Measures FP64 fused multiply-add throughput (TFLOP/s, 2 flops per FMA)
+ * and IEEE double division throughput (G divisions/s) on `device` with short
+ * kernels of many independent chains: the roofline denominators of the
+ * division-bound Sturm-count kernels. */
+int  mr3_cuda_fp64_peaks(int device, double *fma_tflops, double *div_gops);
+
 /* Number of kernels launched by the last mr3_cuda_solve on this context. */
 long long mr3_cuda_last_launches(const mr3_cuda_ctx *ctx);
 

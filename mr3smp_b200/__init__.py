@@ -192,3 +192,112 @@ def mrrr_batched_device(problems: list[dict], stream: int | None = None) -> tupl
         q.Zsupp = pb["Zsupp"].data_ptr() if pb.get("Zsupp") is not None else None
     rc = L.mr3_batched_device(P, arr, C.c_void_p(stream) if stream else None)
     return rc, [arr[k] for k in range(P)]
+
+
+class Solver:
+    """A solver context on one device (wraps ``mr3_cuda_ctx``).
+
+    ``solve(probs, stream)`` runs one batched pass over ``CudaProb`` records
+    whose arrays live on the device; ``profile(True)`` turns on per-kernel
+    CUDA-event timing and the device work counters, read back with
+    ``profile_read()``.
+    """
+
+    KERNEL_GROUPS = ("bisect", "refine_root", "newrrr", "refine_cl", "singletons", "other")
+
+    def __init__(self, device: int = 0):
+        L = lib()
+        L.mr3_cuda_ctx_create.restype = C.c_int
+        L.mr3_cuda_ctx_create.argtypes = [C.c_int, C.POINTER(C.c_void_p)]
+        L.mr3_cuda_ctx_destroy.argtypes = [C.c_void_p]
+        L.mr3_cuda_solve.restype = C.c_int
+        L.mr3_cuda_solve.argtypes = [C.c_void_p, C.c_int, C.POINTER(CudaProb), C.c_void_p]
+        L.mr3_cuda_profile.argtypes = [C.c_void_p, C.c_int]
+        L.mr3_cuda_profile_read.restype = C.c_int
+        L.mr3_cuda_profile_read.argtypes = [C.c_void_p, C.c_int, C.c_char_p,
+                                            C.POINTER(C.c_double), C.POINTER(C.c_longlong),
+                                            C.POINTER(C.c_ulonglong)]
+        L.mr3_cuda_last_launches.restype = C.c_longlong
+        L.mr3_cuda_last_launches.argtypes = [C.c_void_p]
+        L.mr3_cuda_last_error.restype = C.c_char_p
+        L.mr3_cuda_last_error.argtypes = [C.c_void_p]
+        self._L = L
+        self._ctx = C.c_void_p()
+        if L.mr3_cuda_ctx_create(int(device), C.byref(self._ctx)) != 0:
+            raise MR3Error("could not create a solver context on device %d" % device)
+
+    def close(self):
+        if self._ctx:
+            self._L.mr3_cuda_ctx_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, probs, stream: int | None = None) -> int:
+        """probs: a ctypes array of CudaProb (device pointers)."""
+        rc = self._L.mr3_cuda_solve(self._ctx, len(probs), probs,
+                                    C.c_void_p(stream) if stream else None)
+        if rc != 0:
+            raise MR3Error("mr3_cuda_solve failed: " + self._L.mr3_cuda_last_error(self._ctx).decode())
+        return rc
+
+    def last_launches(self) -> int:
+        return int(self._L.mr3_cuda_last_launches(self._ctx))
+
+    def profile(self, on: bool):
+        self._L.mr3_cuda_profile(self._ctx, 1 if on else 0)
+
+    def profile_read(self):
+        """-> (dict kernel -> (ms_total, launches), counters[6][4])."""
+        mx = 64
+        names = C.create_string_buffer(32 * mx)
+        ms = (C.c_double * mx)()
+        cnt = (C.c_longlong * mx)()
+        ctr = (C.c_ulonglong * 24)()
+        k = self._L.mr3_cuda_profile_read(self._ctx, mx, names, ms, cnt, ctr)
+        raw = names.raw
+        kern = {}
+        for i in range(k):
+            nm = raw[32 * i: 32 * i + 32].split(b"\0", 1)[0].decode()
+            kern[nm] = (float(ms[i]), int(cnt[i]))
+        counters = [[int(ctr[4 * g + j]) for j in range(4)] for g in range(6)]
+        return kern, counters
+
+
+def device_batch(host_problems, device: str = "cuda", with_z: bool = True):
+    """Lay out a list of (D, E) numpy pairs on the device for batched solves.
+
+    Returns (records, tensors) where ``records`` is a ctypes CudaProb array for
+    jobz V (or N when ``with_z`` is False), range A, and ``tensors`` holds the
+    torch buffers: D0/E0 (pristine inputs), D/E (work copies, overwritten by
+    the solve), W, Z (sum of n^2 doubles, column-major per problem), Zsupp.
+    """
+    import torch
+    ns = [len(D) for D, E in host_problems]
+    offs = np.concatenate([[0], np.cumsum(ns)]).astype(np.int64)
+    N = int(offs[-1])
+    zoffs = np.concatenate([[0], np.cumsum([n * n for n in ns])]).astype(np.int64)
+    D0 = torch.from_numpy(np.concatenate([np.asarray(D, np.float64) for D, E in host_problems])).to(device)
+    E0 = torch.from_numpy(np.concatenate([np.asarray(E, np.float64) for D, E in host_problems])).to(device)
+    D = D0.clone()
+    E = E0.clone()
+    W = torch.zeros(N, dtype=torch.float64, device=device)
+    Z = torch.empty(int(zoffs[-1]) if with_z else 1, dtype=torch.float64, device=device)
+    Zs = torch.zeros(2 * N, dtype=torch.int32, device=device)
+    recs = (CudaProb * len(ns))()
+    for k, n in enumerate(ns):
+        q = recs[k]
+        q.n, q.jobz, q.range = n, (1 if with_z else 0), 1
+        q.il = q.iu = 1
+        q.ldz = n
+        q.D = D.data_ptr() + 8 * int(offs[k])
+        q.E = E.data_ptr() + 8 * int(offs[k])
+        q.W = W.data_ptr() + 8 * int(offs[k])
+        q.Z = (Z.data_ptr() + 8 * int(zoffs[k])) if with_z else None
+        q.Zsupp = (Zs.data_ptr() + 8 * int(offs[k])) if with_z else None
+    tens = dict(D0=D0, E0=E0, D=D, E=E, W=W, Z=Z, Zsupp=Zs, offs=offs, zoffs=zoffs, ns=ns)
+    return recs, tens

@@ -112,7 +112,7 @@ __device__ __noinline__ void dv_ijob3(int n, const double2 *__restrict__ tp, dou
 // counts (na,nb): midpoint bisection of that one interval (odebz.f 90-120).
 __device__ __noinline__ int dv_bisect_one(int n, const double2 *__restrict__ tp, double pivmin,
                                           double abstol, double reltol, int itmax, int j,
-                                          double *a, double *b, int na, int nb) {
+                                          double *a, double *b, int na, int nb, int *iters) {
   double c = 0.5 * (*a + *b);
   for (int it = 1; it <= itmax; it++) {
     int cnt = dv_count_bisect(n, tp, pivmin, c);
@@ -120,14 +120,16 @@ __device__ __noinline__ int dv_bisect_one(int n, const double2 *__restrict__ tp,
     if (j <= cnt) { *b = c; nb = cnt; } else { *a = c; na = cnt; }
     double w = fabs(*b - *a);
     double t = fmax(fabs(*b), fabs(*a));
+    *iters = it;
     if (w < fmax(fmax(abstol, pivmin), reltol * t) || na >= nb) return 1;
     c = 0.5 * (*a + *b);
   }
   return 0;
 }
 
-// dlaneg (SRC/LAPACK/odneg.f:98-163) on packed rows P; r is 1-based.
-__device__ __noinline__ int dv_dlaneg(int n, const double2 *__restrict__ P, double sigma, int r) {
+// dlaneg (SRC/LAPACK/odneg.f:98-163) on packed rows P[(i)*ps]; r is 1-based.
+__device__ __noinline__ int dv_dlaneg(int n, const double2 *__restrict__ P, int ps, double sigma,
+                                      int r) {
   const int blklen = 128;
   int negcnt = 0;
   double t = -sigma;
@@ -136,7 +138,7 @@ __device__ __noinline__ int dv_dlaneg(int n, const double2 *__restrict__ P, doub
     int neg1 = 0;
     double bsav = t;
     for (int j = bj; j <= jend; j++) {
-      const double2 v = P[j - 1];
+      const double2 v = P[(size_t)(j - 1) * ps];
       double dplus = v.x + t;
       neg1 += (dplus < 0.0);
       double tmp = t / dplus;
@@ -146,7 +148,7 @@ __device__ __noinline__ int dv_dlaneg(int n, const double2 *__restrict__ P, doub
       neg1 = 0;
       t = bsav;
       for (int j = bj; j <= jend; j++) {
-        const double2 v = P[j - 1];
+        const double2 v = P[(size_t)(j - 1) * ps];
         double dplus = v.x + t;
         neg1 += (dplus < 0.0);
         double tmp = t / dplus;
@@ -156,13 +158,13 @@ __device__ __noinline__ int dv_dlaneg(int n, const double2 *__restrict__ P, doub
     }
     negcnt += neg1;
   }
-  double p = P[n - 1].x - sigma;
+  double p = P[(size_t)(n - 1) * ps].x - sigma;
   for (int bj = n - 1; bj >= r; bj -= blklen) {
     int jend = d_imax(bj - blklen + 1, r);
     int neg2 = 0;
     double bsav = p;
     for (int j = bj; j >= jend; j--) {
-      const double2 v = P[j - 1];
+      const double2 v = P[(size_t)(j - 1) * ps];
       double dminus = v.y + p;
       neg2 += (dminus < 0.0);
       double tmp = p / dminus;
@@ -172,7 +174,7 @@ __device__ __noinline__ int dv_dlaneg(int n, const double2 *__restrict__ P, doub
       neg2 = 0;
       p = bsav;
       for (int j = bj; j >= jend; j--) {
-        const double2 v = P[j - 1];
+        const double2 v = P[(size_t)(j - 1) * ps];
         double dminus = v.y + p;
         neg2 += (dminus < 0.0);
         double tmp = p / dminus;
@@ -196,26 +198,32 @@ __device__ __noinline__ int dv_dlaneg(int n, const double2 *__restrict__ P, doub
 //   has_left: II > 1 (main-loop left gap is WGAP(II-1))
 //   w, werr: in/out; updated only if the interval went through the main loop
 // Returns the number of counts spent, or -1 if a widening loop hit its cap.
-__device__ __noinline__ int dv_dlarrb_one(int n, const double2 *__restrict__ R, int i, int first,
+__device__ __noinline__ int dv_dlarrb_one(int n, const double2 *__restrict__ R, int ps, int i,
+                                          int first,
                                           int has_left, double rgap_own, double lgap_in,
                                           double rtol1, double rtol2, double pivmin,
-                                          int maxitr, int r, double *w, double *werr) {
+                                          int maxitr, int r, double *w, double *werr,
+                                          int *ncount) {
   double mnwdth = 2.0 * pivmin;
   double left = *w - *werr, right = *w + *werr;
   double gap = fmin(first ? rgap_own : lgap_in, rgap_own);
   double back = *werr;
   int negcnt, cap, status = 0;
+  int nc = 0;
   for (cap = 0; cap < MR3_EXPAND_CAP; cap++) {
-    negcnt = dv_dlaneg(n, R, left, r);
+    negcnt = dv_dlaneg(n, R, ps, left, r);
+    nc++;
     if (negcnt > i - 1) { left = left - back; back = 2.0 * back; } else break;
   }
   if (cap == MR3_EXPAND_CAP) status = -1;
   back = *werr;
   for (cap = 0; cap < MR3_EXPAND_CAP; cap++) {
-    negcnt = dv_dlaneg(n, R, right, r);
+    negcnt = dv_dlaneg(n, R, ps, right, r);
+    nc++;
     if (negcnt < i) { right = right + back; back = 2.0 * back; } else break;
   }
   if (cap == MR3_EXPAND_CAP) status = -1;
+  *ncount += nc;
   double width = 0.5 * fabs(left - right);
   double tmp = fmax(fabs(left), fabs(right));
   double cvrgd = fmax(rtol1 * gap, rtol2 * tmp);
@@ -227,7 +235,8 @@ __device__ __noinline__ int dv_dlarrb_one(int n, const double2 *__restrict__ R, 
     tmp = fmax(fabs(left), fabs(right));
     cvrgd = fmax(rtol1 * gap, rtol2 * tmp);
     if (width <= cvrgd || width <= mnwdth || iter == maxitr) break;
-    negcnt = dv_dlaneg(n, R, mid, r);
+    negcnt = dv_dlaneg(n, R, ps, mid, r);
+    *ncount += 1;
     if (negcnt <= i - 1) left = mid; else right = mid;
   }
   *w = 0.5 * (left + right);
@@ -249,16 +258,26 @@ __device__ __forceinline__ double dv_lcg_uniform(uint64_t seed, uint64_t k) {
   return 2.0 * ((double)s * 3.5527136788005009e-15) - 1.0;   // 2^-48
 }
 
-// dlar1v (SRC/LAPACK/odr1v.f:158-362) with B1 = 1, BN = n, on one thread.
-// Scratch: two per-thread arrays addressed X[i*stride], Y[i*stride], i < n.
-//   pass A (stationary)  : X[i] = LPLUS(i), Y[i] = S(i)
-//   pass B (progressive) : Y[i] = UMINUS(i) once S(i) is no longer needed; the
-//                          twist search runs inside this pass, from the top
-//                          index down with a strict '<', which selects the same
-//                          index as the Fortran's upward scan with '<='.
-//   solve                : z(k) for k < r in X[k], z(r) = 1, z(k) for k > r in
-//                          Y[k-1]; read back with dv_zget().
-// r is in/out: 0 on input means "search the twist index over 1..n".
+// Prefetch the L1 line holding *p (PTX prefetch.global.L1).  Only issued for
+// addresses inside the arrays being read.
+__device__ __forceinline__ void pf_l1(const void *p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
+#define MR3_PF 16   // prefetch distance in rows
+
+// dlar1v (SRC/LAPACK/odr1v.f:158-362) with B1 = 1, BN = n.  Each lane of a
+// warp runs its own eigenvector; the three sweeps (stationary transform,
+// progressive transform, back-substitution) run over the rows in lock-step
+// so every per-lane scratch access is one coalesced 256-byte row.
+// Scratch per lane: X[i*stride], Y[i*stride], i < n.
+//   stationary  : X[i] = LPLUS(i), Y[i] = S(i)
+//   progressive : Y[i] = UMINUS(i) once S(i) has been used; the twist search
+//                 runs inside this sweep from the top index down with a strict
+//                 '<', which selects the same index as the Fortran's upward
+//                 scan with '<='
+//   solve       : z(k) for k < r in X[k], z(r) = 1, z(k) for k > r in Y[k-1]
+// r_in = 0 means "search the twist index over 1..n".
 struct dlar1v_out {
   int negcnt, r, isupp1, isupp2;
   double ztz, mingma, nrminv, resid, rqcorr;
@@ -271,42 +290,32 @@ __device__ __forceinline__ double dv_zget(const double *X, const double *Y, int 
 }
 
 __device__ __noinline__ bool dv_r1v_passA(int n, double lambda, const double2 *__restrict__ P,
-                                          const double2 *__restrict__ Q, double pivmin, int r1,
+                                          const double2 *__restrict__ Q, int ps, double pivmin, int r1,
                                           int r2, double *X, double *Y, int stride, int *neg1o) {
   int neg1 = 0;
   double s = 0.0 - lambda;
   Y[0] = 0.0;
-  for (int i = 1; i <= r1 - 1; i++) {
-    const double dd = P[i - 1].x;
-    const double2 q = Q[i - 1];
+  bool sawnan = false;
+  for (int i = 1; i <= r2 - 1; i++) {
+    if (i + MR3_PF <= n - 1) { pf_l1(&P[(size_t)(i + MR3_PF - 1) * ps]); pf_l1(&Q[(size_t)(i + MR3_PF - 1) * ps]); }
+    const double dd = P[(size_t)(i - 1) * ps].x;
+    const double2 q = Q[(size_t)(i - 1) * ps];
     double dplus = dd + s;
     double lp = q.y / dplus;
     X[(size_t)i * stride] = lp;
-    neg1 += (dplus < 0.0);
+    if (i <= r1 - 1) neg1 += (dplus < 0.0);
     double si = s * lp * q.x;
     Y[(size_t)i * stride] = si;
     s = si - lambda;
+    if (i == r1 - 1 && isnan(s)) { sawnan = true; break; }
   }
-  bool sawnan = isnan(s);
-  if (!sawnan) {
-    for (int i = r1; i <= r2 - 1; i++) {
-      const double dd = P[i - 1].x;
-      const double2 q = Q[i - 1];
-      double dplus = dd + s;
-      double lp = q.y / dplus;
-      X[(size_t)i * stride] = lp;
-      double si = s * lp * q.x;
-      Y[(size_t)i * stride] = si;
-      s = si - lambda;
-    }
-    sawnan = isnan(s);
-  }
+  if (!sawnan) sawnan = isnan(s);
   if (sawnan) {
     neg1 = 0;
     s = 0.0 - lambda;
     for (int i = 1; i <= r2 - 1; i++) {
-      const double2 pp = P[i - 1];
-      const double2 q = Q[i - 1];
+      const double2 pp = P[(size_t)(i - 1) * ps];
+      const double2 q = Q[(size_t)(i - 1) * ps];
       double dplus = pp.x + s;
       if (fabs(dplus) < pivmin) dplus = -pivmin;
       double lp = q.y / dplus;
@@ -324,12 +333,12 @@ __device__ __noinline__ bool dv_r1v_passA(int n, double lambda, const double2 *_
 
 // Progressive transform with the fused twist search.  Returns P(R1-1).
 __device__ __noinline__ double dv_r1v_passB(int n, double lambda, const double2 *__restrict__ P,
-                                            const double2 *__restrict__ Q, double pivmin, int r1,
+                                            const double2 *__restrict__ Q, int ps, double pivmin, int r1,
                                             int r2, bool slow, double *Y, int stride, int *neg2o,
                                             int *rbest, double *best, bool *have) {
   const double eps = MR3_EPS;
   int neg2 = 0;
-  double p = P[n - 1].x - lambda;   // P(n-1)
+  double p = P[(size_t)(n - 1) * ps].x - lambda;   // P(n-1)
   *have = false;
   if (r2 == n && n > r1) {          // candidate r = n
     double s = Y[(size_t)(n - 1) * stride];
@@ -338,8 +347,14 @@ __device__ __noinline__ double dv_r1v_passB(int n, double lambda, const double2 
     *best = c; *rbest = n; *have = true;
   }
   for (int i = n - 1; i >= r1; i--) {
-    const double2 pp = P[i - 1];
-    const double2 q = Q[i - 1];
+    if (i - MR3_PF >= 1) {
+      pf_l1(&P[(size_t)(i - MR3_PF - 1) * ps]);
+      pf_l1(&Q[(size_t)(i - MR3_PF - 1) * ps]);
+      pf_l1(&Y[(size_t)(i - MR3_PF - 1) * stride]);
+    }
+    const double2 pp = P[(size_t)(i - 1) * ps];
+    const double2 q = Q[(size_t)(i - 1) * ps];
+    const double sprev = Y[(size_t)(i - 1) * stride];
     double dminus = pp.y + p;
     if (slow && fabs(dminus) < pivmin) dminus = -pivmin;
     double tmp = pp.x / dminus;
@@ -350,9 +365,8 @@ __device__ __noinline__ double dv_r1v_passB(int n, double lambda, const double2 
     Y[(size_t)i * stride] = um;
     p = pn;
     if (i > r1 && i <= r2) {        // candidate r = i: S(i-1) + P(i-1)
-      double s = Y[(size_t)(i - 1) * stride];
-      double c = s + p;
-      if (c == 0.0) c = eps * s;
+      double c = sprev + p;
+      if (c == 0.0) c = eps * sprev;
       if (!*have || fabs(c) < fabs(*best)) { *best = c; *rbest = i; *have = true; }
     }
   }
@@ -360,90 +374,127 @@ __device__ __noinline__ double dv_r1v_passB(int n, double lambda, const double2 
   return p;
 }
 
-__device__ __noinline__ void dv_dlar1v(int n, double lambda, const double2 *__restrict__ P,
-                                       const double2 *__restrict__ Q, double pivmin,
-                                       double gaptol, bool wantnc, int r_in, double *X, double *Y,
-                                       int stride, dlar1v_out *o) {
+// The two factorisation sweeps and the twist choice of dlar1v.  Leaves the
+// lane's state for dv_r1v_solve.
+struct r1v_state {
+  int r;
+  double mingma;
+  bool sawnan;
+};
+
+__device__ __noinline__ void dv_r1v_factor(int n, double lambda, const double2 *__restrict__ P,
+                                           const double2 *__restrict__ Q, int ps, double pivmin,
+                                           bool wantnc, int r_in, double *X, double *Y,
+                                           int stride, int *negcnt, r1v_state *st) {
   const double eps = MR3_EPS;
   int r1, r2, neg1, neg2, rbest = 0;
   if (r_in == 0) { r1 = 1; r2 = n; } else { r1 = r_in; r2 = r_in; }
-  bool sawnan1 = dv_r1v_passA(n, lambda, P, Q, pivmin, r1, r2, X, Y, stride, &neg1);
+  bool sawnan1 = dv_r1v_passA(n, lambda, P, Q, ps, pivmin, r1, r2, X, Y, stride, &neg1);
   double best = 0.0;
   bool have;
-  double pr1 = dv_r1v_passB(n, lambda, P, Q, pivmin, r1, r2, false, Y, stride, &neg2, &rbest,
+  double pr1 = dv_r1v_passB(n, lambda, P, Q, ps, pivmin, r1, r2, false, Y, stride, &neg2, &rbest,
                             &best, &have);
   bool sawnan2 = isnan(pr1);
   if (sawnan2) {
-    // S was overwritten by UMINUS; recompute pass A (same bits), then the slow pass B.
-    dv_r1v_passA(n, lambda, P, Q, pivmin, r1, r2, X, Y, stride, &neg1);
-    pr1 = dv_r1v_passB(n, lambda, P, Q, pivmin, r1, r2, true, Y, stride, &neg2, &rbest, &best,
+    // S was overwritten by UMINUS; recompute the stationary sweep (same bits)
+    // and run the slow progressive sweep
+    dv_r1v_passA(n, lambda, P, Q, ps, pivmin, r1, r2, X, Y, stride, &neg1);
+    pr1 = dv_r1v_passB(n, lambda, P, Q, ps, pivmin, r1, r2, true, Y, stride, &neg2, &rbest, &best,
                        &have);
   }
   double sr1 = Y[(size_t)(r1 - 1) * stride];
   double mg = sr1 + pr1;
   if (mg < 0.0) neg1++;
-  o->negcnt = wantnc ? neg1 + neg2 : -1;
+  *negcnt = wantnc ? neg1 + neg2 : -1;
   if (fabs(mg) == 0.0) mg = eps * sr1;
   int r = r1;
   if (have && fabs(best) <= fabs(mg)) { mg = best; r = rbest; }
-  o->mingma = mg;
-  o->r = r;
+  st->mingma = mg;
+  st->r = r;
+  st->sawnan = sawnan1 || sawnan2;
+}
 
+// Back-substitution N^T z = e_r of dlar1v (odr1v.f:285-355) for a whole warp
+// in lock-step: rows are visited from the largest twist index down (upward
+// solve) and then from the smallest up (downward solve); a lane works on the
+// rows where it is active.  `active` says whether this lane has a solve to do.
+// Writes z over X/Y as described above and returns the outputs.
+__device__ __noinline__ void dv_r1v_solve(bool active, int n, const double2 *__restrict__ Q, int ps,
+                                          double gaptol, double *X, double *Y, int stride,
+                                          const r1v_state &st, dlar1v_out *o) {
+  const int r = active ? st.r : 0;
+  const int rmax = __reduce_max_sync(0xffffffffu, active ? r : 0);
+  int rmin = __reduce_min_sync(0xffffffffu, active ? r : 0x7fffffff);
   int is1 = 1, is2 = n;
   double ztz = 1.0;
-  if (!sawnan1 && !sawnan2) {
-    double zp = 1.0;
-    for (int i = r - 1; i >= 1; i--) {
-      double zi = -(X[(size_t)i * stride] * zp);
-      if ((fabs(zi) + fabs(zp)) * fabs(Q[i - 1].y) < gaptol) {
-        X[(size_t)i * stride] = 0.0; is1 = i + 1; break;
-      }
-      ztz = ztz + zi * zi;
-      X[(size_t)i * stride] = zi;
-      zp = zi;
-    }
-    double zc = 1.0;
-    for (int i = r; i <= n - 1; i++) {
-      double zn = -(Y[(size_t)i * stride] * zc);
-      if ((fabs(zc) + fabs(zn)) * fabs(Q[i - 1].y) < gaptol) {
-        Y[(size_t)i * stride] = 0.0; is2 = i; break;
-      }
-      ztz = ztz + zn * zn;
-      Y[(size_t)i * stride] = zn;
-      zc = zn;
-    }
-  } else {
-    for (int i = r - 1; i >= 1; i--) {
-      double zi1 = dv_zget(X, Y, stride, r, i + 1);
+  const bool slow = active && st.sawnan;
+  // upward solve: i = r-1 .. 1
+  bool go = active;
+  double zp = 1.0;
+  for (int i = rmax - 1; i >= 1; i--) {
+    if (!__any_sync(0xffffffffu, go)) break;
+    if (i - MR3_PF >= 1) pf_l1(&X[(size_t)(i - MR3_PF) * stride]);
+    if (go && i < r) {
       double zi;
-      if (zi1 == 0.0) zi = -(Q[i].y / Q[i - 1].y) * dv_zget(X, Y, stride, r, i + 2);
-      else zi = -(X[(size_t)i * stride] * zi1);
-      if ((fabs(zi) + fabs(zi1)) * fabs(Q[i - 1].y) < gaptol) {
-        X[(size_t)i * stride] = 0.0; is1 = i + 1; break;
+      if (!slow) {
+        zi = -(X[(size_t)i * stride] * zp);
+      } else {
+        double zi1 = dv_zget(X, Y, stride, r, i + 1);
+        if (zi1 == 0.0) zi = -(Q[(size_t)i * ps].y / Q[(size_t)(i - 1) * ps].y) * dv_zget(X, Y, stride, r, i + 2);
+        else zi = -(X[(size_t)i * stride] * zi1);
+        zp = zi1;
       }
-      ztz = ztz + zi * zi;
-      X[(size_t)i * stride] = zi;
-    }
-    for (int i = r; i <= n - 1; i++) {
-      double zc = dv_zget(X, Y, stride, r, i);
-      double zn;
-      if (zc == 0.0) zn = -(Q[i - 2].y / Q[i - 1].y) * dv_zget(X, Y, stride, r, i - 1);
-      else zn = -(Y[(size_t)i * stride] * zc);
-      if ((fabs(zc) + fabs(zn)) * fabs(Q[i - 1].y) < gaptol) {
-        Y[(size_t)i * stride] = 0.0; is2 = i; break;
+      if ((fabs(zi) + fabs(zp)) * fabs(Q[(size_t)(i - 1) * ps].y) < gaptol) {
+        X[(size_t)i * stride] = 0.0;
+        is1 = i + 1;
+        go = false;
+      } else {
+        ztz = ztz + zi * zi;
+        X[(size_t)i * stride] = zi;
+        zp = zi;
       }
-      ztz = ztz + zn * zn;
-      Y[(size_t)i * stride] = zn;
     }
   }
-  o->isupp1 = is1;
-  o->isupp2 = is2;
-  o->ztz = ztz;
-  double tmp = 1.0 / ztz;
-  o->nrminv = sqrt(tmp);
-  o->resid = fabs(o->mingma) * o->nrminv;
-  o->rqcorr = o->mingma * tmp;
-  o->sawnan = sawnan1 || sawnan2;
+  // downward solve: i = r .. n-1
+  go = active;
+  double zc = 1.0;
+  if (rmin == 0x7fffffff) rmin = n;
+  for (int i = rmin; i <= n - 1; i++) {
+    if (!__any_sync(0xffffffffu, go)) break;
+    if (i + MR3_PF <= n - 1) pf_l1(&Y[(size_t)(i + MR3_PF) * stride]);
+    if (go && i >= r) {
+      double zn;
+      if (!slow) {
+        zn = -(Y[(size_t)i * stride] * zc);
+      } else {
+        double zci = dv_zget(X, Y, stride, r, i);
+        if (zci == 0.0) zn = -(Q[(size_t)(i - 2) * ps].y / Q[(size_t)(i - 1) * ps].y) * dv_zget(X, Y, stride, r, i - 1);
+        else zn = -(Y[(size_t)i * stride] * zci);
+        zc = zci;
+      }
+      if ((fabs(zc) + fabs(zn)) * fabs(Q[(size_t)(i - 1) * ps].y) < gaptol) {
+        Y[(size_t)i * stride] = 0.0;
+        is2 = i;
+        go = false;
+      } else {
+        ztz = ztz + zn * zn;
+        Y[(size_t)i * stride] = zn;
+        zc = zn;
+      }
+    }
+  }
+  if (active) {
+    o->r = r;
+    o->mingma = st.mingma;
+    o->isupp1 = is1;
+    o->isupp2 = is2;
+    o->ztz = ztz;
+    double tmp = 1.0 / ztz;
+    o->nrminv = sqrt(tmp);
+    o->resid = fabs(o->mingma) * o->nrminv;
+    o->rqcorr = o->mingma * tmp;
+    o->sawnan = st.sawnan;
+  }
 }
 
 // dlarrf, LAPACK 3.2.2 with NOFAIL (SRC/LAPACK/odrrf.f:140-378), one thread.
@@ -451,11 +502,14 @@ __device__ __noinline__ void dv_dlar1v(int n, double lambda, const double2 *__re
 // cluster's first eigenvalue (CLSTRT = 1, CLEND = clend).  dplus, lplus: out;
 // work: 2n scratch.  Returns the shift sigma.
 __device__ __noinline__ double dv_dlarrf(int n, const double2 *__restrict__ P,
-                                         const double2 *__restrict__ Q, int clend,
+                                         const double2 *__restrict__ Q, int ps, int clend,
                                          const double *w, const double *wgap, const double *werr,
                                          double spdiam, double clgapl, double clgapr,
-                                         double pivmin, double *dplus, double *lplus,
-                                         double *work) {
+                                         double pivmin, double *dp_, double *lp_, double *wk_,
+                                         int os) {
+#define dplus(i) dp_[(size_t)(i) * os]
+#define lplus(i) lp_[(size_t)(i) * os]
+#define work(i) wk_[(size_t)(i) * os]
   const double maxgrowth1 = 8.0, maxgrowth2 = 8.0, eps = MR3_EPS, fact = 2.0;
   const int ktrymax = 1;
   int shift = 0, indx = 0, ktry = 0;
@@ -483,32 +537,32 @@ __device__ __noinline__ double dv_dlarrf(int n, const double2 *__restrict__ P,
     ldelta = fmin(ldmax, ldelta);
     rdelta = fmin(rdmax, rdelta);
     double s = -lsigma;
-    dplus[0] = P[0].x + s;
-    if (fabs(dplus[0]) < pivmin) { dplus[0] = -pivmin; sawnan1 = true; }
-    max1 = fabs(dplus[0]);
+    dplus(0) = P[0].x + s;
+    if (fabs(dplus(0)) < pivmin) { dplus(0) = -pivmin; sawnan1 = true; }
+    max1 = fabs(dplus(0));
     for (int i = 0; i < n - 1; i++) {
-      const double2 q = Q[i];
-      lplus[i] = q.y / dplus[i];
-      s = s * lplus[i] * q.x - lsigma;
-      double dp = P[i + 1].x + s;
+      const double2 q = Q[(size_t)i * ps];
+      lplus(i) = q.y / dplus(i);
+      s = s * lplus(i) * q.x - lsigma;
+      double dp = P[(size_t)(i + 1) * ps].x + s;
       if (fabs(dp) < pivmin) { dp = -pivmin; sawnan1 = true; }
-      dplus[i + 1] = dp;
+      dplus(i + 1) = dp;
       max1 = fmax(max1, fabs(dp));
     }
     sawnan1 = sawnan1 || isnan(max1);
     if (forcer || (max1 <= growthbound && !sawnan1)) { sigma = lsigma; shift = 1; break; }
 
     s = -rsigma;
-    work[0] = P[0].x + s;
-    if (fabs(work[0]) < pivmin) { work[0] = -pivmin; sawnan2 = true; }
-    max2 = fabs(work[0]);
+    work(0) = P[0].x + s;
+    if (fabs(work(0)) < pivmin) { work(0) = -pivmin; sawnan2 = true; }
+    max2 = fabs(work(0));
     for (int i = 0; i < n - 1; i++) {
-      const double2 q = Q[i];
-      work[n + i] = q.y / work[i];
-      s = s * work[n + i] * q.x - rsigma;
-      double dp = P[i + 1].x + s;
+      const double2 q = Q[(size_t)i * ps];
+      work(n + i) = q.y / work(i);
+      s = s * work(n + i) * q.x - rsigma;
+      double dp = P[(size_t)(i + 1) * ps].x + s;
       if (fabs(dp) < pivmin) { dp = -pivmin; sawnan2 = true; }
-      work[i + 1] = dp;
+      work(i + 1) = dp;
       max2 = fmax(max2, fabs(dp));
     }
     sawnan2 = sawnan2 || isnan(max2);
@@ -527,28 +581,28 @@ __device__ __noinline__ double dv_dlarrf(int n, const double2 *__restrict__ P,
                     !sawnan2;
       if (dorrr1) {
         if (indx == 1) {
-          double tmp = fabs(dplus[n - 1]), znm2 = 1.0, prod = 1.0, oldp = 1.0;
+          double tmp = fabs(dplus(n - 1)), znm2 = 1.0, prod = 1.0, oldp = 1.0;
           for (int i = n - 1; i >= 1; i--) {
             if (prod <= eps)
-              prod = ((dplus[i] * work[n + i]) / (dplus[i - 1] * work[n + i - 1])) * oldp;
+              prod = ((dplus(i) * work(n + i)) / (dplus(i - 1) * work(n + i - 1))) * oldp;
             else
-              prod = prod * fabs(work[n + i - 1]);
+              prod = prod * fabs(work(n + i - 1));
             oldp = prod;
             znm2 = znm2 + prod * prod;
-            tmp = fmax(tmp, fabs(dplus[i - 1] * prod));
+            tmp = fmax(tmp, fabs(dplus(i - 1) * prod));
           }
           double rrr1 = tmp / (spdiam * sqrt(znm2));
           if (rrr1 <= maxgrowth2) { sigma = lsigma; shift = 1; break; }
         } else if (indx == 2) {
-          double tmp = fabs(work[n - 1]), znm2 = 1.0, prod = 1.0, oldp = 1.0;
+          double tmp = fabs(work(n - 1)), znm2 = 1.0, prod = 1.0, oldp = 1.0;
           for (int i = n - 1; i >= 1; i--) {
             if (prod <= eps)
-              prod = ((work[i] * lplus[i]) / (work[i - 1] * lplus[i - 1])) * oldp;
+              prod = ((work(i) * lplus(i)) / (work(i - 1) * lplus(i - 1))) * oldp;
             else
-              prod = prod * fabs(lplus[i - 1]);
+              prod = prod * fabs(lplus(i - 1));
             oldp = prod;
             znm2 = znm2 + prod * prod;
-            tmp = fmax(tmp, fabs(work[i - 1] * prod));
+            tmp = fmax(tmp, fabs(work(i - 1) * prod));
           }
           double rrr2 = tmp / (spdiam * sqrt(znm2));
           if (rrr2 <= maxgrowth2) { sigma = rsigma; shift = 2; break; }
@@ -569,10 +623,13 @@ __device__ __noinline__ double dv_dlarrf(int n, const double2 *__restrict__ P,
     forcer = true;
   }
   if (shift == 2) {
-    for (int i = 0; i < n; i++) dplus[i] = work[i];
-    for (int i = 0; i < n - 1; i++) lplus[i] = work[n + i];
+    for (int i = 0; i < n; i++) dplus(i) = work(i);
+    for (int i = 0; i < n - 1; i++) lplus(i) = work(n + i);
   }
   return sigma;
+#undef dplus
+#undef lplus
+#undef work
 }
 
 // One interval of dlarrj (SRC/LAPACK/odrrj.f:100-281): bisection on T to

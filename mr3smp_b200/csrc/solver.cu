@@ -22,6 +22,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <string>
 #include <vector>
 
 #include "mr3_cuda.h"
@@ -53,12 +54,20 @@ struct BlockDev {
   double sigma, spdiam, bl_spdiam;
 };
 
+// A cluster of one level.  Sibling clusters (children of one parent, hence
+// of one block) are stored in groups of up to 32 whose representations are
+// interleaved row by row in the level's arena: row i of member g of a group
+// with G members sits at index i*G + g of each field.  Group layout, in
+// doubles from the group's base: P (2*nb*G), Q (2*nb*G), dplus (nb*G),
+// lplus (nb*G), dlarrf work (2*nb*G): 8*nb*G doubles in all.
 struct ClusterDev {
   int begin, end, depth, blk;   // W slots (global), depth, block
   double bl_spdiam, lgap;
-  long long par_off;            // -1: parent is the block's root; else offset in previous arena
-  long long own_off;            // this cluster's slot in the current arena (depth >= 1)
-  double par_sigma, sigma;
+  long long par_off;            // -1: parent is the block's root; else parent group's base
+  int pG, pg;                   // parent's group size and position
+  long long grp_off;            // this cluster's group base in the current arena (depth >= 1)
+  int G, g;                     // group size and position
+  double par_sigma, sigma, tau;
 };
 
 struct SngDev {
@@ -124,6 +133,17 @@ __device__ int cta_exscan(int v, int *sh, int *total) {
 }
 
 __device__ __forceinline__ void set_status(ProbDev *p, int s) { atomicMax(&p->status, s); }
+
+// Device work counters for the roofline: stats[kernel * 4 + kind], kinds
+// 0 = Sturm-count steps on T, 1 = Sturm-count steps on L D L^T (dlaneg),
+// 2 = twisted-factorisation rows (dlar1v), 3 = dlarrf rows.  Every lane of a
+// warp must call stat_add (it reduces over the full warp).
+enum { KID_BISECT = 0, KID_REFROOT, KID_NEWRRR, KID_REFCL, KID_SNG, KID_OTHER, KID_COUNT };
+__device__ __forceinline__ void stat_add(unsigned long long *stats, int slot, unsigned long long v) {
+  if (stats == nullptr) return;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(&stats[slot], v);
+}
 
 // ------------------------------------------------------------------------
 // Stage A0: per-problem prologue (SRC/mrrr.c:206-243, SRC/mrrr_val.c:167-329)
@@ -462,23 +482,33 @@ k_blocks(ProbDev *probs, BlockDev *blocks, const double *D, double *E, const dou
 // (dlarrd/dlaebz IJOB=2, SRC/LAPACK/odrrd.f:450-520).  Thread k of a block
 // bisects eigenvalue nab1+1+k; a block never has more than nbl of them.
 // ------------------------------------------------------------------------
-__global__ void __launch_bounds__(128)
-k_bisect(int N, const ProbDev *probs, const BlockDev *blocks, const int *blk_of_row,
-         const double2 *TP, double *Wt, double *Et, int *It, Tol tol) {
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= N) return;
+__device__ __forceinline__ unsigned long long bisect_body(int g, const ProbDev *probs,
+                                                          const BlockDev *blocks,
+                                                          const int *blk_of_row, const double2 *TP,
+                                                          double *Wt, double *Et, int *It, Tol tol) {
   const BlockDev *B = &blocks[blk_of_row[g]];
   const ProbDev *p = &probs[B->prob];
-  if (p->trivial || p->jobz == MR3_JOB_C || p->status) return;
+  if (p->trivial || p->jobz == MR3_JOB_C || p->status) return 0;
   int k = g - B->ibgn;
-  if (B->nbl < 2 || B->mbl <= 0 || B->none || k >= B->nab2 - B->nab1) return;
+  if (B->nbl < 2 || B->mbl <= 0 || B->none || k >= B->nab2 - B->nab1) return 0;
   int j = B->nab1 + 1 + k;
   double a = B->gl3, b = B->gu3;
+  int it = 0;
   dv_bisect_one(B->nbl, TP + B->ibgn, p->pivmin, B->atoli, tol.bsrtol, B->itmax2, j, &a, &b,
-                B->nab1, B->nab2);
+                B->nab1, B->nab2, &it);
   Wt[g] = 0.5 * (a + b);
   Et[g] = 0.5 * fabs(a - b);
   It[g] = j;
+  return (unsigned long long)it * (unsigned long long)B->nbl;
+}
+
+__global__ void __launch_bounds__(128)
+k_bisect(int N, const ProbDev *probs, const BlockDev *blocks, const int *blk_of_row,
+         const double2 *TP, double *Wt, double *Et, int *It, Tol tol, unsigned long long *stats) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long work = 0;
+  if (g < N) work = bisect_body(g, probs, blocks, blk_of_row, TP, Wt, Et, It, tol);
+  stat_add(stats, KID_BISECT * 4 + 0, work);
 }
 
 // ------------------------------------------------------------------------
@@ -715,14 +745,15 @@ k_root(ProbDev *probs, BlockDev *blocks, double *D, double *E, const double2 *TP
 // Stage A5: refine the approximations w.r.t. the root representation
 // (refine_eigval_approx, unchunked dlarrb, SRC/mrrr_val.c:992-1082).
 // ------------------------------------------------------------------------
-__global__ void __launch_bounds__(128)
-k_refine_root(int N, const ProbDev *probs, const BlockDev *blocks, const int *iblk,
-              const double2 *RP, double *W, double *Werr, const double *Wgap, Tol tol) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= N || iblk[s] < 0) return;
+__device__ __forceinline__ unsigned long long refine_root_body(int s, const ProbDev *probs,
+                                                               const BlockDev *blocks,
+                                                               const int *iblk, const double2 *RP,
+                                                               double *W, double *Werr,
+                                                               const double *Wgap, Tol tol) {
+  if (iblk[s] < 0) return 0;
   const BlockDev *B = &blocks[iblk[s]];
   const ProbDev *p = &probs[B->prob];
-  if (p->status || B->nbl < 2) return;
+  if (p->status || B->nbl < 2) return 0;
   const bool onlyW = (p->jobz == MR3_JOB_N);   // rtol1 = rtol2 = 4 eps (SRC/mrrr.c:230-232)
   const int II = s - B->wbgn + 1;
   const int i = B->ilow + II - 1;
@@ -733,10 +764,22 @@ k_refine_root(int N, const ProbDev *probs, const BlockDev *blocks, const int *ib
   const int maxitr = dv_itmax(B->spdiam + p->pivmin, p->pivmin);
   const double rtol1 = onlyW ? 4.0 * MR3_EPS : tol.rtol1;
   const double rtol2 = onlyW ? 4.0 * MR3_EPS : tol.rtol2;
-  dv_dlarrb_one(B->nbl, RP + B->ibgn, i, II == 1, II > 1, rgap, lgap, rtol1, rtol2, p->pivmin,
-                maxitr, B->nbl, &w, &werr);
+  int nc = 0;
+  dv_dlarrb_one(B->nbl, RP + B->ibgn, 1, i, II == 1, II > 1, rgap, lgap, rtol1, rtol2, p->pivmin,
+                maxitr, B->nbl, &w, &werr, &nc);
   W[s] = w;
   Werr[s] = werr;
+  return (unsigned long long)nc * (unsigned long long)B->nbl;
+}
+
+__global__ void __launch_bounds__(128)
+k_refine_root(int N, const ProbDev *probs, const BlockDev *blocks, const int *iblk,
+              const double2 *RP, double *W, double *Werr, const double *Wgap, Tol tol,
+              unsigned long long *stats) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long work = 0;
+  if (s < N) work = refine_root_body(s, probs, blocks, iblk, RP, W, Werr, Wgap, tol);
+  stat_add(stats, KID_REFROOT * 4 + 1, work);
 }
 
 // Final gaps of the root refinement (dlarrb loop 111) and the last gap of the
@@ -1022,8 +1065,9 @@ __global__ void k_level0(ProbDev *probs, BlockDev *blocks, const double *E, cons
       int c = atomicAdd(&lc->n_cl, 1);
       ClusterDev C;
       C.begin = wb; C.end = we; C.depth = 0; C.blk = p->off + b;
-      C.bl_spdiam = gu - gl; C.lgap = lgap; C.par_off = -1; C.own_off = -1;
-      C.par_sigma = sigma; C.sigma = sigma;
+      C.bl_spdiam = gu - gl; C.lgap = lgap; C.par_off = -1; C.pG = 1; C.pg = 0;
+      C.grp_off = -1; C.G = 1; C.g = 0;
+      C.par_sigma = sigma; C.sigma = sigma; C.tau = 0.0;
       cl[c] = C;
     }
   }
@@ -1033,115 +1077,179 @@ __global__ void k_level0(ProbDev *probs, BlockDev *blocks, const double *E, cons
 // Child representation of each cluster of depth >= 1
 // (compute_new_rrr, SRC/process_cluster.c:105-235).  One warp per cluster.
 // ------------------------------------------------------------------------
-__device__ __forceinline__ void rrr_ptrs(const ClusterDev &C, const BlockDev &B, const double2 *RP,
-                                         const double2 *RQ, const double *arena,
-                                         const double2 **P, const double2 **Q) {
-  if (C.par_off < 0) { *P = RP + B.ibgn; *Q = RQ + B.ibgn; }
+// Parent representation of a cluster: rows P[i*ps], Q[i*ps].
+__device__ __forceinline__ void par_rrr(const ClusterDev &C, const BlockDev &B, const double2 *RP,
+                                        const double2 *RQ, const double *arena,
+                                        const double2 **P, const double2 **Q, int *ps) {
+  if (C.par_off < 0) { *P = RP + B.ibgn; *Q = RQ + B.ibgn; *ps = 1; }
   else {
-    *P = reinterpret_cast<const double2 *>(arena + C.par_off);
-    *Q = reinterpret_cast<const double2 *>(arena + C.par_off + 2 * (long long)B.nbl);
+    *P = reinterpret_cast<const double2 *>(arena + C.par_off) + C.pg;
+    *Q = reinterpret_cast<const double2 *>(arena + C.par_off + 2LL * B.nbl * C.pG) + C.pg;
+    *ps = C.pG;
   }
 }
 
-__global__ void __launch_bounds__(MR3_THREADS)
-k_newrrr(int ncl, ClusterDev *cl, const ProbDev *probs, const BlockDev *blocks,
-         const double2 *RP, const double2 *RQ, const double *arena_prev, double *arena_cur,
-         double *Wsh, double *Werr, double *Wgap, const int *Windex, int *cl_of_slot,
-         int *lvl_of_slot, int level, Tol tol) {
-  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int lane = threadIdx.x & 31;
-  if (w >= ncl) return;
-  ClusterDev C = cl[w];
-  const BlockDev B = blocks[C.blk];
-  const ProbDev *p = &probs[B.prob];
-  const int nb = B.nbl, cb = C.begin, ce = C.end, csz = ce - cb + 1;
-  const double pivmin = p->pivmin;
-  const double2 *Pp, *Qp;
-  rrr_ptrs(C, B, RP, RQ, arena_prev, &Pp, &Qp);
-  double *slot = arena_cur + C.own_off;
-  double2 *Pn = reinterpret_cast<double2 *>(slot);
-  double2 *Qn = reinterpret_cast<double2 *>(slot + 2 * (long long)nb);
-  double *dplus = slot + 4 * (long long)nb, *lplus = slot + 5 * (long long)nb;
-  double *work = slot + 6 * (long long)nb;
-
-  // refine the extremal eigenvalues to full accuracy (dlarrb, RQtol) -- the
-  // two calls see a zero right gap, so their convergence test is independent
-  // of every other gap and they run side by side on lanes 0 and 1
-  const int maxitr = dv_itmax(C.bl_spdiam + pivmin, pivmin);
-  const int off1 = Windex[cb] - 1;
-  double wv = 0.0, ev = 0.0;
-  if (lane < 2) {
-    int sx = (lane == 0) ? cb : ce;
-    int i = Windex[sx];
-    int II = i - off1;
-    wv = Wsh[sx];
-    ev = Werr[sx];
-    dv_dlarrb_one(nb, Pp, i, 1, II > 1, 0.0, 0.0, tol.rqtol, tol.rqtol, pivmin, maxitr, nb, &wv,
-                  &ev);
+// The cluster's own representation (the root for depth 0).
+__device__ __forceinline__ void own_rrr(const ClusterDev &C, const BlockDev &B, const double2 *RP,
+                                        const double2 *RQ, const double *arena,
+                                        const double2 **P, const double2 **Q, int *ps) {
+  if (C.depth == 0) { *P = RP + B.ibgn; *Q = RQ + B.ibgn; *ps = 1; }
+  else {
+    *P = reinterpret_cast<const double2 *>(arena + C.grp_off) + C.g;
+    *Q = reinterpret_cast<const double2 *>(arena + C.grp_off + 2LL * B.nbl * C.G) + C.g;
+    *ps = C.G;
   }
-  double w0 = __shfl_sync(0xffffffffu, wv, 0), e0 = __shfl_sync(0xffffffffu, ev, 0);
-  double w1 = __shfl_sync(0xffffffffu, wv, 1), e1 = __shfl_sync(0xffffffffu, ev, 1);
-  if (lane == 0) {
-    // gap right of the first eigenvalue uses its neighbour before the second call
-    double nw_ = Wsh[cb + 1], ne_ = Werr[cb + 1];
+}
+
+// (a) the two extremal eigenvalues of each cluster refined to full accuracy
+// (dlarrb with RQtol, SRC/process_cluster.c:170-195), one thread per end.
+// Both calls see a zero right gap, so their convergence test does not depend
+// on any other gap and the two ends are independent.
+__global__ void __launch_bounds__(128)
+k_cl_ext(int ncl, const ClusterDev *cl, const ProbDev *probs, const BlockDev *blocks,
+         const double2 *RP, const double2 *RQ, const double *arena_prev, const double *Wsh,
+         const double *Werr, const int *Windex, double *xw, double *xe, Tol tol,
+         unsigned long long *stats) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int w = t >> 1;
+  unsigned long long work = 0;
+  if (w < ncl) {
+    const ClusterDev C = cl[w];
+    const BlockDev &B = blocks[C.blk];
+    const ProbDev *p = &probs[B.prob];
+    const int nb = B.nbl;
+    const double2 *Pp, *Qp;
+    int ps;
+    par_rrr(C, B, RP, RQ, arena_prev, &Pp, &Qp, &ps);
+    const int sx = (t & 1) ? C.end : C.begin;
+    const int i = Windex[sx], II = i - (Windex[C.begin] - 1);
+    const int maxitr = dv_itmax(C.bl_spdiam + p->pivmin, p->pivmin);
+    double wv = Wsh[sx], ev = Werr[sx];
+    int nc = 0;
+    dv_dlarrb_one(nb, Pp, ps, i, 1, II > 1, 0.0, 0.0, tol.rqtol, tol.rqtol, p->pivmin, maxitr, nb,
+                  &wv, &ev, &nc);
+    xw[t] = wv;
+    xe[t] = ev;
+    work = (unsigned long long)nc * nb;
+  }
+  stat_add(stats, KID_NEWRRR * 4 + 1, work);
+}
+
+// (b) child representation by dlarrf (SRC/process_cluster.c:197-210), one
+// thread per cluster, after storing the refined extremes and the gap right of
+// the first eigenvalue (computed against its neighbour's value before the
+// second extreme was refined).
+__global__ void __launch_bounds__(128)
+k_cl_rrf(int ncl, ClusterDev *cl, const ProbDev *probs, const BlockDev *blocks, const double2 *RP,
+         const double2 *RQ, const double *arena_prev, double *arena_cur, const double *xw,
+         const double *xe, double *Wsh, double *Werr, double *Wgap, unsigned long long *stats) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long work = 0;
+  if (w < ncl) {
+    const ClusterDev C = cl[w];
+    const BlockDev &B = blocks[C.blk];
+    const ProbDev *p = &probs[B.prob];
+    const int nb = B.nbl, cb = C.begin, ce = C.end;
+    const double2 *Pp, *Qp;
+    int ps;
+    par_rrr(C, B, RP, RQ, arena_prev, &Pp, &Qp, &ps);
+    double *grp = arena_cur + C.grp_off;
+    const long long nG = (long long)nb * C.G;
+    double *dplus = grp + 4 * nG + C.g, *lplus = grp + 5 * nG + C.g, *wk = grp + 6 * nG + C.g;
+    const double w0 = xw[2 * w], e0 = xe[2 * w], w1 = xw[2 * w + 1], e1 = xe[2 * w + 1];
+    const double nw_ = Wsh[cb + 1], ne_ = Werr[cb + 1];
     Wgap[cb] = fmax(0.0, (nw_ - ne_) - (w0 + e0));
     Wsh[cb] = w0; Werr[cb] = e0;
     Wsh[ce] = w1; Werr[ce] = e1;
+    const double tau = dv_dlarrf(nb, Pp, Qp, ps, ce - cb + 1, Wsh + cb, Wgap + cb, Werr + cb,
+                                 C.bl_spdiam, C.lgap, Wgap[ce], p->pivmin, dplus, lplus, wk, C.G);
+    cl[w].tau = tau;
+    cl[w].sigma = C.par_sigma + tau;
+    work = 2ull * nb;
   }
-  __syncwarp();
-  double tau = 0.0;
-  if (lane == 0) {
-    tau = dv_dlarrf(nb, Pp, Qp, csz, Wsh + cb, Wgap + cb, Werr + cb, C.bl_spdiam, C.lgap, Wgap[ce],
-                    pivmin, dplus, lplus, work);
-  }
-  tau = __shfl_sync(0xffffffffu, tau, 0);
-  __syncwarp();
-  const double sigma = C.par_sigma + tau;
-  for (int k = cb + lane; k <= ce; k += 32) {
-    double f = 3.0 * MR3_EPS * fabs(Wsh[k]);
-    double x = Wsh[k] - tau;
-    Wsh[k] = x;
-    f += 4.0 * MR3_EPS * fabs(x);
-    Werr[k] += f;
-    cl_of_slot[k] = w;
-    lvl_of_slot[k] = level;
-  }
-  for (int i = lane; i < nb; i += 32) {
-    double dv = dplus[i];
-    if (i < nb - 1) {
-      double lv = lplus[i];
-      double ld = dv * lv;
-      Pn[i] = make_double2(dv, ld * lv);
-      Qn[i] = make_double2(lv, ld);
-    } else {
-      Pn[i] = make_double2(dv, 0.0);
-      Qn[i] = make_double2(sigma, 0.0);
+  stat_add(stats, KID_NEWRRR * 4 + 3, work);
+}
+
+// (c) shift the cluster's eigenvalues and errors by tau
+// (SRC/process_cluster.c:212-218) and pack the new representations' rows;
+// one CTA per sibling group, rows of the group's members interleaved.
+__global__ void k_cl_pack(int ncl, const ClusterDev *cl, const BlockDev *blocks, double *arena_cur,
+                          double *Wsh, double *Werr, int *cl_of_slot, int *lvl_of_slot, int level) {
+  for (int w = blockIdx.x; w < ncl; w += gridDim.x) {
+    const ClusterDev L0 = cl[w];
+    if (L0.g != 0) continue;   // the group's first member packs the group
+    const int G = L0.G, nb = blocks[L0.blk].nbl;
+    const long long nG = (long long)nb * G;
+    double *grp = arena_cur + L0.grp_off;
+    double2 *Pn = reinterpret_cast<double2 *>(grp);
+    double2 *Qn = reinterpret_cast<double2 *>(grp + 2 * nG);
+    const double *dplus = grp + 4 * nG, *lplus = grp + 5 * nG;
+    for (int m = 0; m < G; m++) {
+      const ClusterDev C = cl[w + m];
+      const double tau = C.tau;
+      for (int k = C.begin + threadIdx.x; k <= C.end; k += blockDim.x) {
+        double f = 3.0 * MR3_EPS * fabs(Wsh[k]);
+        double x = Wsh[k] - tau;
+        Wsh[k] = x;
+        f += 4.0 * MR3_EPS * fabs(x);
+        Werr[k] += f;
+        cl_of_slot[k] = w + m;
+        lvl_of_slot[k] = level;
+      }
+    }
+    for (long long idx = threadIdx.x; idx < nG; idx += blockDim.x) {
+      const int i = (int)(idx / G);
+      double dv = dplus[idx];
+      if (i < nb - 1) {
+        double lv = lplus[idx];
+        double ld = dv * lv;
+        Pn[idx] = make_double2(dv, ld * lv);
+        Qn[idx] = make_double2(lv, ld);
+      } else {
+        Pn[idx] = make_double2(dv, 0.0);
+        Qn[idx] = make_double2(cl[w + (int)(idx % G)].sigma, 0.0);
+      }
     }
   }
-  if (lane == 0) cl[w].sigma = sigma;
 }
 
 // Refinement of a level's clusters w.r.t. their new representation
 // (refine_eigvals without R-tasks, SRC/process_cluster.c:394-428).
-__global__ void __launch_bounds__(128)
-k_refine_cl(int N, const ClusterDev *cl, const ProbDev *probs, const BlockDev *blocks,
-            const double *arena_cur, double *Wsh, double *Werr, const double *Wgap,
-            const int *Windex, const int *cl_of_slot, const int *lvl_of_slot, int level, Tol tol) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= N || lvl_of_slot[s] != level) return;
+__device__ __forceinline__ unsigned long long refine_cl_body(
+    int s, const ClusterDev *cl, const ProbDev *probs, const BlockDev *blocks,
+    const double *arena_cur, double *Wsh, double *Werr, const double *Wgap, const int *Windex,
+    const int *cl_of_slot, const int *lvl_of_slot, int level, Tol tol) {
+  if (lvl_of_slot[s] != level) return 0;
   const ClusterDev C = cl[cl_of_slot[s]];
   const BlockDev &B = blocks[C.blk];
   const ProbDev *p = &probs[B.prob];
   const int pidx = Windex[C.begin], i = Windex[s], II = i - (pidx - 1);
-  const double2 *P = reinterpret_cast<const double2 *>(arena_cur + C.own_off);
+  const double2 *P, *Q;
+  int ps;
+  own_rrr(C, B, nullptr, nullptr, arena_cur, &P, &Q, &ps);
   const double rgap = Wgap[s];
   const double lgap = (II > 1) ? Wgap[s - 1] : rgap;
   const int maxitr = dv_itmax(C.bl_spdiam + p->pivmin, p->pivmin);
   double w = Wsh[s], e = Werr[s];
-  dv_dlarrb_one(B.nbl, P, i, i == pidx, II > 1, rgap, lgap, tol.rtol1, tol.rtol2, p->pivmin,
-                maxitr, B.nbl, &w, &e);
+  int nc = 0;
+  dv_dlarrb_one(B.nbl, P, ps, i, i == pidx, II > 1, rgap, lgap, tol.rtol1, tol.rtol2, p->pivmin,
+                maxitr, B.nbl, &w, &e, &nc);
   Wsh[s] = w;
   Werr[s] = e;
+  return (unsigned long long)nc * (unsigned long long)B.nbl;
+}
+
+__global__ void __launch_bounds__(128)
+k_refine_cl(int N, const ClusterDev *cl, const ProbDev *probs, const BlockDev *blocks,
+            const double *arena_cur, double *Wsh, double *Werr, const double *Wgap,
+            const int *Windex, const int *cl_of_slot, const int *lvl_of_slot, int level, Tol tol,
+            unsigned long long *stats) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long work = 0;
+  if (s < N)
+    work = refine_cl_body(s, cl, probs, blocks, arena_cur, Wsh, Werr, Wgap, Windex, cl_of_slot,
+                          lvl_of_slot, level, tol);
+  stat_add(stats, KID_REFCL * 4 + 1, work);
 }
 
 __global__ void k_gaps_cl(int N, const ClusterDev *cl, const double *Wsh, const double *Werr,
@@ -1157,14 +1265,33 @@ __global__ void k_gaps_cl(int N, const ClusterDev *cl, const double *Wsh, const 
 // ------------------------------------------------------------------------
 // Classification of a cluster's eigenvalues into singletons and child
 // clusters (PMR_create_subtasks, SRC/process_cluster.c:438-629).  One warp
-// per cluster and two passes: count, then write to the device queues.
+// per cluster.  Three launches: count (and reserve the children and their
+// arena), allocate the singleton records of each sibling group contiguously
+// and cut them into warp tasks, then write the records.
 // ------------------------------------------------------------------------
+struct ClsScratch {
+  int *ns;          // singletons of each cluster
+  int *soff;        // first singleton record of each cluster
+  int *cbase;       // first child of each cluster in the next level's list
+  long long *abase; // arena base of each cluster's children
+};
+
+// Child cluster number `rank` of `nc` children, all of block size nb: its
+// group and its position in the group (groups of 32 consecutive children).
+__device__ __forceinline__ void child_group(ClusterDev &c, int rank, int nc, int nb,
+                                            long long a_base) {
+  const int grp = rank >> 5;
+  c.G = min(32, nc - 32 * grp);
+  c.g = rank & 31;
+  c.grp_off = a_base + 8LL * nb * 32 * grp;
+}
+
 // Children of a segment [first, last] of a depth-0 cluster with more than
 // three members, split where the gap exceeds twice the average gap
 // (SRC/process_cluster.c:542-577).  Returns their number; writes them if out.
 __device__ int split_children(int first, int last, const ClusterDev &parent, double avggap,
                               const double *Wgap, ClusterDev proto, ClusterDev *out,
-                              long long a_base, int crank, long long slot_sz) {
+                              int crank, int nc, int nb, long long a_base) {
   int cnt = 0, cl_first = first;
   for (int k = first + 1; k < last; k++) {
     int cl_last;
@@ -1175,7 +1302,7 @@ __device__ int split_children(int first, int last, const ClusterDev &parent, dou
       ClusterDev c = proto;
       c.begin = cl_first; c.end = cl_last;
       c.lgap = (cl_first == parent.begin) ? parent.lgap : Wgap[cl_first - 1];
-      c.own_off = a_base + (long long)(crank + cnt) * slot_sz;
+      child_group(c, crank + cnt, nc, nb, a_base);
       out[crank + cnt] = c;
     }
     cnt++;
@@ -1184,112 +1311,162 @@ __device__ int split_children(int first, int last, const ClusterDev &parent, dou
   return cnt;
 }
 
+template <int PASS>
 __global__ void __launch_bounds__(MR3_THREADS)
 k_classify(int ncl, const ClusterDev *cl, const BlockDev *blocks, const double *Wsh,
-           const double *Wgap, ClusterDev *cl_next, SngDev *sng, WTask *wt,
-           LevelCounters *lcn, SngCounters *sc, int cap) {
-  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int lane = threadIdx.x & 31;
+           const double *Wgap, ClusterDev *cl_next, SngDev *sng, LevelCounters *lcn,
+           ClsScratch xs, int cap) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   if (w >= ncl) return;
   const ClusterDev C = cl[w];
   const BlockDev &B = blocks[C.blk];
   const int cb = C.begin, ce = C.end, depth = C.depth, nb = B.nbl;
-  const long long slot_sz = 8LL * nb;
   const double avggap = C.bl_spdiam / (nb - 1);
   ClusterDev proto;
   proto.begin = 0; proto.end = 0; proto.lgap = 0.0;
   proto.depth = depth + 1; proto.blk = C.blk; proto.bl_spdiam = C.bl_spdiam;
-  proto.par_off = (depth == 0) ? -1 : C.own_off;
-  proto.par_sigma = C.sigma; proto.sigma = 0.0; proto.own_off = 0;
-  int s_base = 0, c_base = 0;
+  proto.par_off = (depth == 0) ? -1 : C.grp_off;
+  proto.pG = C.G; proto.pg = C.g;
+  proto.par_sigma = C.sigma; proto.sigma = 0.0; proto.tau = 0.0;
+  proto.grp_off = 0; proto.G = 1; proto.g = 0;
+  int s_base = 0, c_base = 0, nc_tot = 0;
   long long a_base = 0;
-  for (int pass = 0; pass < 2; pass++) {
-    int ns = 0, nc = 0, prev_end = cb - 1;
+  if (PASS == 1) {
+    s_base = xs.soff[w]; c_base = xs.cbase[w]; a_base = xs.abase[w];
+    nc_tot = -1;   // filled from the count of pass 0 below
+  }
+  int ns = 0, nc = 0, prev_end = cb - 1;
+  // PASS 1 needs the total child count for the group sizes: recount first
+  if (PASS == 1) {
+    int tot = 0, pe = cb - 1;
     for (int c0 = cb; c0 <= ce; c0 += 32) {
       const int s = c0 + lane;
       bool flag = false;
       if (s <= ce) flag = (s == ce) || (Wgap[s] >= MR3_MIN_RELGAP * fabs(Wsh[s]));
       const unsigned bal = __ballot_sync(0xffffffffu, flag);
       const unsigned below = bal & ((1u << lane) - 1u);
-      const int first = below ? (c0 + 31 - __clz(below)) + 1 : prev_end + 1;
-      int is_sng = 0, nchild = 0;
-      const bool split = flag && depth == 0 && (s - first + 1) > 3;
-      if (flag) {
-        if (s == first) is_sng = 1;
-        else if (split) nchild = split_children(first, s, C, avggap, Wgap, proto, nullptr, 0, 0, 0);
-        else nchild = 1;
-      }
-      int sr = is_sng, cr = nchild;
-      for (int o = 1; o < 32; o <<= 1) {
-        int a = __shfl_up_sync(0xffffffffu, sr, o), b = __shfl_up_sync(0xffffffffu, cr, o);
-        if (lane >= o) { sr += a; cr += b; }
-      }
-      if (pass == 1 && flag) {
-        const int srank = ns + sr - is_sng, crank = nc + cr - nchild;
-        if (is_sng) {
-          SngDev r;
-          r.slot = s; r.cl = w;
-          r.lgap = (s == cb) ? C.lgap : Wgap[s - 1];
-          sng[s_base + srank] = r;
-        } else if (split) {
-          split_children(first, s, C, avggap, Wgap, proto, cl_next + c_base, a_base, crank, slot_sz);
-        } else {
-          ClusterDev c = proto;
-          c.begin = first; c.end = s;
-          c.lgap = (first == cb) ? C.lgap : Wgap[first - 1];
-          c.own_off = a_base + (long long)crank * slot_sz;
-          cl_next[c_base + crank] = c;
-        }
-      }
-      ns += __shfl_sync(0xffffffffu, sr, 31);
-      nc += __shfl_sync(0xffffffffu, cr, 31);
-      prev_end = bal ? (c0 + 31 - __clz(bal)) : prev_end;
+      const int first = below ? (c0 + 31 - __clz(below)) + 1 : pe + 1;
+      int nchild = 0;
+      if (flag && s != first)
+        nchild = (depth == 0 && s - first + 1 > 3)
+                     ? split_children(first, s, C, avggap, Wgap, proto, nullptr, 0, 0, nb, 0)
+                     : 1;
+      for (int o = 16; o > 0; o >>= 1) nchild += __shfl_xor_sync(0xffffffffu, nchild, o);
+      tot += nchild;
+      pe = bal ? (c0 + 31 - __clz(bal)) : pe;
     }
-    if (pass == 0) {
-      int err = 0;
-      if (lane == 0) {
-        s_base = atomicAdd(&sc->n_sng, ns);
-        const int nwt = (ns + 31) / 32;
-        const int t0 = atomicAdd(&sc->n_wt, nwt);
-        c_base = atomicAdd(&lcn->n_cl, nc);
-        a_base = (long long)atomicAdd(&lcn->arena_need, (unsigned long long)(nc * slot_sz));
-        if (s_base + ns > cap || c_base + nc > cap || t0 + nwt > cap) {
-          atomicOr(&lcn->err, 1);
-          err = 1;
-        } else {
-          for (int t = 0; t < nwt; t++) {
-            WTask x;
-            x.first = s_base + 32 * t;
-            x.count = min(32, ns - 32 * t);
-            wt[t0 + t] = x;
-          }
-        }
-      }
-      s_base = __shfl_sync(0xffffffffu, s_base, 0);
-      c_base = __shfl_sync(0xffffffffu, c_base, 0);
-      a_base = __shfl_sync(0xffffffffu, a_base, 0);
-      if (__shfl_sync(0xffffffffu, err, 0)) return;
+    nc_tot = tot;
+  }
+  for (int c0 = cb; c0 <= ce; c0 += 32) {
+    const int s = c0 + lane;
+    bool flag = false;
+    if (s <= ce) flag = (s == ce) || (Wgap[s] >= MR3_MIN_RELGAP * fabs(Wsh[s]));
+    const unsigned bal = __ballot_sync(0xffffffffu, flag);
+    const unsigned below = bal & ((1u << lane) - 1u);
+    const int first = below ? (c0 + 31 - __clz(below)) + 1 : prev_end + 1;
+    int is_sng = 0, nchild = 0;
+    const bool split = flag && depth == 0 && (s - first + 1) > 3;
+    if (flag) {
+      if (s == first) is_sng = 1;
+      else if (split)
+        nchild = split_children(first, s, C, avggap, Wgap, proto, nullptr, 0, 0, nb, 0);
+      else nchild = 1;
     }
+    int sr = is_sng, cr = nchild;
+    for (int o = 1; o < 32; o <<= 1) {
+      int a = __shfl_up_sync(0xffffffffu, sr, o), b = __shfl_up_sync(0xffffffffu, cr, o);
+      if (lane >= o) { sr += a; cr += b; }
+    }
+    if (PASS == 1 && flag) {
+      const int srank = ns + sr - is_sng, crank = nc + cr - nchild;
+      if (is_sng) {
+        SngDev r;
+        r.slot = s; r.cl = w;
+        r.lgap = (s == cb) ? C.lgap : Wgap[s - 1];
+        sng[s_base + srank] = r;
+      } else if (split) {
+        split_children(first, s, C, avggap, Wgap, proto, cl_next + c_base, crank, nc_tot, nb,
+                       a_base);
+      } else {
+        ClusterDev c = proto;
+        c.begin = first; c.end = s;
+        c.lgap = (first == cb) ? C.lgap : Wgap[first - 1];
+        child_group(c, crank, nc_tot, nb, a_base);
+        cl_next[c_base + crank] = c;
+      }
+    }
+    ns += __shfl_sync(0xffffffffu, sr, 31);
+    nc += __shfl_sync(0xffffffffu, cr, 31);
+    prev_end = bal ? (c0 + 31 - __clz(bal)) : prev_end;
+  }
+  if (PASS == 0 && lane == 0) {
+    xs.ns[w] = ns;
+    const int cb0 = atomicAdd(&lcn->n_cl, nc);
+    // groups of 32 children; only the last group can be smaller
+    const long long need = 8LL * nb * nc;
+    const long long ab = (long long)atomicAdd(&lcn->arena_need, (unsigned long long)need);
+    xs.cbase[w] = cb0;
+    xs.abase[w] = ab;
+    if (cb0 + nc > cap) atomicOr(&lcn->err, 1);
+  }
+}
+
+// Per sibling group (led by the member with g == 0): reserve the group's
+// singleton records contiguously and cut them into warp tasks of 32.
+__global__ void k_group_tasks(int ncl, const ClusterDev *cl, ClsScratch xs, WTask *wt,
+                              SngCounters *sc, LevelCounters *lcn, int cap) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= ncl) return;
+  const ClusterDev C = cl[w];
+  if (C.g != 0) return;
+  int tot = 0;
+  for (int m = 0; m < C.G; m++) tot += xs.ns[w + m];
+  if (tot == 0) return;
+  const int base = atomicAdd(&sc->n_sng, tot);
+  const int nwt = (tot + 31) / 32;
+  const int t0 = atomicAdd(&sc->n_wt, nwt);
+  if (base + tot > cap || t0 + nwt > cap) { atomicOr(&lcn->err, 1); return; }
+  int o = base;
+  for (int m = 0; m < C.G; m++) { xs.soff[w + m] = o; o += xs.ns[w + m]; }
+  for (int t = 0; t < nwt; t++) {
+    WTask x;
+    x.first = base + 32 * t;
+    x.count = min(32, tot - 32 * t);
+    wt[t0 + t] = x;
   }
 }
 
 // ------------------------------------------------------------------------
 // Singletons (PMR_process_s_task, SRC/process_singleton.c:65-317): one lane
-// per eigenvector, 32 eigenvectors of one cluster per warp.  Persistent warps
-// pull warp tasks from a device counter.  Each warp owns a scratch region of
-// 2 x nmax x 32 doubles laid out [array][row][lane] so that the lock-step
-// passes of the twisted factorisation read and write whole 256-byte rows.
+// per eigenvector, up to 32 eigenvectors of one cluster per warp.  Persistent
+// warps pull warp tasks from a device counter.  Each warp owns a scratch
+// region of 2 x nmax x 32 doubles laid out [array][row][lane]; the twisted
+// factorisations of the 32 lanes sweep the rows in lock-step, so every
+// scratch access is one coalesced 256-byte row.  The Rayleigh-quotient loop
+// of each lane is a small state machine: in every round each lane that still
+// needs a factorisation takes one, so lanes that need more iterations do not
+// hold the others' sweeps apart.  Eigenvectors leave through a shared-memory
+// transpose, so the Z columns are written in coalesced rows.
 // ------------------------------------------------------------------------
-__global__ void __launch_bounds__(MR3_THREADS)
+#define SNG_WARPS 8
+#define SNG_TILE_LD 33
+enum { PH_LOOP = 0, PH_STEP2 = 1, PH_DONE = 2 };
+
+__global__ void __launch_bounds__(SNG_WARPS * 32, 2)
 k_singletons(const WTask *wt, const SngDev *sng, const ClusterDev *cl, const ProbDev *probs,
              const BlockDev *blocks, const double2 *RP, const double2 *RQ, const double *arena,
              double *W, double *Wsh, double *Werr, double *Wgap, const int *Windex,
-             const int *Zindex, SngCounters *sc, double *scratch, long long nmax) {
+             const int *Zindex, SngCounters *sc, double *scratch, long long nmax,
+             unsigned long long *stats) {
+  extern __shared__ double sm_tile[];
   const int lane = threadIdx.x & 31;
+  double *tile = sm_tile + (threadIdx.x >> 5) * 32 * SNG_TILE_LD;
   const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   double *X = scratch + gw * 2 * nmax * 32 + lane;
   double *Y = X + nmax * 32;
   const int nwt = sc->n_wt;
+  unsigned long long w_r1v = 0, w_neg = 0, w_sweep = 0, w_rounds = 0, w_tasks = 0;
   for (;;) {
     int t = 0;
     if (lane == 0) t = atomicAdd(&sc->wt_next, 1);
@@ -1303,105 +1480,136 @@ k_singletons(const WTask *wt, const SngDev *sng, const ClusterDev *cl, const Pro
     const ProbDev *p = &probs[B.prob];
     const int nb = B.nbl;
     const double pivmin = p->pivmin;
+    // lanes of one task come from sibling clusters of one group: same block
+    // and block size, each lane reading its own (interleaved) representation
     const double2 *P, *Q;
-    if (C.depth == 0) { P = RP + B.ibgn; Q = RQ + B.ibgn; }
-    else {
-      P = reinterpret_cast<const double2 *>(arena + C.own_off);
-      Q = reinterpret_cast<const double2 *>(arena + C.own_off + 2 * (long long)nb);
-    }
-    const double sigma = C.sigma;
-    int r = 0, is1 = 1, is2 = nb;
-    double norminv = 0.0;
-    int zind = 0;
+    int ps;
+    own_rrr(C, B, RP, RQ, arena, &P, &Q, &ps);
+    const double twoeps = 2.0 * MR3_EPS, rqtol = 2.0 * MR3_EPS;
+    const double tolr = 4.0 * dv_log((double)nb) * MR3_EPS;
+    const int maxitr = dv_itmax(C.bl_spdiam + pivmin, pivmin);
+    const int s = S.slot;
+    double lambda = 0.0, wsh = 0.0, werr = 0.0, left = 0.0, right = 0.0, gap = 0.0, gaptol = 0.0;
+    int iloc = 0;
     if (active) {
-      const int s = S.slot;
-      const double twoeps = 2.0 * MR3_EPS, rqtol = 2.0 * MR3_EPS;
-      const double tolr = 4.0 * dv_log((double)nb) * MR3_EPS;
-      double lambda = Wsh[s], wsh = Wsh[s], werr = Werr[s];
-      double left = lambda - werr, right = lambda + werr;
-      const int iloc = Windex[s];
+      lambda = Wsh[s]; wsh = lambda; werr = Werr[s];
+      left = lambda - werr; right = lambda + werr;
+      iloc = Windex[s];
       // the reference compares the eigenvalue index with the block's first
       // and last row (SRC/process_singleton.c:142-157); W slots and rows of a
       // problem start at the same offset, so the same comparison is s == row
       double lgap = (s == B.ibgn) ? MR3_EPS * fmax(fabs(left), fabs(right)) : S.lgap;
       double rgap = (s == B.iend) ? MR3_EPS * fmax(fabs(left), fabs(right)) : Wgap[s];
-      double gap = fmin(lgap, rgap);
-      double gaptol = (s == B.ibgn || s == B.iend) ? 0.0 : gap * MR3_EPS;
-      int supmn = nb, supmx = 1;
-      bool usedBS = false, usedRQ = false, needBS = false, wantNC = true;
-      double bstres = 0.0, bstw = 0.0, resid = 0.0;
-      const int maxitr = dv_itmax(C.bl_spdiam + pivmin, pivmin);
-      dlar1v_out o;
-      for (int k = 1; k <= MR3_MAXITER; k++) {
-        if (needBS) {
-          usedBS = true;
-          int tw = (r < 1 || r > nb) ? nb : r;
-          dv_dlarrb_one(nb, P, iloc, 1, 0, 0.0, 0.0, 0.0, twoeps, pivmin, maxitr, tw, &wsh, &werr);
-          lambda = wsh;
-          r = 0;
-        }
-        wantNC = !usedBS;
-        dv_dlar1v(nb, lambda, P, Q, pivmin, gaptol, wantNC, r, X, Y, 32, &o);
+      gap = fmin(lgap, rgap);
+      gaptol = (s == B.ibgn || s == B.iend) ? 0.0 : gap * MR3_EPS;
+    }
+    int phase = active ? PH_LOOP : PH_DONE;
+    int k = 1, r = 0;
+    bool usedBS = false, usedRQ = false, needBS = false;
+    double bstres = 0.0, bstw = 0.0, resid = 0.0;
+    dlar1v_out o;
+    o.isupp1 = 1; o.isupp2 = nb; o.nrminv = 0.0; o.r = 0;
+    if (lane == 0) w_tasks++;
+    while (__any_sync(0xffffffffu, phase != PH_DONE)) {
+      const bool call = (phase != PH_DONE);
+      if (lane == 0) { w_rounds++; w_sweep += nb; }
+      if (call && phase == PH_LOOP && needBS) {
+        usedBS = true;
+        int tw = (r < 1 || r > nb) ? nb : r;
+        int nc = 0;
+        dv_dlarrb_one(nb, P, ps, iloc, 1, 0, 0.0, 0.0, 0.0, twoeps, pivmin, maxitr, tw, &wsh, &werr,
+                      &nc);
+        w_neg += (unsigned long long)nc * nb;
+        lambda = wsh;
+        r = 0;
+      }
+      const bool wantNC = !usedBS;
+      const double lam_call = (phase == PH_STEP2) ? bstw : lambda;
+      r1v_state st;
+      st.r = 0; st.mingma = 0.0; st.sawnan = false;
+      int negc = 0;
+      if (call) {
+        dv_r1v_factor(nb, lam_call, P, Q, ps, pivmin, wantNC, r, X, Y, 32, &negc, &st);
+        w_r1v += nb;
+      }
+      dv_r1v_solve(call, nb, Q, ps, gaptol, X, Y, 32, st, &o);
+      if (call) {
         r = o.r;
-        resid = o.resid;
-        if (k == 1 || o.resid < bstres) { bstres = o.resid; bstw = lambda; }
-        supmn = min(supmn, o.isupp1);
-        supmx = max(supmx, o.isupp2);
-        if (!usedBS && o.resid > tolr * gap && fabs(o.rqcorr) > rqtol * fabs(lambda)) {
-          int sgndef = (iloc <= o.negcnt) ? -1 : 1;
-          if (o.rqcorr * sgndef >= 0.0 && lambda + o.rqcorr <= right &&
-              lambda + o.rqcorr >= left) {
-            usedRQ = true;
-            if (sgndef == 1) left = lambda; else right = lambda;
-            wsh = 0.5 * (left + right);
-            lambda += o.rqcorr;
-          } else {
-            needBS = true;
-          }
-          if (right - left < rqtol * fabs(lambda)) usedBS = true;
-          else if (k == MR3_MAXITER - 1) needBS = true;
+        if (phase == PH_STEP2) {
+          lambda = bstw;
+          phase = PH_DONE;
         } else {
-          break;
+          resid = o.resid;
+          if (k == 1 || o.resid < bstres) { bstres = o.resid; bstw = lambda; }
+          bool more = false;
+          if (!usedBS && o.resid > tolr * gap && fabs(o.rqcorr) > rqtol * fabs(lambda)) {
+            int sgndef = (iloc <= negc) ? -1 : 1;
+            if (o.rqcorr * sgndef >= 0.0 && lambda + o.rqcorr <= right &&
+                lambda + o.rqcorr >= left) {
+              usedRQ = true;
+              if (sgndef == 1) left = lambda; else right = lambda;
+              wsh = 0.5 * (left + right);
+              lambda += o.rqcorr;
+            } else {
+              needBS = true;
+            }
+            if (right - left < rqtol * fabs(lambda)) usedBS = true;
+            else if (k == MR3_MAXITER - 1) needBS = true;
+            k++;
+            more = (k <= MR3_MAXITER);
+          }
+          if (!more) phase = (usedRQ && usedBS && bstres <= resid) ? PH_STEP2 : PH_DONE;
         }
       }
-      if (usedRQ && usedBS && bstres <= resid) {
-        lambda = bstw;
-        dv_dlar1v(nb, lambda, P, Q, pivmin, gaptol, wantNC, r, X, Y, 32, &o);
-        r = o.r;
-      }
-      (void)supmn; (void)supmx;
+    }
+    const int bl0 = B.ibgn - p->off;   // block's first row inside the problem
+    int zind = 0;
+    if (active) {
       Wsh[s] = lambda;
       Werr[s] = werr;
       Wgap[s] = gap;
-      W[s] = lambda + sigma;
-      is1 = o.isupp1;
-      is2 = o.isupp2;
-      norminv = o.nrminv;
+      W[s] = lambda + C.sigma;
       zind = Zindex[s];
-      const int bl0 = B.ibgn - p->off;   // block's first row inside the problem
-      p->Zsupp[2 * (size_t)zind] = is1 + bl0;
-      p->Zsupp[2 * (size_t)zind + 1] = is2 + bl0;
+      p->Zsupp[2 * (size_t)zind] = o.isupp1 + bl0;
+      p->Zsupp[2 * (size_t)zind + 1] = o.isupp2 + bl0;
     }
-    __syncwarp();
-    // write the warp's eigenvectors: whole columns, rows spread over lanes
-    const int np = p->n, bl0 = B.ibgn - p->off;
+    // eigenvectors out: tiles of 32 rows, transposed through shared memory
+    const int np = p->n;
     const size_t ldz = (size_t)p->ldz;
-    for (int v = 0; v < T.count; v++) {
-      const int rv = __shfl_sync(0xffffffffu, r, v);
-      const int a1 = __shfl_sync(0xffffffffu, is1, v), a2 = __shfl_sync(0xffffffffu, is2, v);
-      const double nv = __shfl_sync(0xffffffffu, norminv, v);
-      const int zc = __shfl_sync(0xffffffffu, zind, v);
-      double *Zc = p->Z + (size_t)zc * ldz;
-      const double *Xv = X - lane + v, *Yv = Y - lane + v;
-      for (int row = lane; row < np; row += 32) {
-        int k = row - bl0 + 1;   // 1-based row inside the block
+    const int a1 = o.isupp1, a2 = o.isupp2;
+    const double nv = o.nrminv;
+    for (int k0 = 1; k0 <= nb; k0 += 32) {
+#pragma unroll 4
+      for (int j = 0; j < 32; j++) {
+        const int kk = k0 + j;
         double val = 0.0;
-        if (k >= a1 && k <= a2) val = dv_zget(Xv, Yv, 32, rv, k) * nv;
-        Zc[row] = val;
+        if (active && kk <= nb && kk >= a1 && kk <= a2) val = dv_zget(X, Y, 32, r, kk) * nv;
+        tile[j * SNG_TILE_LD + lane] = val;
+      }
+      __syncwarp();
+      const int row = bl0 + k0 - 1 + lane;
+      for (int v = 0; v < T.count; v++) {
+        const int zc = __shfl_sync(0xffffffffu, zind, v);
+        if (k0 + lane <= nb) p->Z[(size_t)zc * ldz + row] = tile[lane * SNG_TILE_LD + v];
+      }
+      __syncwarp();
+    }
+    if (np > nb) {   // rows of the problem outside this block are zero
+      for (int v = 0; v < T.count; v++) {
+        const int zc = __shfl_sync(0xffffffffu, zind, v);
+        double *Zc = p->Z + (size_t)zc * ldz;
+        for (int row = lane; row < bl0; row += 32) Zc[row] = 0.0;
+        for (int row = bl0 + nb + lane; row < np; row += 32) Zc[row] = 0.0;
       }
     }
     __syncwarp();
   }
+  stat_add(stats, KID_SNG * 4 + 1, w_neg);
+  stat_add(stats, KID_SNG * 4 + 2, w_r1v);
+  // diagnostics: warp-level row sweeps, Rayleigh rounds and tasks
+  stat_add(stats, KID_OTHER * 4 + 0, w_sweep);
+  stat_add(stats, KID_OTHER * 4 + 1, w_rounds);
+  stat_add(stats, KID_OTHER * 4 + 2, w_tasks);
 }
 
 // Unit vectors of 1x1 blocks (SRC/process_singleton.c:125-133).
@@ -1515,6 +1723,8 @@ struct mr3_cuda_ctx {
   int *blk_of_row = nullptr, *Windex = nullptr, *iblk = nullptr, *It = nullptr, *Zindex = nullptr;
   int *prob_of_slot = nullptr, *cl_of_slot = nullptr, *lvl_of_slot = nullptr, *unit_list = nullptr;
   int *flag = nullptr, *tmp2 = nullptr;
+  int *cls_ns = nullptr, *cls_soff = nullptr, *cls_cbase = nullptr;
+  long long *cls_abase = nullptr;
   double *D = nullptr, *E = nullptr, *E2 = nullptr, *Wt = nullptr, *Et = nullptr, *W = nullptr;
   double *Werr = nullptr, *Wgap = nullptr, *Wcopy = nullptr, *Wsh = nullptr, *Dt = nullptr;
   double *Lt = nullptr, *Wout = nullptr;
@@ -1538,7 +1748,44 @@ struct mr3_cuda_ctx {
   int *h_iconst = nullptr;     // {1, 1}
   void *ws[MR3_CUDA_WS_SLOTS] = {nullptr};
   size_t ws_cap[MR3_CUDA_WS_SLOTS] = {0};
+  // profiling: per-kernel CUDA-event timing and device work counters
+  int prof = 0;
+  unsigned long long *stats = nullptr;
+  std::vector<cudaEvent_t> evpool;
+  size_t evnext = 0;
+  struct Pending { const char *name; cudaEvent_t a, b; };
+  std::vector<Pending> pending;
+  std::vector<std::string> knames;
+  std::vector<double> kms;
+  std::vector<long long> kcount;
 };
+
+static cudaEvent_t prof_event(mr3_cuda_ctx *c) {
+  if (c->evnext == c->evpool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    c->evpool.push_back(e);
+  }
+  return c->evpool[c->evnext++];
+}
+
+static void prof_flush(mr3_cuda_ctx *c) {
+  for (auto &q : c->pending) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, q.a, q.b);
+    size_t k = 0;
+    while (k < c->knames.size() && c->knames[k] != q.name) k++;
+    if (k == c->knames.size()) {
+      c->knames.emplace_back(q.name);
+      c->kms.push_back(0.0);
+      c->kcount.push_back(0);
+    }
+    c->kms[k] += ms;
+    c->kcount[k] += 1;
+  }
+  c->pending.clear();
+  c->evnext = 0;
+}
 
 #define CK(call, what)                                                    \
   do {                                                                    \
@@ -1549,12 +1796,23 @@ struct mr3_cuda_ctx {
     }                                                                     \
   } while (0)
 
-#define LAUNCH(kern, grid, block, ...)                                    \
+#define LAUNCH(kern, grid, block, ...) LAUNCH_SMEM(kern, grid, block, 0, __VA_ARGS__)
+#define LAUNCH_SMEM(kern, grid, block, smem, ...)                         \
   do {                                                                    \
     if ((grid) > 0) {                                                     \
-      kern<<<(grid), (block), 0, st>>>(__VA_ARGS__);                      \
+      cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;                         \
+      if (c->prof) {                                                      \
+        ev0_ = prof_event(c);                                             \
+        ev1_ = prof_event(c);                                             \
+        cudaEventRecord(ev0_, st);                                        \
+      }                                                                   \
+      kern<<<(grid), (block), (smem), st>>>(__VA_ARGS__);                 \
       c->launches++;                                                      \
       CK(cudaGetLastError(), #kern);                                      \
+      if (c->prof) {                                                      \
+        cudaEventRecord(ev1_, st);                                        \
+        c->pending.push_back({#kern, ev0_, ev1_});                        \
+      }                                                                   \
     }                                                                     \
   } while (0)
 
@@ -1579,6 +1837,10 @@ static int ensure_rows(mr3_cuda_ctx *c, size_t N, size_t P) {
     CK(regrow(&c->lvl_of_slot, n), "lvl_of_slot");
     CK(regrow(&c->unit_list, n), "unit_list");
     CK(regrow(&c->tmp2, 2 * n), "tmp2");
+    CK(regrow(&c->cls_ns, n), "cls_ns");
+    CK(regrow(&c->cls_soff, n), "cls_soff");
+    CK(regrow(&c->cls_cbase, n), "cls_cbase");
+    CK(regrow(&c->cls_abase, n), "cls_abase");
     double **dd[] = {&c->D, &c->E, &c->E2, &c->Wt, &c->Et, &c->W, &c->Werr, &c->Wgap,
                      &c->Wcopy, &c->Wsh, &c->Dt, &c->Lt, &c->Wout};
     for (double **q : dd) CK(regrow(q, n), "rows");
@@ -1625,10 +1887,13 @@ extern "C" int mr3_cuda_ctx_create(int device, mr3_cuda_ctx **out) {
       cudaMallocHost((void **)&c->h_lc, 2 * sizeof(LevelCounters)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_sc, sizeof(SngCounters)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_const, sizeof(double)) != cudaSuccess ||
-      cudaMallocHost((void **)&c->h_iconst, 2 * sizeof(int)) != cudaSuccess) {
+      cudaMallocHost((void **)&c->h_iconst, 2 * sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void **)&c->stats, KID_COUNT * 4 * sizeof(unsigned long long)) != cudaSuccess) {
     mr3_cuda_ctx_destroy(c);
     return MR3_EMISC;
   }
+  cudaFuncSetAttribute(k_singletons, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       SNG_WARPS * 32 * SNG_TILE_LD * (int)sizeof(double));
   c->h_const[0] = 1.0;
   c->h_iconst[0] = 1;
   c->h_iconst[1] = 1;
@@ -1644,6 +1909,7 @@ extern "C" void mr3_cuda_ctx_destroy(mr3_cuda_ctx *c) {
                  c->D, c->E, c->E2, c->Wt, c->Et, c->W, c->Werr, c->Wgap, c->Wcopy, c->Wsh,
                  c->Dt, c->Lt, c->Wout, c->gers, c->TP, c->TPc, c->RP, c->RQ, c->rec0, c->rec1,
                  c->cl[0], c->cl[1], c->sng, c->wt, c->lc, c->sc, c->scratch, c->arena[0],
+                 c->cls_ns, c->cls_soff, c->cls_cbase, c->cls_abase,
                  c->arena[1], (void *)c->Din, (void *)c->Ein, c->Wp, c->Dp, c->Ep};
   for (void *q : dev)
     if (q) cudaFree(q);
@@ -1652,6 +1918,8 @@ extern "C" void mr3_cuda_ctx_destroy(mr3_cuda_ctx *c) {
   void *host[] = {c->h_probs, c->h_ptrs, c->h_lc, c->h_sc, c->h_flag, c->h_const, c->h_iconst};
   for (void *q : host)
     if (q) cudaFreeHost(q);
+  if (c->stats) cudaFree(c->stats);
+  for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
 }
@@ -1698,6 +1966,36 @@ extern "C" int mr3_cuda_sync(mr3_cuda_ctx *c) {
   return MR3_OK;
 }
 
+extern "C" void mr3_cuda_profile(mr3_cuda_ctx *c, int on) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->own);
+  c->prof = on;
+  c->pending.clear();
+  c->evnext = 0;
+  c->knames.clear();
+  c->kms.clear();
+  c->kcount.clear();
+  cudaMemset(c->stats, 0, KID_COUNT * 4 * sizeof(unsigned long long));
+  cudaDeviceSynchronize();
+}
+
+extern "C" int mr3_cuda_profile_read(mr3_cuda_ctx *c, int max, char *names, double *ms,
+                                     long long *launches, unsigned long long *counters) {
+  if (!c) return 0;
+  int k = (int)std::min<size_t>((size_t)max, c->knames.size());
+  for (int i = 0; i < k; i++) {
+    strncpy(names + 32 * i, c->knames[i].c_str(), 31);
+    names[32 * i + 31] = 0;
+    ms[i] = c->kms[i];
+    launches[i] = c->kcount[i];
+  }
+  if (counters)
+    cudaMemcpy(counters, c->stats, KID_COUNT * 4 * sizeof(unsigned long long),
+               cudaMemcpyDeviceToHost);
+  return k;
+}
+
 extern "C" long long mr3_cuda_last_launches(const mr3_cuda_ctx *c) { return c ? c->launches : 0; }
 extern "C" const char *mr3_cuda_last_error(const mr3_cuda_ctx *c) { return c ? c->err : ""; }
 
@@ -1713,20 +2011,24 @@ static int valid_prob(const mr3_cuda_prob &q) {
 
 // Sort the records of the problems selected by (want_job, flag) in place in
 // rec0/rec1; returns the buffer holding the result.
-static SortRec *merge_sort(mr3_cuda_ctx *c, cudaStream_t st, int N, int mmax, int want_job,
-                           const int *flag, int *rc) {
+static int merge_sort_impl(mr3_cuda_ctx *c, cudaStream_t st, int N, int mmax, int want_job,
+                           const int *flag, SortRec **result) {
   SortRec *in = c->rec0, *out = c->rec1;
-  *rc = MR3_OK;
+  // every pass writes every element of every selected problem
   for (int width = 1; width < mmax; width *= 2) {
-    k_merge_pass<<<(N + 255) / 256, 256, 0, st>>>(N, c->probs, c->prob_of_slot, in, out, width,
-                                                   want_job, flag);
-    c->launches++;
-    if (cudaGetLastError() != cudaSuccess) { *rc = MR3_EMISC; return in; }
-    // elements of unselected problems stay in `in` only; copy them over by
-    // swapping only what was written: every selected element was written.
+    LAUNCH(k_merge_pass, (N + 255) / 256, 256, N, c->probs, c->prob_of_slot, in, out, width,
+           want_job, flag);
     std::swap(in, out);
   }
-  return in;
+  *result = in;
+  return MR3_OK;
+}
+
+static SortRec *merge_sort(mr3_cuda_ctx *c, cudaStream_t st, int N, int mmax, int want_job,
+                           const int *flag, int *rc) {
+  SortRec *r = c->rec0;
+  *rc = merge_sort_impl(c, st, N, mmax, want_job, flag, &r);
+  return r;
 }
 
 extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *stream) {
@@ -1824,15 +2126,16 @@ extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *s
   LAUNCH(k_prologue, L, MR3_THREADS, c->probs, c->blocks, c->blk_of_row, c->D, c->E, c->E2,
          c->gers, c->TP, c->TPc, tol);
   LAUNCH(k_blocks, L, MR3_THREADS, c->probs, c->blocks, c->D, c->E, c->gers, c->TP, tol);
+  unsigned long long *stats = c->prof ? c->stats : nullptr;
   LAUNCH(k_bisect, gN128, 128, NN, c->probs, c->blocks, c->blk_of_row, c->TP, c->Wt, c->Et, c->It,
-         tol);
+         tol, stats);
   LAUNCH(k_compact, L, MR3_THREADS, c->probs, c->blocks, c->D, c->Wt, c->Et, c->It, c->W, c->Werr,
          c->Windex, c->iblk, c->Wcopy);
   LAUNCH(k_gaps_init, gN, 256, NN, c->probs, c->blocks, c->iblk, c->W, c->Werr, c->Wgap);
   LAUNCH(k_root, L, MR3_THREADS, c->probs, c->blocks, c->D, c->E, c->TP, c->Dt, c->Lt, c->W,
          c->Werr, c->Wgap, c->RP, c->RQ);
   LAUNCH(k_refine_root, gN128, 128, NN, c->probs, c->blocks, c->iblk, c->RP, c->W, c->Werr,
-         c->Wgap, tol);
+         c->Wgap, tol, stats);
   LAUNCH(k_gaps_root, gN, 256, NN, c->probs, c->blocks, c->iblk, c->W, c->Werr, c->Wgap);
   LAUNCH(k_discard, (L + 127) / 128, 128, c->probs, L, c->blocks, c->W, c->Werr, c->Wgap,
          c->Windex, c->iblk, c->Wcopy);
@@ -1858,38 +2161,47 @@ extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *s
     const size_t per_warp = 2ull * (size_t)nmaxV * 32ull;
     const size_t budget = (size_t)8 << 30;   // bytes
     size_t nwarps = std::min<size_t>((size_t)c->nsm * 32, std::max<size_t>(c->nsm, budget / (per_warp * 8)));
-    nwarps = (nwarps + 7) / 8 * 8;
+    nwarps = (nwarps + SNG_WARPS - 1) / SNG_WARPS * SNG_WARPS;
     if (nwarps * per_warp > c->capScratch) {
       CK(regrow(&c->scratch, nwarps * per_warp), "scratch");
       c->capScratch = nwarps * per_warp;
     }
     int ncl = c->h_lc[0].n_cl;
     const int DEPTH_CAP = 512;
+    ClsScratch xs;
+    xs.ns = c->cls_ns; xs.soff = c->cls_soff; xs.cbase = c->cls_cbase; xs.abase = c->cls_abase;
     for (int level = 0; ncl > 0; level++) {
       if (level >= DEPTH_CAP) { snprintf(c->err, sizeof(c->err), "representation tree too deep"); return MR3_EMISC; }
       const int cur = level & 1, nxt = cur ^ 1;
       const int gW = (ncl * 32 + MR3_THREADS - 1) / MR3_THREADS;
       if (level > 0) {
-        LAUNCH(k_newrrr, gW, MR3_THREADS, ncl, c->cl[cur], c->probs, c->blocks, c->RP, c->RQ,
-               c->arena[nxt], c->arena[cur], c->Wsh, c->Werr, c->Wgap, c->Windex, c->cl_of_slot,
-               c->lvl_of_slot, level, tol);
+        LAUNCH(k_cl_ext, (2 * ncl + 127) / 128, 128, ncl, c->cl[cur], c->probs, c->blocks, c->RP,
+               c->RQ, c->arena[nxt], c->Wsh, c->Werr, c->Windex, c->Wt, c->Et, tol, stats);
+        LAUNCH(k_cl_rrf, (ncl + 127) / 128, 128, ncl, c->cl[cur], c->probs, c->blocks, c->RP, c->RQ,
+               c->arena[nxt], c->arena[cur], c->Wt, c->Et, c->Wsh, c->Werr, c->Wgap, stats);
+        LAUNCH(k_cl_pack, std::min(ncl, 65535 * 16), 256, ncl, c->cl[cur], c->blocks, c->arena[cur],
+               c->Wsh, c->Werr, c->cl_of_slot, c->lvl_of_slot, level);
         LAUNCH(k_refine_cl, gN128, 128, NN, c->cl[cur], c->probs, c->blocks, c->arena[cur], c->Wsh,
-               c->Werr, c->Wgap, c->Windex, c->cl_of_slot, c->lvl_of_slot, level, tol);
+               c->Werr, c->Wgap, c->Windex, c->cl_of_slot, c->lvl_of_slot, level, tol, stats);
         LAUNCH(k_gaps_cl, gN, 256, NN, c->cl[cur], c->Wsh, c->Werr, c->Wgap, c->W, c->cl_of_slot,
                c->lvl_of_slot, level);
       }
       CK(cudaMemsetAsync(&c->lc[nxt], 0, sizeof(LevelCounters), st), "lcn");
       CK(cudaMemsetAsync(c->sc, 0, 3 * sizeof(int), st), "scn");
-      LAUNCH(k_classify, gW, MR3_THREADS, ncl, c->cl[cur], c->blocks, c->Wsh, c->Wgap, c->cl[nxt],
-             c->sng, c->wt, &c->lc[nxt], c->sc, NN);
+      LAUNCH(k_classify<0>, gW, MR3_THREADS, ncl, c->cl[cur], c->blocks, c->Wsh, c->Wgap,
+             c->cl[nxt], c->sng, &c->lc[nxt], xs, NN);
+      LAUNCH(k_group_tasks, (ncl + 127) / 128, 128, ncl, c->cl[cur], xs, c->wt, c->sc, &c->lc[nxt], NN);
+      LAUNCH(k_classify<1>, gW, MR3_THREADS, ncl, c->cl[cur], c->blocks, c->Wsh, c->Wgap,
+             c->cl[nxt], c->sng, &c->lc[nxt], xs, NN);
       CK(cudaMemcpyAsync(c->h_lc, &c->lc[nxt], sizeof(LevelCounters), cudaMemcpyDeviceToHost, st), "lcn d2h");
       CK(cudaMemcpyAsync(c->h_sc, c->sc, sizeof(SngCounters), cudaMemcpyDeviceToHost, st), "sc d2h");
       CK(cudaStreamSynchronize(st), "level sync");
       if (c->h_lc->err) { snprintf(c->err, sizeof(c->err), "queue overflow"); return MR3_EMISC; }
       if (c->h_sc->n_wt > 0)
-        LAUNCH(k_singletons, (int)(nwarps / 8), MR3_THREADS, c->wt, c->sng, c->cl[cur], c->probs,
+        LAUNCH_SMEM(k_singletons, (int)(nwarps / SNG_WARPS), SNG_WARPS * 32,
+                    SNG_WARPS * 32 * SNG_TILE_LD * sizeof(double), c->wt, c->sng, c->cl[cur], c->probs,
                c->blocks, c->RP, c->RQ, c->arena[cur], c->W, c->Wsh, c->Werr, c->Wgap, c->Windex,
-               c->Zindex, c->sc, c->scratch, (long long)nmaxV);
+               c->Zindex, c->sc, c->scratch, (long long)nmaxV, stats);
       ncl = c->h_lc->n_cl;
       const size_t need = (size_t)c->h_lc->arena_need;
       if (ncl > 0 && need > c->capArena[nxt]) {
@@ -1958,6 +2270,7 @@ extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *s
   LAUNCH(k_scatter, L, 256, c->probs, c->Wp, c->Dp, c->Ep, c->Wout, c->D, c->E);
   CK(cudaMemcpyAsync(c->h_probs, c->probs, L * sizeof(ProbDev), cudaMemcpyDeviceToHost, st), "probs d2h");
   CK(cudaStreamSynchronize(st), "final sync");
+  if (c->prof) prof_flush(c);
 
   for (int k = 0; k < L; k++) {
     const ProbDev &h = c->h_probs[k];

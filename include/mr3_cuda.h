@@ -96,6 +96,25 @@ int  mr3_cuda_profile_read(mr3_cuda_ctx *ctx, int max, char *names, double *ms,
  * division-bound Sturm-count kernels. */
 int  mr3_cuda_fp64_peaks(int device, double *fma_tflops, double *div_gops);
 
+/* Eigenvectors of an L D L^T representation without any allocation.
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * code inside a device-memory budget owned by another allocator, or
+ * latency-critical loops that cannot afford cudaMalloc's implicit device
+ * synchronisation.  One twisted factorisation (dlar1v, twist index searched
+ * over 1..n) per eigenvalue lambda[j] of L D L^T; column j of Z gets the unit
+ * eigenvector, zero outside its support, Zsupp[2j..2j+1] the 1-based support.
+ * D (n), L (n-1), lambda (m), Z (ldz*m), Zsupp (2m) are device pointers;
+ * gaptol is dlar1v's support-truncation tolerance (0 keeps every entry).
+ * Scratch is one static device array of the library (16.8 MB per GPU), so
+ * n <= MR3_NOALLOC_NMAX; larger n, m < 0 or ldz < n return 1.  The first call
+ * on a device looks the array up (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race.  Returns 0 when the kernels were queued on `stream`. */
+#define MR3_NOALLOC_NMAX 2048
+int  mr3_cuda_eigvec_noalloc(int n, const double *D, const double *L, int m,
+                             const double *lambda, double gaptol, double *Z, int ldz,
+                             int *Zsupp, void *stream);
+
 /* Number of kernels launched by the last mr3_cuda_solve on this context. */
 long long mr3_cuda_last_launches(const mr3_cuda_ctx *ctx);
 

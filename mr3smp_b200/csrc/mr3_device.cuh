@@ -23,13 +23,13 @@
 //   P[i] = (D(i), D(i)L(i)^2)   read by every Sturm count (dlaneg)
 //   Q[i] = (L(i), D(i)L(i))     read in addition by the twisted factorization
 
-__device__ __forceinline__ int d_imin(int a, int b) { return a < b ? a : b; }
-__device__ __forceinline__ int d_imax(int a, int b) { return a > b ? a : b; }
+static __device__ __forceinline__ int d_imin(int a, int b) { return a < b ? a : b; }
+static __device__ __forceinline__ int d_imax(int a, int b) { return a > b ? a : b; }
 
 // Deterministic natural log: log(x) = e*ln2 + 2*atanh((m-1)/(m+1)) with the
 // atanh Taylor series to s^25 and the fdlibm hi/lo split of ln2.  Same
 // operations as the CPU copy used by the oracle, hence the same bits.
-__device__ __noinline__ double dv_log(double x) {
+static __device__ __noinline__ double dv_log(double x) {
   const double ln2_hi = 6.93147180369123816490e-01;
   const double ln2_lo = 1.90821492927058770002e-10;
   if (isnan(x) || x < 0.0) return __longlong_as_double(0x7ff8000000000000LL);
@@ -57,13 +57,13 @@ __device__ __noinline__ double dv_log(double x) {
 }
 
 // INT((LOG(a)-LOG(b))/LOG(2)) + 2: iteration cap of dlarrb/dlarrd/dlarrj.
-__device__ __forceinline__ int dv_itmax(double a, double b) {
+static __device__ __forceinline__ int dv_itmax(double a, double b) {
   return (int)((dv_log(a) - dv_log(b)) / dv_log(2.0)) + 2;
 }
 
 // Sturm count of T - x, IJOB=1 rule of dlaebz (SRC/LAPACK/odebz.f:255-270).
 // tp[j] = (d[j], e2[j-1]); tp[0].y unused.
-__device__ __noinline__ int dv_count_ijob1(int n, const double2 *__restrict__ tp,
+static __device__ __noinline__ int dv_count_ijob1(int n, const double2 *__restrict__ tp,
                                            double pivmin, double x) {
   double2 v = tp[0];
   double tmp = v.x - x;
@@ -79,7 +79,7 @@ __device__ __noinline__ int dv_count_ijob1(int n, const double2 *__restrict__ tp
 }
 
 // Sturm count, IJOB=2/3 rule of dlaebz's serial loop (odebz.f loop 90).
-__device__ __forceinline__ int dv_count_bisect(int n, const double2 *__restrict__ tp,
+static __device__ __forceinline__ int dv_count_bisect(int n, const double2 *__restrict__ tp,
                                                double pivmin, double c) {
   double2 v = tp[0];
   double tmp2 = v.x - c;
@@ -94,7 +94,7 @@ __device__ __forceinline__ int dv_count_bisect(int n, const double2 *__restrict_
 }
 
 // One interval of dlaebz IJOB=3 from the user-supplied point c.
-__device__ __noinline__ void dv_ijob3(int n, const double2 *__restrict__ tp, double pivmin,
+static __device__ __noinline__ void dv_ijob3(int n, const double2 *__restrict__ tp, double pivmin,
                                       double abstol, double reltol, int nitmax, int nval,
                                       double c, double *a, double *b, int *na, int *nb) {
   for (int it = 1; it <= nitmax; it++) {
@@ -110,7 +110,7 @@ __device__ __noinline__ void dv_ijob3(int n, const double2 *__restrict__ tp, dou
 
 // The interval of eigenvalue j under dlaebz IJOB=2 started from [a,b] with
 // counts (na,nb): midpoint bisection of that one interval (odebz.f 90-120).
-__device__ __noinline__ int dv_bisect_one(int n, const double2 *__restrict__ tp, double pivmin,
+static __device__ __noinline__ int dv_bisect_one(int n, const double2 *__restrict__ tp, double pivmin,
                                           double abstol, double reltol, int itmax, int j,
                                           double *a, double *b, int na, int nb, int *iters) {
   double c = 0.5 * (*a + *b);
@@ -128,7 +128,7 @@ __device__ __noinline__ int dv_bisect_one(int n, const double2 *__restrict__ tp,
 }
 
 // dlaneg (SRC/LAPACK/odneg.f:98-163) on packed rows P[(i)*ps]; r is 1-based.
-__device__ __noinline__ int dv_dlaneg(int n, const double2 *__restrict__ P, int ps, double sigma,
+static __device__ __noinline__ int dv_dlaneg(int n, const double2 *__restrict__ P, int ps, double sigma,
                                       int r) {
   const int blklen = 128;
   int negcnt = 0;
@@ -198,7 +198,7 @@ __device__ __noinline__ int dv_dlaneg(int n, const double2 *__restrict__ P, int 
 //   has_left: II > 1 (main-loop left gap is WGAP(II-1))
 //   w, werr: in/out; updated only if the interval went through the main loop
 // Returns the number of counts spent, or -1 if a widening loop hit its cap.
-__device__ __noinline__ int dv_dlarrb_one(int n, const double2 *__restrict__ R, int ps, int i,
+static __device__ __noinline__ int dv_dlarrb_one(int n, const double2 *__restrict__ R, int ps, int i,
                                           int first,
                                           int has_left, double rgap_own, double lgap_in,
                                           double rtol1, double rtol2, double pivmin,
@@ -246,7 +246,7 @@ __device__ __noinline__ int dv_dlarrb_one(int n, const double2 *__restrict__ R, 
 
 // x_k = 2*(s*a^k mod 2^48)/2^48 - 1: the k-th (1-based) number of dlarnv(2)
 // from the 48-bit seed s (SRC/LAPACK/odrnv.f, odruv.f).
-__device__ __forceinline__ double dv_lcg_uniform(uint64_t seed, uint64_t k) {
+static __device__ __forceinline__ double dv_lcg_uniform(uint64_t seed, uint64_t k) {
   const uint64_t mask = (1ULL << 48) - 1ULL;
   uint64_t acc = 1, base = MR3_LCG_A;
   while (k) {
@@ -260,7 +260,7 @@ __device__ __forceinline__ double dv_lcg_uniform(uint64_t seed, uint64_t k) {
 
 // Prefetch the L1 line holding *p (PTX prefetch.global.L1).  Only issued for
 // addresses inside the arrays being read.
-__device__ __forceinline__ void pf_l1(const void *p) {
+static __device__ __forceinline__ void pf_l1(const void *p) {
   asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
@@ -284,12 +284,12 @@ struct dlar1v_out {
   bool sawnan;
 };
 
-__device__ __forceinline__ double dv_zget(const double *X, const double *Y, int stride, int r,
+static __device__ __forceinline__ double dv_zget(const double *X, const double *Y, int stride, int r,
                                           int k) {
   return k < r ? X[(size_t)k * stride] : (k == r ? 1.0 : Y[(size_t)(k - 1) * stride]);
 }
 
-__device__ __noinline__ bool dv_r1v_passA(int n, double lambda, const double2 *__restrict__ P,
+static __device__ __noinline__ bool dv_r1v_passA(int n, double lambda, const double2 *__restrict__ P,
                                           const double2 *__restrict__ Q, int ps, double pivmin, int r1,
                                           int r2, double *X, double *Y, int stride, int *neg1o) {
   int neg1 = 0;
@@ -332,7 +332,7 @@ __device__ __noinline__ bool dv_r1v_passA(int n, double lambda, const double2 *_
 }
 
 // Progressive transform with the fused twist search.  Returns P(R1-1).
-__device__ __noinline__ double dv_r1v_passB(int n, double lambda, const double2 *__restrict__ P,
+static __device__ __noinline__ double dv_r1v_passB(int n, double lambda, const double2 *__restrict__ P,
                                             const double2 *__restrict__ Q, int ps, double pivmin, int r1,
                                             int r2, bool slow, double *Y, int stride, int *neg2o,
                                             int *rbest, double *best, bool *have) {
@@ -382,7 +382,7 @@ struct r1v_state {
   bool sawnan;
 };
 
-__device__ __noinline__ void dv_r1v_factor(int n, double lambda, const double2 *__restrict__ P,
+static __device__ __noinline__ void dv_r1v_factor(int n, double lambda, const double2 *__restrict__ P,
                                            const double2 *__restrict__ Q, int ps, double pivmin,
                                            bool wantnc, int r_in, double *X, double *Y,
                                            int stride, int *negcnt, r1v_state *st) {
@@ -419,7 +419,7 @@ __device__ __noinline__ void dv_r1v_factor(int n, double lambda, const double2 *
 // solve) and then from the smallest up (downward solve); a lane works on the
 // rows where it is active.  `active` says whether this lane has a solve to do.
 // Writes z over X/Y as described above and returns the outputs.
-__device__ __noinline__ void dv_r1v_solve(bool active, int n, const double2 *__restrict__ Q, int ps,
+static __device__ __noinline__ void dv_r1v_solve(bool active, int n, const double2 *__restrict__ Q, int ps,
                                           double gaptol, double *X, double *Y, int stride,
                                           const r1v_state &st, dlar1v_out *o) {
   const int r = active ? st.r : 0;
@@ -501,7 +501,7 @@ __device__ __noinline__ void dv_r1v_solve(bool active, int n, const double2 *__r
 // Parent rows: d = P[i].x, l = Q[i].x, ld = Q[i].y.  w/wgap/werr point at the
 // cluster's first eigenvalue (CLSTRT = 1, CLEND = clend).  dplus, lplus: out;
 // work: 2n scratch.  Returns the shift sigma.
-__device__ __noinline__ double dv_dlarrf(int n, const double2 *__restrict__ P,
+static __device__ __noinline__ double dv_dlarrf(int n, const double2 *__restrict__ P,
                                          const double2 *__restrict__ Q, int ps, int clend,
                                          const double *w, const double *wgap, const double *werr,
                                          double spdiam, double clgapl, double clgapr,
@@ -635,7 +635,7 @@ __device__ __noinline__ double dv_dlarrf(int n, const double2 *__restrict__ P,
 // One interval of dlarrj (SRC/LAPACK/odrrj.f:100-281): bisection on T to
 // relative tolerance rtol.  Intervals are independent (no gaps involved).
 // tp[j] = (d[j], e2[j-1]) of the unshifted matrix.
-__device__ __forceinline__ int dv_count_rrj(int n, const double2 *__restrict__ tp, double s) {
+static __device__ __forceinline__ int dv_count_rrj(int n, const double2 *__restrict__ tp, double s) {
   double dplus = tp[0].x - s;
   int cnt = (dplus < 0.0);
   for (int j = 1; j < n; j++) {
@@ -646,7 +646,7 @@ __device__ __forceinline__ int dv_count_rrj(int n, const double2 *__restrict__ t
   return cnt;
 }
 
-__device__ __noinline__ void dv_dlarrj_one(int n, const double2 *__restrict__ tp, int i,
+static __device__ __noinline__ void dv_dlarrj_one(int n, const double2 *__restrict__ tp, int i,
                                            double rtol, int maxitr, double *w, double *werr) {
   double left = *w - *werr, mid = *w, right = *w + *werr;
   double width = right - mid;

@@ -148,12 +148,17 @@ def cpu_reference(problems, budget_s: float, check: bool = True):
     return pairs / el, info
 
 
+def _workload(args):
+    return (f"mixed batch: {args.count} tridiagonals, n log-uniform [32,{args.nmax}], "
+            "25% 1-2-1, D,E uniform(-1,1), jobz=V range=A")
+
+
 def run_reference(args):
     ws, rank, local = _dist()
     if rank != 0:
         return 0
     from mr3smp_b200 import workloads as wl
-    probs = [(D, E) for D, E, _ in wl.mixed_batch(args.count, seed=args.seed)]
+    probs = [(D, E) for D, E, _ in wl.mixed_batch(args.count, seed=args.seed, nmax=args.nmax)]
     budget = args.ref_step_seconds
     for _ in range(args.warmup):
         cpu_reference(probs, budget / 4, check=False)
@@ -169,8 +174,7 @@ def run_reference(args):
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "eigenpairs/s",
            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "mixed batch: 4096 tridiagonals, n log-uniform [32,4096], "
-                                  "25% 1-2-1, jobz=V range=A", "problems": args.count,
+           "config": {"workload": _workload(args), "problems_per_gpu": args.count,
                       "seed": args.seed},
            "cpu_baseline": {**info, "value": value},
            "e2e": {"value": value, "unit": "eigenpairs/s", "h2d_bytes_per_step": 0,
@@ -190,6 +194,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--count", type=int, default=4096)
     ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--nmax", type=int, default=4096,
+                    help="largest n of the batch (smaller values make small profiling cases)")
     ap.add_argument("--percall-sample", type=int, default=128)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--ref-step-seconds", type=float, default=20.0)
@@ -215,7 +221,7 @@ def main():
     peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
 
     # workload: this rank's batch
-    batch = wl.mixed_batch(args.count, seed=args.seed + rank)
+    batch = wl.mixed_batch(args.count, seed=args.seed + rank, nmax=args.nmax)
     problems = [(D, E) for D, E, _ in batch]
     ns = [len(D) for D, E in problems]
     pairs_per_step = int(sum(ns))
@@ -274,12 +280,18 @@ def main():
     if L.mr3_cuda_fp64_peaks(local, ctypes.byref(a), ctypes.byref(b)) == 0:
         fma_tflops, div_gops = a.value, b.value
     groups = M.Solver.KERNEL_GROUPS
-    # kernel -> counter group; divisions per counted unit
+    # kernel family -> (counter group, divisions per counted unit); the two
+    # instantiations of the singleton round kernel are one family
+    fam = {}
+    for k, (kms, kc) in kern.items():
+        f = "k_sng_round" if k.startswith("k_sng_round") else k
+        a_, b_ = fam.get(f, (0.0, 0))
+        fam[f] = (a_ + kms, b_ + kc)
     kmap = {"k_bisect": (0, [1, 0, 0, 0]), "k_refine_root": (1, [0, 1, 0, 0]),
             "k_cl_ext": (2, [0, 1, 0, 0]), "k_cl_rrf": (2, [0, 0, 0, 1]),
-            "k_refine_cl": (3, [0, 1, 0, 0]), "k_singletons": (4, [0, 1, 2, 0])}
-    top = max(kern.items(), key=lambda kv: kv[1][0])
-    tname, (tms, tcnt) = top
+            "k_refine_cl": (3, [0, 1, 0, 0]), "k_sng_round": (4, [0, 0, 2, 0]),
+            "k_sng_bisect": (4, [0, 1, 0, 0])}
+    tname, (tms, tcnt) = max(fam.items(), key=lambda kv: kv[1][0])
     roof = None
     if tname in kmap:
         g, w = kmap[tname]
@@ -399,8 +411,7 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded numpy)",
-        "config": {"workload": "mixed batch: 4096 tridiagonals, n log-uniform [32,4096], "
-                               "25% 1-2-1, D,E uniform(-1,1), jobz=V range=A",
+        "config": {"workload": _workload(args),
                    "problems_per_gpu": args.count, "seed": args.seed,
                    "eigenpairs_per_step_per_gpu": pairs_per_step,
                    "z_bytes_per_step_per_gpu": zbytes,

@@ -77,6 +77,25 @@ int  mr3_cuda_copy2d(mr3_cuda_ctx *ctx, void *dst, size_t dpitch, const void *sr
                      size_t spitch, size_t width, size_t height, int dir);
 int  mr3_cuda_sync(mr3_cuda_ctx *ctx);
 
+/* Second stream of the context for copies that overlap the solves, and the
+ * events that order the two.  stream: MR3_STREAM_MAIN (the stream of the
+ * copies above and of solves given stream NULL) or MR3_STREAM_COPY.
+ * mr3_cuda_event: ev in 0..MR3_CUDA_EVENTS-1; when record_on >= 0 the event
+ * is recorded on that stream, then when wait_on >= 0 that stream waits for
+ * the event's last recording.  mr3_cuda_sync_all waits for both streams.
+ * mr3_cuda_host_ws: grow-only page-locked host buffer of the context (NULL
+ * on failure); its contents do not survive a call that grows it. */
+#define MR3_STREAM_MAIN 0
+#define MR3_STREAM_COPY 1
+#define MR3_CUDA_EVENTS 4
+int  mr3_cuda_copy_on(mr3_cuda_ctx *ctx, int stream, void *dst, const void *src, size_t bytes,
+                      int dir);
+int  mr3_cuda_copy2d_on(mr3_cuda_ctx *ctx, int stream, void *dst, size_t dpitch, const void *src,
+                        size_t spitch, size_t width, size_t height, int dir);
+int  mr3_cuda_event(mr3_cuda_ctx *ctx, int ev, int record_on, int wait_on);
+int  mr3_cuda_sync_all(mr3_cuda_ctx *ctx);
+void *mr3_cuda_host_ws(mr3_cuda_ctx *ctx, size_t bytes);
+
 /* Profiling switch: with on = 1 every kernel launch is bracketed by CUDA
  * events on the solve's stream and the kernels add their work to device
  * counters; the accumulators are reset by every call of this function. */

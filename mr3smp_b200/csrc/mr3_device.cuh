@@ -61,8 +61,14 @@ static __device__ __forceinline__ int dv_itmax(double a, double b) {
   return (int)((dv_log(a) - dv_log(b)) / dv_log(2.0)) + 2;
 }
 
+#ifndef MR3_U
+#define MR3_U 4     // rows per chunk of the software-pipelined sweeps
+#endif
+
 // Sturm count of T - x, IJOB=1 rule of dlaebz (SRC/LAPACK/odebz.f:255-270).
-// tp[j] = (d[j], e2[j-1]); tp[0].y unused.
+// tp[j] = (d[j], e2[j-1]); tp[0].y unused.  The threads of a warp count the
+// same matrix, so every load is a broadcast that L1 serves; the plain loop
+// is faster here than the chunked sweeps used for per-lane data.
 static __device__ __noinline__ int dv_count_ijob1(int n, const double2 *__restrict__ tp,
                                            double pivmin, double x) {
   double2 v = tp[0];
@@ -128,61 +134,152 @@ static __device__ __noinline__ int dv_bisect_one(int n, const double2 *__restric
 }
 
 // dlaneg (SRC/LAPACK/odneg.f:98-163) on packed rows P[(i)*ps]; r is 1-based.
+// U > 1: rows are read in chunks of U with the next chunk's loads issued
+// ahead of the current chunk's arithmetic (see the dlar1v sweeps below),
+// for representations that the threads of a warp do not share (cluster
+// groups in the level arenas); the NaN re-run of a 128-row block reads its
+// rows again.  U == 1: the plain row loop, best when a warp's threads all
+// read the same rows (a block's root representation), which L1 serves.
+template <int U>
 static __device__ __noinline__ int dv_dlaneg(int n, const double2 *__restrict__ P, int ps, double sigma,
                                       int r) {
+  static_assert(128 % U == 0, "chunks must not straddle the 128-row blocks");
   const int blklen = 128;
   int negcnt = 0;
   double t = -sigma;
-  for (int bj = 1; bj <= r - 1; bj += blklen) {
-    int jend = d_imin(bj + blklen - 1, r - 1);
-    int neg1 = 0;
-    double bsav = t;
-    for (int j = bj; j <= jend; j++) {
-      const double2 v = P[(size_t)(j - 1) * ps];
-      double dplus = v.x + t;
-      neg1 += (dplus < 0.0);
-      double tmp = t / dplus;
-      t = tmp * v.y - sigma;
-    }
-    if (isnan(t)) {
-      neg1 = 0;
-      t = bsav;
+  if constexpr (U == 1) {
+    for (int bj = 1; bj <= r - 1; bj += blklen) {
+      int jend = d_imin(bj + blklen - 1, r - 1);
+      int neg1 = 0;
+      double bsav = t;
       for (int j = bj; j <= jend; j++) {
         const double2 v = P[(size_t)(j - 1) * ps];
         double dplus = v.x + t;
         neg1 += (dplus < 0.0);
         double tmp = t / dplus;
-        if (isnan(tmp)) tmp = 1.0;
         t = tmp * v.y - sigma;
       }
+      if (isnan(t)) {
+        neg1 = 0;
+        t = bsav;
+        for (int j = bj; j <= jend; j++) {
+          const double2 v = P[(size_t)(j - 1) * ps];
+          double dplus = v.x + t;
+          neg1 += (dplus < 0.0);
+          double tmp = t / dplus;
+          if (isnan(tmp)) tmp = 1.0;
+          t = tmp * v.y - sigma;
+        }
+      }
+      negcnt += neg1;
     }
-    negcnt += neg1;
-  }
-  double p = P[(size_t)(n - 1) * ps].x - sigma;
-  for (int bj = n - 1; bj >= r; bj -= blklen) {
-    int jend = d_imax(bj - blklen + 1, r);
-    int neg2 = 0;
-    double bsav = p;
-    for (int j = bj; j >= jend; j--) {
-      const double2 v = P[(size_t)(j - 1) * ps];
-      double dminus = v.y + p;
-      neg2 += (dminus < 0.0);
-      double tmp = p / dminus;
-      p = tmp * v.x - sigma;
-    }
-    if (isnan(p)) {
-      neg2 = 0;
-      p = bsav;
+    double p = P[(size_t)(n - 1) * ps].x - sigma;
+    for (int bj = n - 1; bj >= r; bj -= blklen) {
+      int jend = d_imax(bj - blklen + 1, r);
+      int neg2 = 0;
+      double bsav = p;
       for (int j = bj; j >= jend; j--) {
         const double2 v = P[(size_t)(j - 1) * ps];
         double dminus = v.y + p;
         neg2 += (dminus < 0.0);
         double tmp = p / dminus;
-        if (isnan(tmp)) tmp = 1.0;
         p = tmp * v.x - sigma;
       }
+      if (isnan(p)) {
+        neg2 = 0;
+        p = bsav;
+        for (int j = bj; j >= jend; j--) {
+          const double2 v = P[(size_t)(j - 1) * ps];
+          double dminus = v.y + p;
+          neg2 += (dminus < 0.0);
+          double tmp = p / dminus;
+          if (isnan(tmp)) tmp = 1.0;
+          p = tmp * v.x - sigma;
+        }
+      }
+      negcnt += neg2;
     }
-    negcnt += neg2;
+    double gamma = (t + sigma) + p;
+    if (gamma < 0.0) negcnt++;
+    return negcnt;
+  }
+  if (r - 1 >= 1) {
+    const int last = r - 1;
+    double2 c[U], nx[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) c[u] = P[(size_t)(d_imin(1 + u, last) - 1) * ps];
+    for (int bj = 1; bj <= last; bj += blklen) {
+      const int jend = d_imin(bj + blklen - 1, last);
+      int neg1 = 0;
+      const double bsav = t;
+      for (int j0 = bj; j0 <= jend; j0 += U) {
+#pragma unroll
+        for (int u = 0; u < U; u++) nx[u] = P[(size_t)(d_imin(j0 + U + u, last) - 1) * ps];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          if (j0 + u <= jend) {
+            double dplus = c[u].x + t;
+            neg1 += (dplus < 0.0);
+            double tmp = t / dplus;
+            t = tmp * c[u].y - sigma;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) c[u] = nx[u];
+      }
+      if (isnan(t)) {
+        neg1 = 0;
+        t = bsav;
+        for (int j = bj; j <= jend; j++) {
+          const double2 v = P[(size_t)(j - 1) * ps];
+          double dplus = v.x + t;
+          neg1 += (dplus < 0.0);
+          double tmp = t / dplus;
+          if (isnan(tmp)) tmp = 1.0;
+          t = tmp * v.y - sigma;
+        }
+      }
+      negcnt += neg1;
+    }
+  }
+  double p = P[(size_t)(n - 1) * ps].x - sigma;
+  if (n - 1 >= r) {
+    double2 c[U], nx[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) c[u] = P[(size_t)(d_imax(n - 1 - u, r) - 1) * ps];
+    for (int bj = n - 1; bj >= r; bj -= blklen) {
+      const int jend = d_imax(bj - blklen + 1, r);
+      int neg2 = 0;
+      const double bsav = p;
+      for (int j0 = bj; j0 >= jend; j0 -= U) {
+#pragma unroll
+        for (int u = 0; u < U; u++) nx[u] = P[(size_t)(d_imax(j0 - U - u, r) - 1) * ps];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          if (j0 - u >= jend) {
+            double dminus = c[u].y + p;
+            neg2 += (dminus < 0.0);
+            double tmp = p / dminus;
+            p = tmp * c[u].x - sigma;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) c[u] = nx[u];
+      }
+      if (isnan(p)) {
+        neg2 = 0;
+        p = bsav;
+        for (int j = bj; j >= jend; j--) {
+          const double2 v = P[(size_t)(j - 1) * ps];
+          double dminus = v.y + p;
+          neg2 += (dminus < 0.0);
+          double tmp = p / dminus;
+          if (isnan(tmp)) tmp = 1.0;
+          p = tmp * v.x - sigma;
+        }
+      }
+      negcnt += neg2;
+    }
   }
   double gamma = (t + sigma) + p;
   if (gamma < 0.0) negcnt++;
@@ -198,6 +295,7 @@ static __device__ __noinline__ int dv_dlaneg(int n, const double2 *__restrict__ 
 //   has_left: II > 1 (main-loop left gap is WGAP(II-1))
 //   w, werr: in/out; updated only if the interval went through the main loop
 // Returns the number of counts spent, or -1 if a widening loop hit its cap.
+template <int U>
 static __device__ __noinline__ int dv_dlarrb_one(int n, const double2 *__restrict__ R, int ps, int i,
                                           int first,
                                           int has_left, double rgap_own, double lgap_in,
@@ -211,14 +309,14 @@ static __device__ __noinline__ int dv_dlarrb_one(int n, const double2 *__restric
   int negcnt, cap, status = 0;
   int nc = 0;
   for (cap = 0; cap < MR3_EXPAND_CAP; cap++) {
-    negcnt = dv_dlaneg(n, R, ps, left, r);
+    negcnt = dv_dlaneg<U>(n, R, ps, left, r);
     nc++;
     if (negcnt > i - 1) { left = left - back; back = 2.0 * back; } else break;
   }
   if (cap == MR3_EXPAND_CAP) status = -1;
   back = *werr;
   for (cap = 0; cap < MR3_EXPAND_CAP; cap++) {
-    negcnt = dv_dlaneg(n, R, ps, right, r);
+    negcnt = dv_dlaneg<U>(n, R, ps, right, r);
     nc++;
     if (negcnt < i) { right = right + back; back = 2.0 * back; } else break;
   }
@@ -235,12 +333,119 @@ static __device__ __noinline__ int dv_dlarrb_one(int n, const double2 *__restric
     tmp = fmax(fabs(left), fabs(right));
     cvrgd = fmax(rtol1 * gap, rtol2 * tmp);
     if (width <= cvrgd || width <= mnwdth || iter == maxitr) break;
-    negcnt = dv_dlaneg(n, R, ps, mid, r);
+    negcnt = dv_dlaneg<U>(n, R, ps, mid, r);
     *ncount += 1;
     if (negcnt <= i - 1) left = mid; else right = mid;
   }
   *w = 0.5 * (left + right);
   *werr = right - *w;
+  return status;
+}
+
+// dv_dlarrb_one for one interval per group of L lanes (L = 4, 8, 16 or 32,
+// the same for the whole warp; every lane calls it, the lanes of a group
+// with the same arguments, and they get the same results).  The bisection
+// midpoints of the next log2(L) steps form a binary tree whose nodes follow
+// from the current interval alone: lane t of the group evaluates the count
+// at node max(t,1) (heap numbering, computed along the node's path with the
+// same operations the sequential loop uses), then the group walks the tree
+// with the counts, applying the sequential loop's convergence test before
+// each step.  The widening loops are evaluated the same way, L/2 candidate
+// ends per side in one sweep.  The sequence of intervals is exactly the
+// sequential one.
+static __device__ __noinline__ int dv_dlarrb_tree(int L, int n, const double2 *__restrict__ R, int ps,
+                                           int i, int first, int has_left, double rgap_own,
+                                           double lgap_in, double rtol1, double rtol2,
+                                           double pivmin, int maxitr, int r, double *w,
+                                           double *werr, int *ncount) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int t = lane & (L - 1), g0 = lane - t, half = L >> 1;
+  const int depth = 31 - __clz(L);
+  const unsigned gbits = (L == 32) ? full : ((1u << L) - 1u);
+  const double mnwdth = 2.0 * pivmin;
+  double left = *w - *werr, right = *w + *werr;
+  double gap = fmin(first ? rgap_own : lgap_in, rgap_own);
+  int status = 0;
+  // widening: the first L/2 lanes hold the left end after 0..L/2-1 widening
+  // steps, the others the right end; the first candidate that passes is the
+  // end the sequential loop stops at
+  {
+    const int side = t >= half, k = t & (half - 1);
+    double xs0 = left, xs1 = right, bs0 = *werr, bs1 = *werr;
+    bool need0 = true, need1 = true;
+    int steps0 = 0, steps1 = 0;
+    while (__any_sync(full, need0 || need1)) {
+      double x = side ? xs1 : xs0, back = side ? bs1 : bs0;
+      for (int j = 0; j < k; j++) { x = side ? x + back : x - back; back = 2.0 * back; }
+      const bool mine = side ? need1 : need0;
+      int cnt = 0;
+      if (mine) cnt = dv_dlaneg<1>(n, R, ps, x, r);
+      const bool ok = mine && (side ? (cnt >= i) : (cnt <= i - 1));
+      const unsigned gb = (__ballot_sync(full, ok) >> g0) & gbits;
+      for (int sd = 0; sd < 2; sd++) {
+        const unsigned pass = (gb >> (half * sd)) & ((1u << half) - 1u);
+        const int k0 = pass ? __ffs(pass) - 1 : half - 1;
+        const double xsrc = __shfl_sync(full, x, g0 + half * sd + k0);
+        const double bsrc = __shfl_sync(full, back, g0 + half * sd + k0);
+        bool &need = sd ? need1 : need0;
+        double &xs = sd ? xs1 : xs0, &bs = sd ? bs1 : bs0;
+        int &steps = sd ? steps1 : steps0;
+        if (!need) continue;
+        if (pass) {
+          *ncount += k0 + 1;
+          xs = xsrc;
+          need = false;
+        } else {
+          *ncount += half;
+          xs = sd ? xsrc + bsrc : xsrc - bsrc;
+          bs = 2.0 * bsrc;
+          steps += half;
+          if (steps >= MR3_EXPAND_CAP) { status = -1; need = false; }
+        }
+      }
+    }
+    left = xs0;
+    right = xs1;
+  }
+  double width = 0.5 * fabs(left - right);
+  double tmp = fmax(fabs(left), fabs(right));
+  double cvrgd = fmax(rtol1 * gap, rtol2 * tmp);
+  const bool early = (width <= cvrgd || width <= mnwdth);   // W, WERR kept
+  bool done = early;
+  gap = fmin(has_left ? lgap_in : rgap_own, rgap_own);
+  int iter = 0;
+  const int node_t = t == 0 ? 1 : t;
+  while (__any_sync(full, !done)) {
+    double l = left, rr = right;
+    for (int b = 30 - __clz(node_t); b >= 0; b--) {
+      const double m = 0.5 * (l + rr);
+      if ((node_t >> b) & 1) l = m; else rr = m;
+    }
+    int cnt = 0;
+    if (!done) cnt = dv_dlaneg<1>(n, R, ps, 0.5 * (l + rr), r);
+    int node = 1;
+    for (int d = 0; d < depth; d++) {
+      const int c = __shfl_sync(full, cnt, g0 + node);
+      if (!done) {
+        const double mid = 0.5 * (left + right);
+        width = right - mid;
+        tmp = fmax(fabs(left), fabs(right));
+        cvrgd = fmax(rtol1 * gap, rtol2 * tmp);
+        if (width <= cvrgd || width <= mnwdth || iter == maxitr) {
+          done = true;
+        } else {
+          *ncount += 1;
+          if (c <= i - 1) { left = mid; node = 2 * node + 1; } else { right = mid; node = 2 * node; }
+          iter++;
+        }
+      }
+    }
+  }
+  if (!early) {
+    *w = 0.5 * (left + right);
+    *werr = right - *w;
+  }
   return status;
 }
 
@@ -264,13 +469,15 @@ static __device__ __forceinline__ void pf_l1(const void *p) {
   asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
-#define MR3_PF 16   // prefetch distance in rows
+#ifndef MR3_PF
+#define MR3_PF 16   // L1 prefetch distance in rows (0: none)
+#endif
 
 // dlar1v (SRC/LAPACK/odr1v.f:158-362) with B1 = 1, BN = n.  Each lane of a
 // warp runs its own eigenvector; the three sweeps (stationary transform,
 // progressive transform, back-substitution) run over the rows in lock-step
 // so every per-lane scratch access is one coalesced 256-byte row.
-// Scratch per lane: X[i*stride], Y[i*stride], i < n.
+// Scratch per lane: X[i*R1V_LD], Y[i*R1V_LD], i < n (lane-interleaved rows).
 //   stationary  : X[i] = LPLUS(i), Y[i] = S(i)
 //   progressive : Y[i] = UMINUS(i) once S(i) has been used; the twist search
 //                 runs inside this sweep from the top index down with a strict
@@ -278,36 +485,74 @@ static __device__ __forceinline__ void pf_l1(const void *p) {
 //                 scan with '<='
 //   solve       : z(k) for k < r in X[k], z(r) = 1, z(k) for k > r in Y[k-1]
 // r_in = 0 means "search the twist index over 1..n".
+//
+// The sweeps are latency chains (one division per row) whose inputs come
+// from memory that is mostly not in L1: the rows are read in chunks of MR3_U
+// rows, and the loads of the next chunk are issued before the current chunk
+// is computed, so a load's latency overlaps MR3_U rows of arithmetic.  The
+// arithmetic of every row is exactly that of the row-by-row recurrence.
+#define R1V_LD 32
+
 struct dlar1v_out {
   int negcnt, r, isupp1, isupp2;
   double ztz, mingma, nrminv, resid, rqcorr;
   bool sawnan;
 };
 
-static __device__ __forceinline__ double dv_zget(const double *X, const double *Y, int stride, int r,
-                                          int k) {
-  return k < r ? X[(size_t)k * stride] : (k == r ? 1.0 : Y[(size_t)(k - 1) * stride]);
+static __device__ __forceinline__ double dv_zget(const double *X, const double *Y, int r, int k) {
+  return k < r ? X[(size_t)k * R1V_LD] : (k == r ? 1.0 : Y[(size_t)(k - 1) * R1V_LD]);
 }
 
 static __device__ __noinline__ bool dv_r1v_passA(int n, double lambda, const double2 *__restrict__ P,
                                           const double2 *__restrict__ Q, int ps, double pivmin, int r1,
-                                          int r2, double *X, double *Y, int stride, int *neg1o) {
+                                          int r2, double *__restrict__ X, double *__restrict__ Y,
+                                          int *neg1o) {
+  constexpr int U = MR3_U;
   int neg1 = 0;
   double s = 0.0 - lambda;
   Y[0] = 0.0;
   bool sawnan = false;
-  for (int i = 1; i <= r2 - 1; i++) {
-    if (i + MR3_PF <= n - 1) { pf_l1(&P[(size_t)(i + MR3_PF - 1) * ps]); pf_l1(&Q[(size_t)(i + MR3_PF - 1) * ps]); }
-    const double dd = P[(size_t)(i - 1) * ps].x;
-    const double2 q = Q[(size_t)(i - 1) * ps];
-    double dplus = dd + s;
-    double lp = q.y / dplus;
-    X[(size_t)i * stride] = lp;
-    if (i <= r1 - 1) neg1 += (dplus < 0.0);
-    double si = s * lp * q.x;
-    Y[(size_t)i * stride] = si;
-    s = si - lambda;
-    if (i == r1 - 1 && isnan(s)) { sawnan = true; break; }
+  const int last = r2 - 1;   // rows 1..last
+  if (last >= 1) {
+    double cd[U], cl[U], cld[U], nd[U], nl[U], nld[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int i = d_imin(1 + u, last);
+      cd[u] = P[(size_t)(i - 1) * ps].x;
+      const double2 q = Q[(size_t)(i - 1) * ps];
+      cl[u] = q.x; cld[u] = q.y;
+    }
+    for (int i0 = 1; i0 <= last; i0 += U) {
+#pragma unroll
+      for (int u = 0; u < U; u++) {   // next chunk (clamped to the last row)
+        const int i = d_imin(i0 + U + u, last);
+        nd[u] = P[(size_t)(i - 1) * ps].x;
+        const double2 q = Q[(size_t)(i - 1) * ps];
+        nl[u] = q.x; nld[u] = q.y;
+        if (MR3_PF && i0 + u + MR3_PF <= last) {
+          pf_l1(&P[(size_t)(i0 + u + MR3_PF - 1) * ps]);
+          pf_l1(&Q[(size_t)(i0 + u + MR3_PF - 1) * ps]);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int i = i0 + u;
+        if (i <= last) {
+          double dplus = cd[u] + s;
+          double lp = cld[u] / dplus;
+          X[(size_t)i * R1V_LD] = lp;
+          if (i <= r1 - 1) neg1 += (dplus < 0.0);
+          double si = s * lp * cl[u];
+          Y[(size_t)i * R1V_LD] = si;
+          s = si - lambda;
+          // rows past R1-1 computed after a NaN are redone by the slow sweep
+          if (i == r1 - 1 && isnan(s)) sawnan = true;
+        }
+      }
+      if (sawnan) break;
+#pragma unroll
+      for (int u = 0; u < U; u++) { cd[u] = nd[u]; cl[u] = nl[u]; cld[u] = nld[u]; }
+    }
   }
   if (!sawnan) sawnan = isnan(s);
   if (sawnan) {
@@ -319,11 +564,11 @@ static __device__ __noinline__ bool dv_r1v_passA(int n, double lambda, const dou
       double dplus = pp.x + s;
       if (fabs(dplus) < pivmin) dplus = -pivmin;
       double lp = q.y / dplus;
-      X[(size_t)i * stride] = lp;
+      X[(size_t)i * R1V_LD] = lp;
       if (i <= r1 - 1) neg1 += (dplus < 0.0);
       double si = s * lp * q.x;
       if (lp == 0.0) si = pp.y;
-      Y[(size_t)i * stride] = si;
+      Y[(size_t)i * R1V_LD] = si;
       s = si - lambda;
     }
   }
@@ -331,78 +576,130 @@ static __device__ __noinline__ bool dv_r1v_passA(int n, double lambda, const dou
   return sawnan;
 }
 
-// Progressive transform with the fused twist search.  Returns P(R1-1).
-static __device__ __noinline__ double dv_r1v_passB(int n, double lambda, const double2 *__restrict__ P,
+// Progressive transform with the fused twist search, for the whole warp:
+// the lanes sweep the rows by absolute index from the largest N-1 of the
+// active lanes down to the smallest R1, each lane working on its own rows
+// (R1..N-1), so the per-lane scratch rows stay aligned across lanes when
+// the lanes' matrices differ in size.  Returns P(R1-1) of this lane.
+static __device__ __noinline__ double dv_r1v_passB(bool active, int n, double lambda,
+                                            const double2 *__restrict__ P,
                                             const double2 *__restrict__ Q, int ps, double pivmin, int r1,
-                                            int r2, bool slow, double *Y, int stride, int *neg2o,
+                                            int r2, bool slow, double *__restrict__ Y, int *neg2o,
                                             int *rbest, double *best, bool *have) {
+  constexpr int U = MR3_U;
   const double eps = MR3_EPS;
   int neg2 = 0;
-  double p = P[(size_t)(n - 1) * ps].x - lambda;   // P(n-1)
+  double p = 0.0;
   *have = false;
-  if (r2 == n && n > r1) {          // candidate r = n
-    double s = Y[(size_t)(n - 1) * stride];
-    double c = s + p;
-    if (c == 0.0) c = eps * s;
-    *best = c; *rbest = n; *have = true;
-  }
-  for (int i = n - 1; i >= r1; i--) {
-    if (i - MR3_PF >= 1) {
-      pf_l1(&P[(size_t)(i - MR3_PF - 1) * ps]);
-      pf_l1(&Q[(size_t)(i - MR3_PF - 1) * ps]);
-      pf_l1(&Y[(size_t)(i - MR3_PF - 1) * stride]);
+  const int top = n - 1;   // this lane's rows top..r1, descending
+  if (active) {
+    p = P[(size_t)(n - 1) * ps].x - lambda;   // P(n-1)
+    if (r2 == n && n > r1) {          // candidate r = n
+      double s = Y[(size_t)(n - 1) * R1V_LD];
+      double c = s + p;
+      if (c == 0.0) c = eps * s;
+      *best = c; *rbest = n; *have = true;
     }
-    const double2 pp = P[(size_t)(i - 1) * ps];
-    const double2 q = Q[(size_t)(i - 1) * ps];
-    const double sprev = Y[(size_t)(i - 1) * stride];
-    double dminus = pp.y + p;
-    if (slow && fabs(dminus) < pivmin) dminus = -pivmin;
-    double tmp = pp.x / dminus;
-    neg2 += (dminus < 0.0);
-    double um = q.x * tmp;
-    double pn = p * tmp - lambda;
-    if (slow && tmp == 0.0) pn = pp.x - lambda;
-    Y[(size_t)i * stride] = um;
-    p = pn;
-    if (i > r1 && i <= r2) {        // candidate r = i: S(i-1) + P(i-1)
-      double c = sprev + p;
-      if (c == 0.0) c = eps * sprev;
-      if (!*have || fabs(c) < fabs(*best)) { *best = c; *rbest = i; *have = true; }
+  }
+  const bool work = active && top >= r1;
+  const int topw = __reduce_max_sync(0xffffffffu, work ? top : 0);
+  const int r1w = __reduce_min_sync(0xffffffffu, work ? r1 : 0x7fffffff);
+  if (topw >= 1) {
+    double cpx[U], cpy[U], cqx[U], csp[U], npx[U], npy[U], nqx[U], nsp[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (work) {
+        const int i = d_imax(d_imin(topw - u, top), r1);
+        const double2 pp = P[(size_t)(i - 1) * ps];
+        cpx[u] = pp.x; cpy[u] = pp.y;
+        cqx[u] = Q[(size_t)(i - 1) * ps].x;
+        csp[u] = Y[(size_t)(i - 1) * R1V_LD];
+      }
+    }
+    for (int i0 = topw; i0 >= r1w; i0 -= U) {
+      // next chunk: rows i0-U .. i0-2U+1, none of which this chunk writes
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        if (work) {
+          const int i = d_imax(d_imin(i0 - U - u, top), r1);
+          const double2 pp = P[(size_t)(i - 1) * ps];
+          npx[u] = pp.x; npy[u] = pp.y;
+          nqx[u] = Q[(size_t)(i - 1) * ps].x;
+          nsp[u] = Y[(size_t)(i - 1) * R1V_LD];
+          const int f = i0 - u - MR3_PF;
+          if (MR3_PF && f >= r1 && f <= top) {
+            pf_l1(&P[(size_t)(f - 1) * ps]);
+            pf_l1(&Q[(size_t)(f - 1) * ps]);
+            pf_l1(&Y[(size_t)(f - 1) * R1V_LD]);
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int i = i0 - u;
+        if (work && i >= r1 && i <= top) {
+          double dminus = cpy[u] + p;
+          if (slow && fabs(dminus) < pivmin) dminus = -pivmin;
+          double tmp = cpx[u] / dminus;
+          neg2 += (dminus < 0.0);
+          double um = cqx[u] * tmp;
+          double pn = p * tmp - lambda;
+          if (slow && tmp == 0.0) pn = cpx[u] - lambda;
+          Y[(size_t)i * R1V_LD] = um;
+          p = pn;
+          if (i > r1 && i <= r2) {        // candidate r = i: S(i-1) + P(i-1)
+            const double sprev = csp[u];
+            double c = sprev + p;
+            if (c == 0.0) c = eps * sprev;
+            if (!*have || fabs(c) < fabs(*best)) { *best = c; *rbest = i; *have = true; }
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) { cpx[u] = npx[u]; cpy[u] = npy[u]; cqx[u] = nqx[u]; csp[u] = nsp[u]; }
     }
   }
   *neg2o = neg2;
   return p;
 }
 
-// The two factorisation sweeps and the twist choice of dlar1v.  Leaves the
-// lane's state for dv_r1v_solve.
+// The two factorisation sweeps and the twist choice of dlar1v, for the
+// whole warp (every lane calls it; `active` lanes have a factorisation to
+// do).  Leaves the lane's state for dv_r1v_solve.
 struct r1v_state {
   int r;
   double mingma;
   bool sawnan;
 };
 
-static __device__ __noinline__ void dv_r1v_factor(int n, double lambda, const double2 *__restrict__ P,
+static __device__ __noinline__ void dv_r1v_factor(bool active, int n, double lambda,
+                                           const double2 *__restrict__ P,
                                            const double2 *__restrict__ Q, int ps, double pivmin,
                                            bool wantnc, int r_in, double *X, double *Y,
-                                           int stride, int *negcnt, r1v_state *st) {
+                                           int *negcnt, r1v_state *st) {
   const double eps = MR3_EPS;
-  int r1, r2, neg1, neg2, rbest = 0;
-  if (r_in == 0) { r1 = 1; r2 = n; } else { r1 = r_in; r2 = r_in; }
-  bool sawnan1 = dv_r1v_passA(n, lambda, P, Q, ps, pivmin, r1, r2, X, Y, stride, &neg1);
+  int r1 = 1, r2 = n, neg1 = 0, neg2 = 0, rbest = 0;
+  if (r_in != 0) { r1 = r_in; r2 = r_in; }
+  bool sawnan1 = false;
+  if (active) sawnan1 = dv_r1v_passA(n, lambda, P, Q, ps, pivmin, r1, r2, X, Y, &neg1);
   double best = 0.0;
-  bool have;
-  double pr1 = dv_r1v_passB(n, lambda, P, Q, ps, pivmin, r1, r2, false, Y, stride, &neg2, &rbest,
+  bool have = false;
+  double pr1 = dv_r1v_passB(active, n, lambda, P, Q, ps, pivmin, r1, r2, false, Y, &neg2, &rbest,
                             &best, &have);
-  bool sawnan2 = isnan(pr1);
-  if (sawnan2) {
+  bool sawnan2 = active && isnan(pr1);
+  if (__any_sync(0xffffffffu, sawnan2)) {
     // S was overwritten by UMINUS; recompute the stationary sweep (same bits)
     // and run the slow progressive sweep
-    dv_r1v_passA(n, lambda, P, Q, ps, pivmin, r1, r2, X, Y, stride, &neg1);
-    pr1 = dv_r1v_passB(n, lambda, P, Q, ps, pivmin, r1, r2, true, Y, stride, &neg2, &rbest, &best,
-                       &have);
+    if (sawnan2) dv_r1v_passA(n, lambda, P, Q, ps, pivmin, r1, r2, X, Y, &neg1);
+    int n2b = 0, rbb = 0;
+    double bb = 0.0;
+    bool hb = false;
+    double pb = dv_r1v_passB(sawnan2, n, lambda, P, Q, ps, pivmin, r1, r2, true, Y, &n2b, &rbb,
+                             &bb, &hb);
+    if (sawnan2) { pr1 = pb; neg2 = n2b; rbest = rbb; best = bb; have = hb; }
   }
-  double sr1 = Y[(size_t)(r1 - 1) * stride];
+  if (!active) return;
+  double sr1 = Y[(size_t)(r1 - 1) * R1V_LD];
   double mg = sr1 + pr1;
   if (mg < 0.0) neg1++;
   *negcnt = wantnc ? neg1 + neg2 : -1;
@@ -416,71 +713,127 @@ static __device__ __noinline__ void dv_r1v_factor(int n, double lambda, const do
 
 // Back-substitution N^T z = e_r of dlar1v (odr1v.f:285-355) for a whole warp
 // in lock-step: rows are visited from the largest twist index down (upward
-// solve) and then from the smallest up (downward solve); a lane works on the
-// rows where it is active.  `active` says whether this lane has a solve to do.
-// Writes z over X/Y as described above and returns the outputs.
+// solve) and then from the smallest up to the largest N-1 (downward solve);
+// a lane works on its own rows.  `active` says whether this lane has a
+// solve to do.  Writes z over X/Y as described above and returns the
+// outputs.  Rows are read in chunks as in the factorisation sweeps; a row's
+// LPLUS/UMINUS is read before the row is overwritten with z.
 static __device__ __noinline__ void dv_r1v_solve(bool active, int n, const double2 *__restrict__ Q, int ps,
-                                          double gaptol, double *X, double *Y, int stride,
+                                          double gaptol, double *X, double *Y,
                                           const r1v_state &st, dlar1v_out *o) {
+  constexpr int U = MR3_U;
   const int r = active ? st.r : 0;
   const int rmax = __reduce_max_sync(0xffffffffu, active ? r : 0);
   int rmin = __reduce_min_sync(0xffffffffu, active ? r : 0x7fffffff);
+  const int nw = __reduce_max_sync(0xffffffffu, active ? n : 0);
   int is1 = 1, is2 = n;
   double ztz = 1.0;
   const bool slow = active && st.sawnan;
   // upward solve: i = r-1 .. 1
   bool go = active;
   double zp = 1.0;
-  for (int i = rmax - 1; i >= 1; i--) {
-    if (!__any_sync(0xffffffffu, go)) break;
-    if (i - MR3_PF >= 1) pf_l1(&X[(size_t)(i - MR3_PF) * stride]);
-    if (go && i < r) {
-      double zi;
-      if (!slow) {
-        zi = -(X[(size_t)i * stride] * zp);
-      } else {
-        double zi1 = dv_zget(X, Y, stride, r, i + 1);
-        if (zi1 == 0.0) zi = -(Q[(size_t)i * ps].y / Q[(size_t)(i - 1) * ps].y) * dv_zget(X, Y, stride, r, i + 2);
-        else zi = -(X[(size_t)i * stride] * zi1);
-        zp = zi1;
+  if (rmax - 1 >= 1) {
+    double cx[U], cq[U], nx[U], nq[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (active) {
+        const int i = d_imax(d_imin(rmax - 1 - u, n - 1), 1);
+        cx[u] = X[(size_t)i * R1V_LD];
+        cq[u] = Q[(size_t)(i - 1) * ps].y;
       }
-      if ((fabs(zi) + fabs(zp)) * fabs(Q[(size_t)(i - 1) * ps].y) < gaptol) {
-        X[(size_t)i * stride] = 0.0;
-        is1 = i + 1;
-        go = false;
-      } else {
-        ztz = ztz + zi * zi;
-        X[(size_t)i * stride] = zi;
-        zp = zi;
+    }
+    for (int i0 = rmax - 1; i0 >= 1; i0 -= U) {
+      if (!__any_sync(0xffffffffu, go)) break;
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        if (active) {
+          const int i = d_imax(d_imin(i0 - U - u, n - 1), 1);
+          nx[u] = X[(size_t)i * R1V_LD];
+          nq[u] = Q[(size_t)(i - 1) * ps].y;
+          const int f = i0 - u - MR3_PF;
+          if (MR3_PF && f >= 1 && f < r) pf_l1(&X[(size_t)f * R1V_LD]);
+        }
       }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int i = i0 - u;
+        if (i >= 1 && go && i < r) {
+          double zi;
+          if (!slow) {
+            zi = -(cx[u] * zp);
+          } else {
+            double zi1 = dv_zget(X, Y, r, i + 1);
+            if (zi1 == 0.0) zi = -(Q[(size_t)i * ps].y / cq[u]) * dv_zget(X, Y, r, i + 2);
+            else zi = -(cx[u] * zi1);
+            zp = zi1;
+          }
+          if ((fabs(zi) + fabs(zp)) * fabs(cq[u]) < gaptol) {
+            X[(size_t)i * R1V_LD] = 0.0;
+            is1 = i + 1;
+            go = false;
+          } else {
+            ztz = ztz + zi * zi;
+            X[(size_t)i * R1V_LD] = zi;
+            zp = zi;
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) { cx[u] = nx[u]; cq[u] = nq[u]; }
     }
   }
   // downward solve: i = r .. n-1
   go = active;
   double zc = 1.0;
-  if (rmin == 0x7fffffff) rmin = n;
-  for (int i = rmin; i <= n - 1; i++) {
-    if (!__any_sync(0xffffffffu, go)) break;
-    if (i + MR3_PF <= n - 1) pf_l1(&Y[(size_t)(i + MR3_PF) * stride]);
-    if (go && i >= r) {
-      double zn;
-      if (!slow) {
-        zn = -(Y[(size_t)i * stride] * zc);
-      } else {
-        double zci = dv_zget(X, Y, stride, r, i);
-        if (zci == 0.0) zn = -(Q[(size_t)(i - 2) * ps].y / Q[(size_t)(i - 1) * ps].y) * dv_zget(X, Y, stride, r, i - 1);
-        else zn = -(Y[(size_t)i * stride] * zci);
-        zc = zci;
+  if (rmin == 0x7fffffff) rmin = nw;
+  if (rmin <= nw - 1) {
+    double cy[U], cq[U], ny[U], nq[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (active) {
+        const int i = d_imax(d_imin(rmin + u, n - 1), 1);
+        cy[u] = Y[(size_t)i * R1V_LD];
+        cq[u] = Q[(size_t)(i - 1) * ps].y;
       }
-      if ((fabs(zc) + fabs(zn)) * fabs(Q[(size_t)(i - 1) * ps].y) < gaptol) {
-        Y[(size_t)i * stride] = 0.0;
-        is2 = i;
-        go = false;
-      } else {
-        ztz = ztz + zn * zn;
-        Y[(size_t)i * stride] = zn;
-        zc = zn;
+    }
+    for (int i0 = rmin; i0 <= nw - 1; i0 += U) {
+      if (!__any_sync(0xffffffffu, go)) break;
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        if (active) {
+          const int i = d_imax(d_imin(i0 + U + u, n - 1), 1);
+          ny[u] = Y[(size_t)i * R1V_LD];
+          nq[u] = Q[(size_t)(i - 1) * ps].y;
+          const int f = i0 + u + MR3_PF;
+          if (MR3_PF && f >= r && f <= n - 1) pf_l1(&Y[(size_t)f * R1V_LD]);
+        }
       }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int i = i0 + u;
+        if (i <= n - 1 && go && i >= r) {
+          double zn;
+          if (!slow) {
+            zn = -(cy[u] * zc);
+          } else {
+            double zci = dv_zget(X, Y, r, i);
+            if (zci == 0.0) zn = -(Q[(size_t)(i - 2) * ps].y / cq[u]) * dv_zget(X, Y, r, i - 1);
+            else zn = -(cy[u] * zci);
+            zc = zci;
+          }
+          if ((fabs(zc) + fabs(zn)) * fabs(cq[u]) < gaptol) {
+            Y[(size_t)i * R1V_LD] = 0.0;
+            is2 = i;
+            go = false;
+          } else {
+            ztz = ztz + zn * zn;
+            Y[(size_t)i * R1V_LD] = zn;
+            zc = zn;
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) { cy[u] = ny[u]; cq[u] = nq[u]; }
     }
   }
   if (active) {

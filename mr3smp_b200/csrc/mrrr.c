@@ -91,18 +91,37 @@ static int ncols_of(const mr3_host_prob *h, int jz, int rg)
 
 static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+/* Batches whose eigenvectors exceed PIPE_MIN_BYTES are solved in chunks of
+ * consecutive problems holding about PIPE_CHUNK_BYTES of Z each, so that the
+ * device Z buffers stay within memory; the device-to-host copy of one
+ * chunk's Z (on the context's copy stream) runs while the next chunk is
+ * solved.  Two device Z buffers alternate; a chunk's solve waits for the
+ * copies out of the buffer it reuses.  The device solves a large batch much
+ * faster per eigenpair than a small one, so smaller chunks lose more in the
+ * solves than the overlap wins (a 56 GB batch took 2.5 s whole and 3.1 s in
+ * three chunks); chunking is for capacity only.  MR3_PIPE_BYTES in the
+ * environment replaces both sizes (tests use it to chunk small batches). */
+#define PIPE_MIN_BYTES ((size_t)80 << 30)
+#define PIPE_CHUNK_BYTES ((size_t)40 << 30)
+#define PIPE_MAX_CHUNKS 16
+
 int mr3_batched(int nprob, mr3_host_prob *hp)
 {
-  int i, slot, rc = MR3_OK, worst = 0;
+  int i, c, slot, rc = MR3_OK, worst = 0, nchunk = 1;
+  int cbeg[PIPE_MAX_CHUNKS + 1];
   mr3_cuda_ctx *ctx;
   mr3_cuda_prob *dp;
-  size_t nrow = 0, nz = 0, nzs = 0;
-  char *base;
-  double *dD, *dE, *dW, *dZ;
+  size_t nrow = 0, nzs = 0, ztot = 0, zmax = 0, small, pipe_min, pipe_chunk;
+  size_t *zb, *orow, *ozs;
+  char *base, *stage;
+  double *dD, *dE, *dW, *dZb[2] = {NULL, NULL};
   int *dZs;
   if (nprob <= 0) return 0;
   dp = (mr3_cuda_prob *)calloc((size_t)nprob, sizeof(mr3_cuda_prob));
-  if (!dp) return MR3_EMISC;
+  zb = (size_t *)calloc(3 * (size_t)nprob, sizeof(size_t));
+  if (!dp || !zb) { free(dp); free(zb); return MR3_EMISC; }
+  orow = zb + nprob;
+  ozs = orow + nprob;
   for (i = 0; i < nprob; i++) {
     mr3_host_prob *h = &hp[i];
     int jz = job_code(h->jobz), rg = range_code(h->range);
@@ -113,44 +132,108 @@ int mr3_batched(int nprob, mr3_host_prob *hp)
     dp[i].jobz = ok ? jz : -1;
     dp[i].range = ok ? rg : -1;
     if (!ok) continue;
+    orow[i] = nrow;
+    ozs[i] = nzs;
     nrow += align_up((size_t)h->n, 32);
-    nz += (size_t)h->n * (size_t)ncols_of(h, jz, rg);
     nzs += align_up(2 * (size_t)h->n, 64);
+    zb[i] = (size_t)h->n * (size_t)ncols_of(h, jz, rg) * sizeof(double);
+    ztot += zb[i];
+  }
+  /* chunk boundaries: consecutive problems, about equal Z bytes */
+  cbeg[0] = 0;
+  {
+    const char *ev = getenv("MR3_PIPE_BYTES");
+    long long v = ev ? atoll(ev) : 0;
+    pipe_min = v > 0 ? (size_t)v : PIPE_MIN_BYTES;
+    pipe_chunk = v > 0 ? (size_t)v : PIPE_CHUNK_BYTES;
+  }
+  if (ztot > pipe_min) {
+    size_t acc = 0, target;
+    nchunk = (int)((ztot + pipe_chunk - 1) / pipe_chunk);
+    if (nchunk > PIPE_MAX_CHUNKS) nchunk = PIPE_MAX_CHUNKS;
+    if (nchunk > nprob) nchunk = nprob;
+    target = ztot / (size_t)nchunk;
+    c = 1;
+    for (i = 0; i < nprob && c < nchunk; i++) {
+      acc += zb[i];
+      if (acc >= target * (size_t)c) cbeg[c++] = i + 1;
+    }
+    nchunk = c;
+  }
+  cbeg[nchunk] = nprob;
+  for (c = 0; c < nchunk; c++) {
+    size_t z = 0;
+    for (i = cbeg[c]; i < cbeg[c + 1]; i++) z += zb[i];
+    if (z > zmax) zmax = z;
   }
   slot = pool_acquire();
-  if (slot < 0) { free(dp); return MR3_EMISC; }
+  if (slot < 0) { free(dp); free(zb); return MR3_EMISC; }
   ctx = g_pool[slot].ctx;
-  base = (char *)mr3_cuda_ws(ctx, 0, 3 * nrow * sizeof(double) + nzs * sizeof(int) + 1024);
-  dZ = (double *)mr3_cuda_ws(ctx, 1, nz * sizeof(double) + 256);
-  if (!base || !dZ) { rc = MR3_EMISC; goto done; }
+  /* device layout of the small arrays, mirrored by the staging buffer:
+   * D | E | W (nrow doubles each) | Zsupp (nzs ints) */
+  small = 3 * nrow * sizeof(double) + nzs * sizeof(int);
+  base = (char *)mr3_cuda_ws(ctx, 0, small + 1024);
+  dZb[0] = (double *)mr3_cuda_ws(ctx, 1, zmax + 256);
+  if (nchunk > 1) dZb[1] = (double *)mr3_cuda_ws(ctx, 2, zmax + 256);
+  stage = (char *)mr3_cuda_host_ws(ctx, small + 1024);
+  if (!base || !dZb[0] || (nchunk > 1 && !dZb[1]) || !stage) { rc = MR3_EMISC; goto done; }
   dD = (double *)base;
   dE = dD + nrow;
   dW = dE + nrow;
   dZs = (int *)(dW + nrow);
-  {
-    size_t orow = 0, oz = 0, ozs = 0;
-    for (i = 0; i < nprob; i++) {
+  for (i = 0; i < nprob; i++) {
+    mr3_host_prob *h = &hp[i];
+    mr3_cuda_prob *q = &dp[i];
+    q->n = h->n;
+    q->il = h->il; q->iu = h->iu; q->tryrac = h->tryrac;
+    q->vl = h->vl; q->vu = h->vu;
+    if (q->jobz < 0) continue;
+    q->D = dD + orow[i]; q->E = dE + orow[i]; q->W = dW + orow[i];
+    q->ldz = h->n;
+    q->Zsupp = (q->jobz == MR3_JOB_V) ? dZs + ozs[i] : NULL;
+    memcpy((double *)stage + orow[i], h->D, (size_t)h->n * sizeof(double));
+    memcpy((double *)stage + nrow + orow[i], h->E, (size_t)h->n * sizeof(double));
+  }
+  if (mr3_cuda_copy(ctx, base, stage, 2 * nrow * sizeof(double), 0) != MR3_OK) {
+    rc = MR3_EMISC;
+    goto done;
+  }
+  for (c = 0; c < nchunk; c++) {
+    double *zbuf = dZb[c & 1];
+    size_t oz = 0;
+    for (i = cbeg[c]; i < cbeg[c + 1]; i++) {
+      if (dp[i].jobz < 0) continue;
+      dp[i].Z = (dp[i].jobz == MR3_JOB_V) ? zbuf + oz / sizeof(double) : NULL;
+      oz += zb[i];
+    }
+    /* the buffer's previous chunk must have left it */
+    if (c >= 2 && mr3_cuda_event(ctx, c & 1, -1, MR3_STREAM_MAIN) != MR3_OK) {
+      rc = MR3_EMISC;
+      goto done;
+    }
+    if (mr3_cuda_solve(ctx, cbeg[c + 1] - cbeg[c], dp + cbeg[c], NULL) != MR3_OK ||
+        mr3_cuda_event(ctx, 2, MR3_STREAM_MAIN, MR3_STREAM_COPY) != MR3_OK) {
+      rc = MR3_EMISC;
+      goto done;
+    }
+    for (i = cbeg[c]; i < cbeg[c + 1]; i++) {
       mr3_host_prob *h = &hp[i];
       mr3_cuda_prob *q = &dp[i];
-      q->n = h->n;
-      q->il = h->il; q->iu = h->iu; q->tryrac = h->tryrac;
-      q->vl = h->vl; q->vu = h->vu;
-      if (q->jobz < 0) continue;
-      q->D = dD + orow; q->E = dE + orow; q->W = dW + orow;
-      q->ldz = h->n;
-      q->Z = (q->jobz == MR3_JOB_V) ? dZ + oz : NULL;
-      q->Zsupp = (q->jobz == MR3_JOB_V) ? dZs + ozs : NULL;
-      orow += align_up((size_t)h->n, 32);
-      oz += (size_t)h->n * (size_t)ncols_of(h, q->jobz, q->range);
-      ozs += align_up(2 * (size_t)h->n, 64);
-      if (mr3_cuda_copy(ctx, q->D, h->D, (size_t)h->n * sizeof(double), 0) != MR3_OK ||
-          mr3_cuda_copy(ctx, q->E, h->E, (size_t)h->n * sizeof(double), 0) != MR3_OK) {
+      if (q->jobz != MR3_JOB_V || q->info != MR3_OK || q->m <= 0) continue;
+      if (mr3_cuda_copy2d_on(ctx, MR3_STREAM_COPY, h->Z, (size_t)h->ldz * sizeof(double), q->Z,
+                             (size_t)q->ldz * sizeof(double), (size_t)h->n * sizeof(double),
+                             (size_t)q->m, 1) != MR3_OK) {
         rc = MR3_EMISC;
         goto done;
       }
     }
+    if (mr3_cuda_event(ctx, c & 1, MR3_STREAM_COPY, -1) != MR3_OK) { rc = MR3_EMISC; goto done; }
   }
-  if (mr3_cuda_solve(ctx, nprob, dp, NULL) != MR3_OK) { rc = MR3_EMISC; goto done; }
+  /* W, D, E and Zsupp of all problems in one copy, then to the callers' arrays */
+  if (mr3_cuda_copy(ctx, stage, base, small, 1) != MR3_OK || mr3_cuda_sync_all(ctx) != MR3_OK) {
+    rc = MR3_EMISC;
+    goto done;
+  }
   for (i = 0; i < nprob; i++) {
     mr3_host_prob *h = &hp[i];
     mr3_cuda_prob *q = &dp[i];
@@ -162,34 +245,23 @@ int mr3_batched(int nprob, mr3_host_prob *hp)
     h->il_out = q->il_out; h->iu_out = q->iu_out;
     h->tryrac_out = q->tryrac_out;
     if (q->info != MR3_OK || q->jobz == MR3_JOB_C) continue;
-    if (h->n == 1) {   /* 1x1: nothing was overwritten on the device */
-      if (q->m > 0) {
-        mr3_cuda_copy(ctx, h->W, q->W, sizeof(double), 1);
-        if (q->jobz == MR3_JOB_V) {
-          mr3_cuda_copy(ctx, h->Z, q->Z, sizeof(double), 1);
-          mr3_cuda_copy(ctx, h->Zsupp, q->Zsupp, 2 * sizeof(int), 1);
-        }
-      }
-      continue;
+    if (q->m > 0) memcpy(h->W, (double *)stage + 2 * nrow + orow[i], (size_t)q->m * sizeof(double));
+    if (h->n > 1) {   /* a 1x1 problem's D and E are left as they were */
+      memcpy(h->D, (double *)stage + orow[i], (size_t)h->n * sizeof(double));
+      memcpy(h->E, (double *)stage + nrow + orow[i], (size_t)h->n * sizeof(double));
     }
-    mr3_cuda_copy(ctx, h->W, q->W, (size_t)q->m * sizeof(double), 1);
-    mr3_cuda_copy(ctx, h->D, q->D, (size_t)h->n * sizeof(double), 1);
-    mr3_cuda_copy(ctx, h->E, q->E, (size_t)h->n * sizeof(double), 1);
-    if (q->jobz == MR3_JOB_V && q->m > 0) {
-      mr3_cuda_copy2d(ctx, h->Z, (size_t)h->ldz * sizeof(double), q->Z,
-                      (size_t)q->ldz * sizeof(double), (size_t)h->n * sizeof(double),
-                      (size_t)q->m, 1);
-      mr3_cuda_copy(ctx, h->Zsupp, q->Zsupp, 2 * (size_t)q->m * sizeof(int), 1);
-    }
+    if (q->jobz == MR3_JOB_V && q->m > 0)
+      memcpy(h->Zsupp, (int *)((double *)stage + 3 * nrow) + ozs[i], 2 * (size_t)q->m * sizeof(int));
   }
-  if (mr3_cuda_sync(ctx) != MR3_OK) rc = MR3_EMISC;
 done:
+  if (rc != MR3_OK) mr3_cuda_sync_all(ctx);
   pool_release(slot);
   for (i = 0; i < nprob; i++) {
-    if (rc != MR3_OK && hp[i].info == MR3_OK) hp[i].info = MR3_EMISC;
+    if (rc != MR3_OK) hp[i].info = dp[i].jobz < 0 ? MR3_EARG : MR3_EMISC;
     if (hp[i].info > worst) worst = hp[i].info;
   }
   free(dp);
+  free(zb);
   return worst;
 }
 

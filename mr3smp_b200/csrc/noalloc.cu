@@ -76,16 +76,16 @@ k_na_vec(int n, int m, const double *lambda, double gaptol, double *Z, int ldz, 
     r1v_state st;
     st.r = 0; st.mingma = 0.0; st.sawnan = false;
     int negc = 0;
-    if (active)
-      dv_r1v_factor(n, lambda[v], P, Q, 1, MR3_SAFMIN, false, 0, X, Y, 32, &negc, &st);
+    dv_r1v_factor(active, n, active ? lambda[v] : 0.0, P, Q, 1, MR3_SAFMIN, false, 0, X, Y, &negc,
+                  &st);
     dlar1v_out o;
     o.isupp1 = 1; o.isupp2 = n; o.nrminv = 0.0; o.r = 0;
-    dv_r1v_solve(active, n, Q, 1, gaptol, X, Y, 32, st, &o);
+    dv_r1v_solve(active, n, Q, 1, gaptol, X, Y, st, &o);
     if (active) {
       double *zc = Z + (size_t)v * ldz;
       for (int k = 1; k <= n; k++) {
         double val = 0.0;
-        if (k >= o.isupp1 && k <= o.isupp2) val = dv_zget(X, Y, 32, o.r, k) * o.nrminv;
+        if (k >= o.isupp1 && k <= o.isupp2) val = dv_zget(X, Y, o.r, k) * o.nrminv;
         zc[k - 1] = val;
       }
       Zsupp[2 * v] = o.isupp1;

@@ -75,9 +75,6 @@ struct SngDev {
   double lgap;
 };
 
-struct WTask {
-  int first, count;
-};
 
 // Clusters of one level and their arena need (one record per level parity).
 struct LevelCounters {
@@ -87,7 +84,10 @@ struct LevelCounters {
 
 // Singleton queue of the level being processed.
 struct SngCounters {
-  int n_sng, n_wt, wt_next, n_unit;
+  int n_sng, n_unit;
+  int act_n[2], act_next[2];   // round lists: entries, next entry to take
+  int bs_n, bs_next, err, nin; // bisection list; err: a list outlived the
+                               // rounds; nin: entries of this round's list
 };
 
 struct Tol {
@@ -765,7 +765,7 @@ __device__ __forceinline__ unsigned long long refine_root_body(int s, const Prob
   const double rtol1 = onlyW ? 4.0 * MR3_EPS : tol.rtol1;
   const double rtol2 = onlyW ? 4.0 * MR3_EPS : tol.rtol2;
   int nc = 0;
-  dv_dlarrb_one(B->nbl, RP + B->ibgn, 1, i, II == 1, II > 1, rgap, lgap, rtol1, rtol2, p->pivmin,
+  dv_dlarrb_one<1>(B->nbl, RP + B->ibgn, 1, i, II == 1, II > 1, rgap, lgap, rtol1, rtol2, p->pivmin,
                 maxitr, B->nbl, &w, &werr, &nc);
   W[s] = w;
   Werr[s] = werr;
@@ -1126,7 +1126,7 @@ k_cl_ext(int ncl, const ClusterDev *cl, const ProbDev *probs, const BlockDev *bl
     const int maxitr = dv_itmax(C.bl_spdiam + p->pivmin, p->pivmin);
     double wv = Wsh[sx], ev = Werr[sx];
     int nc = 0;
-    dv_dlarrb_one(nb, Pp, ps, i, 1, II > 1, 0.0, 0.0, tol.rqtol, tol.rqtol, p->pivmin, maxitr, nb,
+    dv_dlarrb_one<MR3_U>(nb, Pp, ps, i, 1, II > 1, 0.0, 0.0, tol.rqtol, tol.rqtol, p->pivmin, maxitr, nb,
                   &wv, &ev, &nc);
     xw[t] = wv;
     xe[t] = ev;
@@ -1232,7 +1232,7 @@ __device__ __forceinline__ unsigned long long refine_cl_body(
   const int maxitr = dv_itmax(C.bl_spdiam + p->pivmin, p->pivmin);
   double w = Wsh[s], e = Werr[s];
   int nc = 0;
-  dv_dlarrb_one(B.nbl, P, ps, i, i == pidx, II > 1, rgap, lgap, tol.rtol1, tol.rtol2, p->pivmin,
+  dv_dlarrb_one<MR3_U>(B.nbl, P, ps, i, i == pidx, II > 1, rgap, lgap, tol.rtol1, tol.rtol2, p->pivmin,
                 maxitr, B.nbl, &w, &e, &nc);
   Wsh[s] = w;
   Werr[s] = e;
@@ -1413,9 +1413,10 @@ k_classify(int ncl, const ClusterDev *cl, const BlockDev *blocks, const double *
 }
 
 // Per sibling group (led by the member with g == 0): reserve the group's
-// singleton records contiguously and cut them into warp tasks of 32.
-__global__ void k_group_tasks(int ncl, const ClusterDev *cl, ClsScratch xs, WTask *wt,
-                              SngCounters *sc, LevelCounters *lcn, int cap) {
+// singleton records contiguously, so that consecutive records share a block
+// (and the size of their sweeps).
+__global__ void k_group_tasks(int ncl, const ClusterDev *cl, ClsScratch xs, SngCounters *sc,
+                              LevelCounters *lcn, int cap) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= ncl) return;
   const ClusterDev C = cl[w];
@@ -1424,192 +1425,373 @@ __global__ void k_group_tasks(int ncl, const ClusterDev *cl, ClsScratch xs, WTas
   for (int m = 0; m < C.G; m++) tot += xs.ns[w + m];
   if (tot == 0) return;
   const int base = atomicAdd(&sc->n_sng, tot);
-  const int nwt = (tot + 31) / 32;
-  const int t0 = atomicAdd(&sc->n_wt, nwt);
-  if (base + tot > cap || t0 + nwt > cap) { atomicOr(&lcn->err, 1); return; }
+  if (base + tot > cap) { atomicOr(&lcn->err, 1); return; }
   int o = base;
   for (int m = 0; m < C.G; m++) { xs.soff[w + m] = o; o += xs.ns[w + m]; }
-  for (int t = 0; t < nwt; t++) {
-    WTask x;
-    x.first = base + 32 * t;
-    x.count = min(32, tot - 32 * t);
-    wt[t0 + t] = x;
-  }
 }
 
 // ------------------------------------------------------------------------
-// Singletons (PMR_process_s_task, SRC/process_singleton.c:65-317): one lane
-// per eigenvector, up to 32 eigenvectors of one cluster per warp.  Persistent
-// warps pull warp tasks from a device counter.  Each warp owns a scratch
-// region of 2 x nmax x 32 doubles laid out [array][row][lane]; the twisted
-// factorisations of the 32 lanes sweep the rows in lock-step, so every
-// scratch access is one coalesced 256-byte row.  The Rayleigh-quotient loop
-// of each lane is a small state machine: in every round each lane that still
-// needs a factorisation takes one, so lanes that need more iterations do not
-// hold the others' sweeps apart.  Eigenvectors leave through a shared-memory
+// Singletons (PMR_process_s_task, SRC/process_singleton.c:65-317), in
+// rounds.  A singleton's Rayleigh-quotient loop is a sequence of dlar1v
+// calls whose only carried state is a handful of scalars (SngState).  Each
+// round gives every unfinished singleton of the level one dlar1v: persistent
+// warps take 32 singletons at a time from the round's list, one lane each,
+// and the singletons that need another call are compacted into the next
+// round's list; those that need a bisection first (needBS) go to a list that
+// k_sng_bisect serves between rounds.  So no lane waits for another lane's
+// extra iterations, and the warps stay full in every round.
+//
+// Each warp owns scratch of 2 x nmax x 32 doubles laid out [array][row]
+// [lane]: the lanes sweep the rows by absolute index, so every scratch
+// access is one coalesced 256-byte row.  Consecutive records of a list
+// mostly share a block; a warp whose lanes hold blocks of different sizes
+// sweeps the largest.  Finished eigenvectors leave through a shared-memory
 // transpose, so the Z columns are written in coalesced rows.
 // ------------------------------------------------------------------------
 #define SNG_WARPS 8
 #define SNG_TILE_LD 33
-enum { PH_LOOP = 0, PH_STEP2 = 1, PH_DONE = 2 };
+#define SNG_ROUNDS (MR3_MAXITER + 1)   // MAXITER loop calls and the step-2 call
+enum { SF_USEDBS = 1, SF_USEDRQ = 2, SF_NEEDBS = 4, SF_STEP2 = 8 };
 
+// Loop variables of one singleton between rounds
+// (SRC/process_singleton.c:159-292: lambda, Wshifted[i], Werr[i], left,
+// right, bstres, bstw, residual, gap, gaptol, r, k and the flags).
+struct SngState {
+  double lambda, wsh, werr, left, right, bstres, bstw, resid, gap, gaptol;
+  int r, k, flags, pad;
+};
+
+__global__ void k_round_reset(SngCounters *sc, int in, int first) {
+  sc->nin = first ? sc->n_sng : sc->act_n[in];
+  sc->act_next[in] = 0;
+  sc->bs_next = 0;
+}
+
+// Stable compaction of a round's list: entry j of the list leaves the round
+// with flag[j] = 0 (finished), 1 (next round) or 2 (bisection first).  The
+// survivors keep their order, so the warps of the next round again take
+// neighbouring singletons (mostly of one block and one representation).
+#define LIST_T 1024   // entries per block: 256 threads x 4
+__global__ void __launch_bounds__(256) k_list_count(const SngCounters *sc,
+                                                    const unsigned char *flag, int *bcnt) {
+  __shared__ int red[2][8];
+  const int nin = sc->nin, base = blockIdx.x * LIST_T;
+  int c1 = 0, c2 = 0;
+  for (int q = 0; q < 4; q++) {
+    const int j = base + threadIdx.x * 4 + q;
+    if (j < nin) { const int f = flag[j]; c1 += f == 1; c2 += f == 2; }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    c1 += __shfl_xor_sync(0xffffffffu, c1, o);
+    c2 += __shfl_xor_sync(0xffffffffu, c2, o);
+  }
+  if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = c1; red[1][threadIdx.x >> 5] = c2; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int a = 0, b = 0;
+    for (int w = 0; w < 8; w++) { a += red[0][w]; b += red[1][w]; }
+    bcnt[2 * blockIdx.x] = a;
+    bcnt[2 * blockIdx.x + 1] = b;
+  }
+}
+
+// Exclusive scan of the block counts (one block of 1024 threads); the totals
+// become the next list's length and the bisection list's length.
+__global__ void __launch_bounds__(1024) k_list_scan(int nblk, SngCounters *sc, int *bcnt, int out,
+                                                    int last_round) {
+  __shared__ int wa[32], wb[32];
+  __shared__ int carry[2];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (threadIdx.x == 0) { carry[0] = 0; carry[1] = 0; }
+  __syncthreads();
+  for (int b0 = 0; b0 < nblk; b0 += 1024) {
+    const int b = b0 + threadIdx.x;
+    const int a = b < nblk ? bcnt[2 * b] : 0, c = b < nblk ? bcnt[2 * b + 1] : 0;
+    int ia = a, ic = c;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int x = __shfl_up_sync(0xffffffffu, ia, o), y = __shfl_up_sync(0xffffffffu, ic, o);
+      if (lane >= o) { ia += x; ic += y; }
+    }
+    if (lane == 31) { wa[wid] = ia; wb[wid] = ic; }
+    __syncthreads();
+    if (wid == 0) {
+      int xa = wa[lane], xc = wb[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        const int x = __shfl_up_sync(0xffffffffu, xa, o), y = __shfl_up_sync(0xffffffffu, xc, o);
+        if (lane >= o) { xa += x; xc += y; }
+      }
+      wa[lane] = xa; wb[lane] = xc;
+    }
+    __syncthreads();
+    const int pa = carry[0] + (wid ? wa[wid - 1] : 0) + ia - a;
+    const int pc = carry[1] + (wid ? wb[wid - 1] : 0) + ic - c;
+    if (b < nblk) { bcnt[2 * b] = pa; bcnt[2 * b + 1] = pc; }
+    __syncthreads();
+    if (threadIdx.x == 0) { carry[0] += wa[31]; carry[1] += wb[31]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    sc->act_n[out] = carry[0];
+    sc->bs_n = carry[1];
+    if (last_round && (carry[0] | carry[1])) sc->err = 1;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_list_scatter(int first, const SngCounters *sc,
+                                                      const unsigned char *flag, const int *bcnt,
+                                                      const int *act0, const int *act1, int in,
+                                                      int *bsl) {
+  __shared__ int wa[8], wb[8];
+  const int nin = sc->nin, base = blockIdx.x * LIST_T;
+  if (base >= nin) return;
+  const int *Ain = in ? act1 : act0;
+  int *Aout = const_cast<int *>(in ? act0 : act1);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int f[4], c1 = 0, c2 = 0;
+  for (int q = 0; q < 4; q++) {
+    const int j = base + threadIdx.x * 4 + q;
+    f[q] = j < nin ? flag[j] : 0;
+    c1 += f[q] == 1;
+    c2 += f[q] == 2;
+  }
+  int i1 = c1, i2 = c2;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int x = __shfl_up_sync(0xffffffffu, i1, o), y = __shfl_up_sync(0xffffffffu, i2, o);
+    if (lane >= o) { i1 += x; i2 += y; }
+  }
+  if (lane == 31) { wa[wid] = i1; wb[wid] = i2; }
+  __syncthreads();
+  int p1 = bcnt[2 * blockIdx.x] + i1 - c1, p2 = bcnt[2 * blockIdx.x + 1] + i2 - c2;
+  for (int w = 0; w < wid; w++) { p1 += wa[w]; p2 += wb[w]; }
+  for (int q = 0; q < 4; q++) {
+    const int j = base + threadIdx.x * 4 + q;
+    if (f[q] == 0) continue;
+    const int idx = first ? j : Ain[j];
+    if (f[q] == 1) Aout[p1++] = idx; else bsl[p2++] = idx;
+  }
+}
+
+template <bool FIRST>
 __global__ void __launch_bounds__(SNG_WARPS * 32, 2)
-k_singletons(const WTask *wt, const SngDev *sng, const ClusterDev *cl, const ProbDev *probs,
-             const BlockDev *blocks, const double2 *RP, const double2 *RQ, const double *arena,
-             double *W, double *Wsh, double *Werr, double *Wgap, const int *Windex,
-             const int *Zindex, SngCounters *sc, double *scratch, long long nmax,
-             unsigned long long *stats) {
+k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, const ProbDev *probs,
+            const BlockDev *blocks, const double2 *RP, const double2 *RQ, const double *arena,
+            double *W, double *Wsh, double *Werr, double *Wgap, const int *Windex,
+            const int *Zindex, SngState *sst, const int *act0, const int *act1,
+            unsigned char *flag, SngCounters *sc, double *scratch, long long nmax,
+            unsigned long long *stats) {
   extern __shared__ double sm_tile[];
+  const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   double *tile = sm_tile + (threadIdx.x >> 5) * 32 * SNG_TILE_LD;
   const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   double *X = scratch + gw * 2 * nmax * 32 + lane;
   double *Y = X + nmax * 32;
-  const int nwt = sc->n_wt;
-  unsigned long long w_r1v = 0, w_neg = 0, w_sweep = 0, w_rounds = 0, w_tasks = 0;
+  const int *Ain = in ? act1 : act0;
+  const int nin = sc->nin;
+  const double rqtol = 2.0 * MR3_EPS;
+  unsigned long long w_r1v = 0, w_sweep = 0, w_chunks = 0;
   for (;;) {
-    int t = 0;
-    if (lane == 0) t = atomicAdd(&sc->wt_next, 1);
-    t = __shfl_sync(0xffffffffu, t, 0);
-    if (t >= nwt) break;
-    const WTask T = wt[t];
-    const bool active = lane < T.count;
-    const SngDev S = sng[T.first + (active ? lane : 0)];
+    int base = 0;
+    if (lane == 0) base = atomicAdd(&sc->act_next[in], 32);
+    base = __shfl_sync(full, base, 0);
+    if (base >= nin) break;
+    const bool active = base + lane < nin;
+    // lanes without a singleton mirror the chunk's first one (valid
+    // pointers) and do no work
+    const int j = active ? base + lane : base;
+    const int idx = FIRST ? j : Ain[j];
+    const SngDev S = sng[idx];
     const ClusterDev C = cl[S.cl];
     const BlockDev &B = blocks[C.blk];
     const ProbDev *p = &probs[B.prob];
     const int nb = B.nbl;
     const double pivmin = p->pivmin;
-    // lanes of one task come from sibling clusters of one group: same block
-    // and block size, each lane reading its own (interleaved) representation
     const double2 *P, *Q;
     int ps;
     own_rrr(C, B, RP, RQ, arena, &P, &Q, &ps);
-    const double twoeps = 2.0 * MR3_EPS, rqtol = 2.0 * MR3_EPS;
-    const double tolr = 4.0 * dv_log((double)nb) * MR3_EPS;
-    const int maxitr = dv_itmax(C.bl_spdiam + pivmin, pivmin);
     const int s = S.slot;
-    double lambda = 0.0, wsh = 0.0, werr = 0.0, left = 0.0, right = 0.0, gap = 0.0, gaptol = 0.0;
-    int iloc = 0;
-    if (active) {
-      lambda = Wsh[s]; wsh = lambda; werr = Werr[s];
-      left = lambda - werr; right = lambda + werr;
-      iloc = Windex[s];
+    SngState st;
+    if (FIRST) {
+      st.lambda = Wsh[s]; st.wsh = st.lambda; st.werr = Werr[s];
+      st.left = st.lambda - st.werr; st.right = st.lambda + st.werr;
       // the reference compares the eigenvalue index with the block's first
       // and last row (SRC/process_singleton.c:142-157); W slots and rows of a
       // problem start at the same offset, so the same comparison is s == row
-      double lgap = (s == B.ibgn) ? MR3_EPS * fmax(fabs(left), fabs(right)) : S.lgap;
-      double rgap = (s == B.iend) ? MR3_EPS * fmax(fabs(left), fabs(right)) : Wgap[s];
-      gap = fmin(lgap, rgap);
-      gaptol = (s == B.ibgn || s == B.iend) ? 0.0 : gap * MR3_EPS;
+      const double lgap = (s == B.ibgn) ? MR3_EPS * fmax(fabs(st.left), fabs(st.right)) : S.lgap;
+      const double rgap = (s == B.iend) ? MR3_EPS * fmax(fabs(st.left), fabs(st.right)) : Wgap[s];
+      st.gap = fmin(lgap, rgap);
+      st.gaptol = (s == B.ibgn || s == B.iend) ? 0.0 : st.gap * MR3_EPS;
+      st.bstres = 0.0; st.bstw = 0.0; st.resid = 0.0;
+      st.r = 0; st.k = 1; st.flags = 0; st.pad = 0;
+    } else {
+      st = sst[idx];
     }
-    int phase = active ? PH_LOOP : PH_DONE;
-    int k = 1, r = 0;
-    bool usedBS = false, usedRQ = false, needBS = false;
-    double bstres = 0.0, bstw = 0.0, resid = 0.0;
+    const bool step2 = (st.flags & SF_STEP2) != 0;
+    const bool usedBS = (st.flags & SF_USEDBS) != 0;
+    const double lam_call = step2 ? st.bstw : st.lambda;
+    r1v_state rs;
+    rs.r = 0; rs.mingma = 0.0; rs.sawnan = false;
+    int negc = 0;
+    dv_r1v_factor(active, nb, lam_call, P, Q, ps, pivmin, !usedBS, st.r, X, Y, &negc, &rs);
     dlar1v_out o;
-    o.isupp1 = 1; o.isupp2 = nb; o.nrminv = 0.0; o.r = 0;
-    if (lane == 0) w_tasks++;
-    while (__any_sync(0xffffffffu, phase != PH_DONE)) {
-      const bool call = (phase != PH_DONE);
-      if (lane == 0) { w_rounds++; w_sweep += nb; }
-      if (call && phase == PH_LOOP && needBS) {
-        usedBS = true;
-        int tw = (r < 1 || r > nb) ? nb : r;
-        int nc = 0;
-        dv_dlarrb_one(nb, P, ps, iloc, 1, 0, 0.0, 0.0, 0.0, twoeps, pivmin, maxitr, tw, &wsh, &werr,
-                      &nc);
-        w_neg += (unsigned long long)nc * nb;
-        lambda = wsh;
-        r = 0;
-      }
-      const bool wantNC = !usedBS;
-      const double lam_call = (phase == PH_STEP2) ? bstw : lambda;
-      r1v_state st;
-      st.r = 0; st.mingma = 0.0; st.sawnan = false;
-      int negc = 0;
-      if (call) {
-        dv_r1v_factor(nb, lam_call, P, Q, ps, pivmin, wantNC, r, X, Y, 32, &negc, &st);
-        w_r1v += nb;
-      }
-      dv_r1v_solve(call, nb, Q, ps, gaptol, X, Y, 32, st, &o);
-      if (call) {
-        r = o.r;
-        if (phase == PH_STEP2) {
-          lambda = bstw;
-          phase = PH_DONE;
-        } else {
-          resid = o.resid;
-          if (k == 1 || o.resid < bstres) { bstres = o.resid; bstw = lambda; }
-          bool more = false;
-          if (!usedBS && o.resid > tolr * gap && fabs(o.rqcorr) > rqtol * fabs(lambda)) {
-            int sgndef = (iloc <= negc) ? -1 : 1;
-            if (o.rqcorr * sgndef >= 0.0 && lambda + o.rqcorr <= right &&
-                lambda + o.rqcorr >= left) {
-              usedRQ = true;
-              if (sgndef == 1) left = lambda; else right = lambda;
-              wsh = 0.5 * (left + right);
-              lambda += o.rqcorr;
-            } else {
-              needBS = true;
-            }
-            if (right - left < rqtol * fabs(lambda)) usedBS = true;
-            else if (k == MR3_MAXITER - 1) needBS = true;
-            k++;
-            more = (k <= MR3_MAXITER);
+    o.isupp1 = 1; o.isupp2 = nb; o.nrminv = 0.0; o.r = 0; o.resid = 0.0; o.rqcorr = 0.0;
+    dv_r1v_solve(active, nb, Q, ps, st.gaptol, X, Y, rs, &o);
+    const int nb_sweep = __reduce_max_sync(full, active ? nb : 0);
+    if (lane == 0) { w_chunks++; w_sweep += nb_sweep; }
+    bool done = false, tobs = false;
+    if (active) {
+      w_r1v += nb;
+      st.r = o.r;
+      if (step2) {
+        st.lambda = st.bstw;
+        done = true;
+      } else {
+        const double tolr = 4.0 * dv_log((double)nb) * MR3_EPS;
+        st.resid = o.resid;
+        if (st.k == 1 || o.resid < st.bstres) { st.bstres = o.resid; st.bstw = st.lambda; }
+        bool more = false;
+        if (!usedBS && o.resid > tolr * st.gap && fabs(o.rqcorr) > rqtol * fabs(st.lambda)) {
+          const int sgndef = (Windex[s] <= negc) ? -1 : 1;
+          if (o.rqcorr * sgndef >= 0.0 && st.lambda + o.rqcorr <= st.right &&
+              st.lambda + o.rqcorr >= st.left) {
+            st.flags |= SF_USEDRQ;
+            if (sgndef == 1) st.left = st.lambda; else st.right = st.lambda;
+            st.wsh = 0.5 * (st.left + st.right);
+            st.lambda += o.rqcorr;
+          } else {
+            st.flags |= SF_NEEDBS;
           }
-          if (!more) phase = (usedRQ && usedBS && bstres <= resid) ? PH_STEP2 : PH_DONE;
+          if (st.right - st.left < rqtol * fabs(st.lambda)) st.flags |= SF_USEDBS;
+          else if (st.k == MR3_MAXITER - 1) st.flags |= SF_NEEDBS;
+          st.k++;
+          more = (st.k <= MR3_MAXITER);
+        }
+        if (!more) {
+          if ((st.flags & SF_USEDRQ) && (st.flags & SF_USEDBS) && st.bstres <= st.resid)
+            st.flags |= SF_STEP2;
+          else
+            done = true;
+        } else if (st.flags & SF_NEEDBS) {
+          tobs = true;
         }
       }
     }
+    // unfinished singletons: state saved, flagged for the next round's list
+    // (or the bisection list); the compaction keeps the list order
+    if (active && !done) sst[idx] = st;
+    if (active) flag[base + lane] = done ? 0 : (tobs ? 2 : 1);
+    // finished eigenvectors out
+    const unsigned fin = __ballot_sync(full, done);
+    if (!fin) continue;
     const int bl0 = B.ibgn - p->off;   // block's first row inside the problem
     int zind = 0;
-    if (active) {
-      Wsh[s] = lambda;
-      Werr[s] = werr;
-      Wgap[s] = gap;
-      W[s] = lambda + C.sigma;
+    if (done) {
+      Wsh[s] = st.lambda;
+      Werr[s] = st.werr;
+      Wgap[s] = st.gap;
+      W[s] = st.lambda + C.sigma;
       zind = Zindex[s];
       p->Zsupp[2 * (size_t)zind] = o.isupp1 + bl0;
       p->Zsupp[2 * (size_t)zind + 1] = o.isupp2 + bl0;
     }
-    // eigenvectors out: tiles of 32 rows, transposed through shared memory
-    const int np = p->n;
-    const size_t ldz = (size_t)p->ldz;
-    const int a1 = o.isupp1, a2 = o.isupp2;
+    double *const Zp = p->Z;
+    const int ldz = p->ldz, np = p->n;
+    const int a1 = o.isupp1, a2 = o.isupp2, rr = o.r;
     const double nv = o.nrminv;
-    for (int k0 = 1; k0 <= nb; k0 += 32) {
+    const int nbw = __reduce_max_sync(full, done ? nb : 0);
+    for (int k0 = 1; k0 <= nbw; k0 += 32) {
 #pragma unroll 4
-      for (int j = 0; j < 32; j++) {
-        const int kk = k0 + j;
+      for (int jj = 0; jj < 32; jj++) {
+        const int kk = k0 + jj;
         double val = 0.0;
-        if (active && kk <= nb && kk >= a1 && kk <= a2) val = dv_zget(X, Y, 32, r, kk) * nv;
-        tile[j * SNG_TILE_LD + lane] = val;
+        if (done && kk <= nb && kk >= a1 && kk <= a2) val = dv_zget(X, Y, rr, kk) * nv;
+        tile[jj * SNG_TILE_LD + lane] = val;
       }
       __syncwarp();
-      const int row = bl0 + k0 - 1 + lane;
-      for (int v = 0; v < T.count; v++) {
-        const int zc = __shfl_sync(0xffffffffu, zind, v);
-        if (k0 + lane <= nb) p->Z[(size_t)zc * ldz + row] = tile[lane * SNG_TILE_LD + v];
+      for (unsigned m = fin; m; m &= m - 1) {
+        const int v = __ffs(m) - 1;
+        const int zc = __shfl_sync(full, zind, v);
+        const int b0 = __shfl_sync(full, bl0, v), nbv = __shfl_sync(full, nb, v);
+        const int ldv = __shfl_sync(full, ldz, v);
+        double *Zv = (double *)__shfl_sync(full, (unsigned long long)Zp, v);
+        if (k0 + lane <= nbv) Zv[(size_t)zc * ldv + b0 + k0 - 1 + lane] = tile[lane * SNG_TILE_LD + v];
       }
       __syncwarp();
     }
-    if (np > nb) {   // rows of the problem outside this block are zero
-      for (int v = 0; v < T.count; v++) {
-        const int zc = __shfl_sync(0xffffffffu, zind, v);
-        double *Zc = p->Z + (size_t)zc * ldz;
-        for (int row = lane; row < bl0; row += 32) Zc[row] = 0.0;
-        for (int row = bl0 + nb + lane; row < np; row += 32) Zc[row] = 0.0;
-      }
+    // rows of the problem outside this block are zero
+    for (unsigned m = fin; m; m &= m - 1) {
+      const int v = __ffs(m) - 1;
+      const int npv = __shfl_sync(full, np, v), nbv = __shfl_sync(full, nb, v);
+      if (npv <= nbv) continue;
+      const int zc = __shfl_sync(full, zind, v), b0 = __shfl_sync(full, bl0, v);
+      const int ldv = __shfl_sync(full, ldz, v);
+      double *Zc = (double *)__shfl_sync(full, (unsigned long long)Zp, v) + (size_t)zc * ldv;
+      for (int row = lane; row < b0; row += 32) Zc[row] = 0.0;
+      for (int row = b0 + nbv + lane; row < npv; row += 32) Zc[row] = 0.0;
+    }
+    __syncwarp();
+  }
+  stat_add(stats, KID_SNG * 4 + 2, w_r1v);
+  // diagnostics: warp-level row sweeps and warp chunks
+  stat_add(stats, KID_OTHER * 4 + 0, w_sweep);
+  stat_add(stats, KID_OTHER * 4 + 1, w_chunks);
+}
+
+// The bisection of a singleton whose Rayleigh-quotient step left its
+// interval (SRC/process_singleton.c:178-192: dlarrb to 2*eps with the twist
+// index of the last dlar1v), by a group of L lanes with the tree bisection
+// of dv_dlarrb_tree.  L is the largest of 32, 16, 8, 4 with which the list
+// still fits the resident lanes, so few singletons get short latency and
+// many get little redundant work.  The singleton joins the next round's list
+// (at its end).
+__global__ void __launch_bounds__(256)
+k_sng_bisect(int out, const SngDev *sng, const ClusterDev *cl, const ProbDev *probs,
+             const BlockDev *blocks, const double2 *RP, const double2 *RQ, const double *arena,
+             const int *Windex, SngState *sst, const int *bsl, int *act0, int *act1,
+             SngCounters *sc, unsigned long long *stats) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  int *Aout = out ? act1 : act0;
+  const int nbs = sc->bs_n;
+  if (nbs == 0) return;
+  const long long lanes = (long long)gridDim.x * blockDim.x;
+  int L = 32;
+  while (L > 4 && (long long)nbs * L > lanes) L >>= 1;
+  const int G = 32 / L, gi = lane / L, t = lane & (L - 1);
+  unsigned long long w_neg = 0;
+  for (;;) {
+    int t0 = 0;
+    if (lane == 0) t0 = atomicAdd(&sc->bs_next, G);
+    t0 = __shfl_sync(full, t0, 0);
+    if (t0 >= nbs) break;
+    const bool valid = t0 + gi < nbs;
+    const int idx = bsl[valid ? t0 + gi : t0];   // spare groups mirror a valid one
+    const SngDev S = sng[idx];
+    const ClusterDev C = cl[S.cl];
+    const BlockDev &B = blocks[C.blk];
+    const ProbDev *p = &probs[B.prob];
+    const int nb = B.nbl;
+    const double pivmin = p->pivmin;
+    const double2 *P, *Q;
+    int ps;
+    own_rrr(C, B, RP, RQ, arena, &P, &Q, &ps);
+    SngState st = sst[idx];
+    const int maxitr = dv_itmax(C.bl_spdiam + pivmin, pivmin);
+    const int tw = (st.r < 1 || st.r > nb) ? nb : st.r;
+    int nc = 0;
+    dv_dlarrb_tree(L, nb, P, ps, Windex[S.slot], 1, 0, 0.0, 0.0, 0.0, 2.0 * MR3_EPS, pivmin, maxitr,
+                   tw, &st.wsh, &st.werr, &nc);
+    st.flags = (st.flags | SF_USEDBS) & ~SF_NEEDBS;
+    st.lambda = st.wsh;
+    st.r = 0;
+    if (valid && t == 0) {
+      w_neg += (unsigned long long)nc * nb;
+      sst[idx] = st;
+      Aout[atomicAdd(&sc->act_n[out], 1)] = idx;
     }
     __syncwarp();
   }
   stat_add(stats, KID_SNG * 4 + 1, w_neg);
-  stat_add(stats, KID_SNG * 4 + 2, w_r1v);
-  // diagnostics: warp-level row sweeps, Rayleigh rounds and tasks
-  stat_add(stats, KID_OTHER * 4 + 0, w_sweep);
-  stat_add(stats, KID_OTHER * 4 + 1, w_rounds);
-  stat_add(stats, KID_OTHER * 4 + 2, w_tasks);
 }
 
 // Unit vectors of 1x1 blocks (SRC/process_singleton.c:125-133).
@@ -1714,7 +1896,12 @@ __global__ void k_perm_zsupp2(int N, const ProbDev *probs, const int *prob_of_sl
 // ========================================================================
 struct mr3_cuda_ctx {
   int device = 0, nsm = 148;
+  int sng_ctas_per_sm = 2;                  // resident k_sng_round CTAs per SM
   cudaStream_t own = nullptr;
+  cudaStream_t aux = nullptr;               // copies that overlap the solves
+  cudaEvent_t xev[MR3_CUDA_EVENTS] = {nullptr};
+  void *hws = nullptr;                      // page-locked staging buffer
+  size_t hws_cap = 0;
   char err[256] = {0};
   long long launches = 0;
   size_t capN = 0, capP = 0, capScratch = 0, capArena[2] = {0, 0};
@@ -1732,7 +1919,9 @@ struct mr3_cuda_ctx {
   SortRec *rec0 = nullptr, *rec1 = nullptr;
   ClusterDev *cl[2] = {nullptr, nullptr};
   SngDev *sng = nullptr;
-  WTask *wt = nullptr;
+  SngState *sst = nullptr;
+  int *act[2] = {nullptr, nullptr}, *bsl = nullptr, *sbcnt = nullptr;
+  unsigned char *sflag = nullptr;
   LevelCounters *lc = nullptr;
   SngCounters *sc = nullptr;
   double *scratch = nullptr, *arena[2] = {nullptr, nullptr};
@@ -1851,7 +2040,12 @@ static int ensure_rows(mr3_cuda_ctx *c, size_t N, size_t P) {
     CK(regrow(&c->cl[0], n), "cl0");
     CK(regrow(&c->cl[1], n), "cl1");
     CK(regrow(&c->sng, n), "sng");
-    CK(regrow(&c->wt, n), "wt");
+    CK(regrow(&c->sst, n), "sst");
+    CK(regrow(&c->act[0], n), "act0");
+    CK(regrow(&c->act[1], n), "act1");
+    CK(regrow(&c->bsl, n), "bsl");
+    CK(regrow(&c->sflag, n), "sflag");
+    CK(regrow(&c->sbcnt, 2 * (n / LIST_T + 1)), "sbcnt");
     c->capN = n;
   }
   if (P > c->capP) {
@@ -1881,7 +2075,11 @@ extern "C" int mr3_cuda_ctx_create(int device, mr3_cuda_ctx **out) {
   c->device = device;
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->nsm = prop.multiProcessorCount;
-  if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
+  bool evok = true;
+  for (int i = 0; i < MR3_CUDA_EVENTS; i++)
+    evok = evok && cudaEventCreateWithFlags(&c->xev[i], cudaEventDisableTiming) == cudaSuccess;
+  if (!evok || cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc((void **)&c->lc, 2 * sizeof(LevelCounters)) != cudaSuccess ||
       cudaMalloc((void **)&c->sc, sizeof(SngCounters)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_lc, 2 * sizeof(LevelCounters)) != cudaSuccess ||
@@ -1892,8 +2090,16 @@ extern "C" int mr3_cuda_ctx_create(int device, mr3_cuda_ctx **out) {
     mr3_cuda_ctx_destroy(c);
     return MR3_EMISC;
   }
-  cudaFuncSetAttribute(k_singletons, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(k_sng_round<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        SNG_WARPS * 32 * SNG_TILE_LD * (int)sizeof(double));
+  cudaFuncSetAttribute(k_sng_round<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       SNG_WARPS * 32 * SNG_TILE_LD * (int)sizeof(double));
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &nb, k_sng_round<false>, SNG_WARPS * 32, SNG_WARPS * 32 * SNG_TILE_LD * sizeof(double)) ==
+          cudaSuccess &&
+      nb > 0)
+    c->sng_ctas_per_sm = nb;
   c->h_const[0] = 1.0;
   c->h_iconst[0] = 1;
   c->h_iconst[1] = 1;
@@ -1908,7 +2114,7 @@ extern "C" void mr3_cuda_ctx_destroy(mr3_cuda_ctx *c) {
                  c->prob_of_slot, c->cl_of_slot, c->lvl_of_slot, c->unit_list, c->flag, c->tmp2,
                  c->D, c->E, c->E2, c->Wt, c->Et, c->W, c->Werr, c->Wgap, c->Wcopy, c->Wsh,
                  c->Dt, c->Lt, c->Wout, c->gers, c->TP, c->TPc, c->RP, c->RQ, c->rec0, c->rec1,
-                 c->cl[0], c->cl[1], c->sng, c->wt, c->lc, c->sc, c->scratch, c->arena[0],
+                 c->cl[0], c->cl[1], c->sng, c->sst, c->act[0], c->act[1], c->bsl, c->sflag, c->sbcnt, c->lc, c->sc, c->scratch, c->arena[0],
                  c->cls_ns, c->cls_soff, c->cls_cbase, c->cls_abase,
                  c->arena[1], (void *)c->Din, (void *)c->Ein, c->Wp, c->Dp, c->Ep};
   for (void *q : dev)
@@ -1920,6 +2126,10 @@ extern "C" void mr3_cuda_ctx_destroy(mr3_cuda_ctx *c) {
     if (q) cudaFreeHost(q);
   if (c->stats) cudaFree(c->stats);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
+  for (int i = 0; i < MR3_CUDA_EVENTS; i++)
+    if (c->xev[i]) cudaEventDestroy(c->xev[i]);
+  if (c->hws) cudaFreeHost(c->hws);
+  if (c->aux) cudaStreamDestroy(c->aux);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
 }
@@ -1929,6 +2139,7 @@ extern "C" void *mr3_cuda_ws(mr3_cuda_ctx *c, int slot, size_t bytes) {
   if (bytes > c->ws_cap[slot] || !c->ws[slot]) {
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->own);
+    cudaStreamSynchronize(c->aux);
     if (c->ws[slot]) cudaFree(c->ws[slot]);
     c->ws[slot] = nullptr;
     c->ws_cap[slot] = 0;
@@ -1964,6 +2175,67 @@ extern "C" int mr3_cuda_sync(mr3_cuda_ctx *c) {
   if (!c) return MR3_EMISC;
   CK(cudaStreamSynchronize(c->own), "sync");
   return MR3_OK;
+}
+
+static cudaStream_t ctx_stream(mr3_cuda_ctx *c, int which) {
+  return which == MR3_STREAM_COPY ? c->aux : c->own;
+}
+
+extern "C" int mr3_cuda_copy_on(mr3_cuda_ctx *c, int stream, void *dst, const void *src,
+                                size_t bytes, int dir) {
+  if (!c || (stream != MR3_STREAM_MAIN && stream != MR3_STREAM_COPY)) return MR3_EMISC;
+  if (bytes == 0) return MR3_OK;
+  CK(cudaMemcpyAsync(dst, src, bytes, dir == 0 ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost,
+                     ctx_stream(c, stream)), "copy_on");
+  return MR3_OK;
+}
+
+extern "C" int mr3_cuda_copy2d_on(mr3_cuda_ctx *c, int stream, void *dst, size_t dpitch,
+                                  const void *src, size_t spitch, size_t width, size_t height,
+                                  int dir) {
+  if (!c || (stream != MR3_STREAM_MAIN && stream != MR3_STREAM_COPY)) return MR3_EMISC;
+  if (width == 0 || height == 0) return MR3_OK;
+  CK(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height,
+                       dir == 0 ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost,
+                       ctx_stream(c, stream)),
+     "copy2d_on");
+  return MR3_OK;
+}
+
+extern "C" int mr3_cuda_event(mr3_cuda_ctx *c, int ev, int record_on, int wait_on) {
+  if (!c || ev < 0 || ev >= MR3_CUDA_EVENTS || record_on > MR3_STREAM_COPY ||
+      wait_on > MR3_STREAM_COPY)
+    return MR3_EMISC;
+  if (record_on >= 0) CK(cudaEventRecord(c->xev[ev], ctx_stream(c, record_on)), "event record");
+  if (wait_on >= 0) CK(cudaStreamWaitEvent(ctx_stream(c, wait_on), c->xev[ev], 0), "event wait");
+  return MR3_OK;
+}
+
+extern "C" int mr3_cuda_sync_all(mr3_cuda_ctx *c) {
+  if (!c) return MR3_EMISC;
+  CK(cudaStreamSynchronize(c->own), "sync main");
+  CK(cudaStreamSynchronize(c->aux), "sync copy");
+  return MR3_OK;
+}
+
+extern "C" void *mr3_cuda_host_ws(mr3_cuda_ctx *c, size_t bytes) {
+  if (!c) return nullptr;
+  if (bytes > c->hws_cap || !c->hws) {
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->own);
+    cudaStreamSynchronize(c->aux);
+    if (c->hws) cudaFreeHost(c->hws);
+    c->hws = nullptr;
+    c->hws_cap = 0;
+    size_t sz = std::max<size_t>(bytes, 4096);
+    if (cudaMallocHost(&c->hws, sz) != cudaSuccess) {
+      c->hws = nullptr;
+      snprintf(c->err, sizeof(c->err), "page-locked buffer of %zu bytes", sz);
+      return nullptr;
+    }
+    c->hws_cap = sz;
+  }
+  return c->hws;
 }
 
 extern "C" void mr3_cuda_profile(mr3_cuda_ctx *c, int on) {
@@ -2160,7 +2432,9 @@ extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *s
     // singleton scratch: 2 x nmax x 32 doubles per persistent warp
     const size_t per_warp = 2ull * (size_t)nmaxV * 32ull;
     const size_t budget = (size_t)8 << 30;   // bytes
-    size_t nwarps = std::min<size_t>((size_t)c->nsm * 32, std::max<size_t>(c->nsm, budget / (per_warp * 8)));
+    // persistent warps: no more than can be resident at once
+    const size_t resident = (size_t)c->nsm * (size_t)c->sng_ctas_per_sm * SNG_WARPS;
+    size_t nwarps = std::min<size_t>(resident, std::max<size_t>(c->nsm, budget / (per_warp * 8)));
     nwarps = (nwarps + SNG_WARPS - 1) / SNG_WARPS * SNG_WARPS;
     if (nwarps * per_warp > c->capScratch) {
       CK(regrow(&c->scratch, nwarps * per_warp), "scratch");
@@ -2187,21 +2461,48 @@ extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *s
                c->lvl_of_slot, level);
       }
       CK(cudaMemsetAsync(&c->lc[nxt], 0, sizeof(LevelCounters), st), "lcn");
-      CK(cudaMemsetAsync(c->sc, 0, 3 * sizeof(int), st), "scn");
+      CK(cudaMemsetAsync(&c->sc->n_sng, 0, sizeof(int), st), "scn");
       LAUNCH(k_classify<0>, gW, MR3_THREADS, ncl, c->cl[cur], c->blocks, c->Wsh, c->Wgap,
              c->cl[nxt], c->sng, &c->lc[nxt], xs, NN);
-      LAUNCH(k_group_tasks, (ncl + 127) / 128, 128, ncl, c->cl[cur], xs, c->wt, c->sc, &c->lc[nxt], NN);
+      LAUNCH(k_group_tasks, (ncl + 127) / 128, 128, ncl, c->cl[cur], xs, c->sc, &c->lc[nxt], NN);
       LAUNCH(k_classify<1>, gW, MR3_THREADS, ncl, c->cl[cur], c->blocks, c->Wsh, c->Wgap,
              c->cl[nxt], c->sng, &c->lc[nxt], xs, NN);
       CK(cudaMemcpyAsync(c->h_lc, &c->lc[nxt], sizeof(LevelCounters), cudaMemcpyDeviceToHost, st), "lcn d2h");
       CK(cudaMemcpyAsync(c->h_sc, c->sc, sizeof(SngCounters), cudaMemcpyDeviceToHost, st), "sc d2h");
       CK(cudaStreamSynchronize(st), "level sync");
       if (c->h_lc->err) { snprintf(c->err, sizeof(c->err), "queue overflow"); return MR3_EMISC; }
-      if (c->h_sc->n_wt > 0)
-        LAUNCH_SMEM(k_singletons, (int)(nwarps / SNG_WARPS), SNG_WARPS * 32,
-                    SNG_WARPS * 32 * SNG_TILE_LD * sizeof(double), c->wt, c->sng, c->cl[cur], c->probs,
-               c->blocks, c->RP, c->RQ, c->arena[cur], c->W, c->Wsh, c->Werr, c->Wgap, c->Windex,
-               c->Zindex, c->sc, c->scratch, (long long)nmaxV, stats);
+      if (c->h_sc->err) { snprintf(c->err, sizeof(c->err), "singleton rounds exhausted"); return MR3_EMISC; }
+      if (c->h_sc->n_sng > 0) {
+        // the level's singletons in rounds (see k_sng_round)
+        const int nsng = c->h_sc->n_sng;
+        const int ctas_all = (int)(nwarps / SNG_WARPS);
+        const int ctas_first = std::min(ctas_all, (nsng + 32 * SNG_WARPS - 1) / (32 * SNG_WARPS));
+        const size_t smem = SNG_WARPS * 32 * SNG_TILE_LD * sizeof(double);
+        const int bis_ctas = c->nsm * 4;
+        const int nblk = (nsng + LIST_T - 1) / LIST_T;
+        for (int rd = 0; rd < SNG_ROUNDS; rd++) {
+          const int in = rd & 1, last = rd == SNG_ROUNDS - 1;
+          LAUNCH(k_round_reset, 1, 1, c->sc, in, rd == 0);
+          if (rd == 0)
+            LAUNCH_SMEM(k_sng_round<true>, ctas_first, SNG_WARPS * 32, smem, in, c->sng,
+                        c->cl[cur], c->probs, c->blocks, c->RP, c->RQ, c->arena[cur], c->W, c->Wsh,
+                        c->Werr, c->Wgap, c->Windex, c->Zindex, c->sst, c->act[0], c->act[1],
+                        c->sflag, c->sc, c->scratch, (long long)nmaxV, stats);
+          else
+            LAUNCH_SMEM(k_sng_round<false>, ctas_all, SNG_WARPS * 32, smem, in, c->sng,
+                        c->cl[cur], c->probs, c->blocks, c->RP, c->RQ, c->arena[cur], c->W, c->Wsh,
+                        c->Werr, c->Wgap, c->Windex, c->Zindex, c->sst, c->act[0], c->act[1],
+                        c->sflag, c->sc, c->scratch, (long long)nmaxV, stats);
+          LAUNCH(k_list_count, nblk, 256, c->sc, c->sflag, c->sbcnt);
+          LAUNCH(k_list_scan, 1, 1024, nblk, c->sc, c->sbcnt, in ^ 1, last);
+          LAUNCH(k_list_scatter, nblk, 256, rd == 0, c->sc, c->sflag, c->sbcnt, c->act[0],
+                 c->act[1], in, c->bsl);
+          if (!last)
+            LAUNCH(k_sng_bisect, bis_ctas, 256, in ^ 1, c->sng, c->cl[cur], c->probs, c->blocks,
+                   c->RP, c->RQ, c->arena[cur], c->Windex, c->sst, c->bsl, c->act[0], c->act[1],
+                   c->sc, stats);
+        }
+      }
       ncl = c->h_lc->n_cl;
       const size_t need = (size_t)c->h_lc->arena_need;
       if (ncl > 0 && need > c->capArena[nxt]) {
@@ -2211,6 +2512,9 @@ extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *s
         c->capArena[nxt] = nsz;
       }
     }
+    CK(cudaMemcpyAsync(c->h_sc, c->sc, sizeof(SngCounters), cudaMemcpyDeviceToHost, st), "sc end");
+    CK(cudaStreamSynchronize(st), "rounds sync");
+    if (c->h_sc->err) { snprintf(c->err, sizeof(c->err), "singleton rounds exhausted"); return MR3_EMISC; }
   }
 
   // ---- post-processing (SRC/mrrr.c:262-285)

@@ -40,3 +40,14 @@ def test_batch_order_does_not_matter():
     rev = M.mrrr_batched(probs[::-1])[::-1]
     for k, (a, b) in enumerate(zip(res, rev)):
         assert_same(a, b, f"order {k}")
+
+
+def test_pipelined_chunks_identical(monkeypatch):
+    """A batch solved in many chunks (Z copies of one chunk overlapping the
+    next chunk's solve) returns exactly what the one-pass batch returns."""
+    probs = _problems()
+    whole = M.mrrr_batched(probs)
+    monkeypatch.setenv("MR3_PIPE_BYTES", str(64 * 1024))
+    chunked = M.mrrr_batched(probs)
+    for k, (a, b) in enumerate(zip(whole, chunked)):
+        assert_same(a, b, f"chunked {k}")

@@ -380,7 +380,7 @@ static __device__ __noinline__ int dv_dlarrb_tree(int L, int n, const double2 *_
       for (int j = 0; j < k; j++) { x = side ? x + back : x - back; back = 2.0 * back; }
       const bool mine = side ? need1 : need0;
       int cnt = 0;
-      if (mine) cnt = dv_dlaneg<1>(n, R, ps, x, r);
+      if (mine) cnt = dv_dlaneg<MR3_U>(n, R, ps, x, r);
       const bool ok = mine && (side ? (cnt >= i) : (cnt <= i - 1));
       const unsigned gb = (__ballot_sync(full, ok) >> g0) & gbits;
       for (int sd = 0; sd < 2; sd++) {
@@ -423,7 +423,7 @@ static __device__ __noinline__ int dv_dlarrb_tree(int L, int n, const double2 *_
       if ((node_t >> b) & 1) l = m; else rr = m;
     }
     int cnt = 0;
-    if (!done) cnt = dv_dlaneg<1>(n, R, ps, 0.5 * (l + rr), r);
+    if (!done) cnt = dv_dlaneg<MR3_U>(n, R, ps, 0.5 * (l + rr), r);
     int node = 1;
     for (int d = 0; d < depth; d++) {
       const int c = __shfl_sync(full, cnt, g0 + node);
@@ -848,6 +848,387 @@ static __device__ __noinline__ void dv_r1v_solve(bool active, int n, const doubl
     o->rqcorr = o->mingma * tmp;
     o->sawnan = st.sawnan;
   }
+}
+
+// ------------------------------------------------------------------------
+// dlar1v with checkpoints (the singleton rounds).  The three sweeps of
+// dlar1v above keep LPLUS, S and UMINUS of every row in per-lane scratch,
+// written by one sweep and read back in the opposite order by the next: for
+// a batch that is several bytes of scratch traffic per row and lane, all of
+// it through DRAM.  Here a sweep keeps only its state at the start of every
+// block of CK_K rows (block j = rows j*CK_K+1 .. (j+1)*CK_K); a consumer
+// that needs a block's values recomputes them from the checkpoint with the
+// same operations, in registers, and uses them in its own order.  The
+// recomputed values are the stored values, bit for bit; the recurrences are
+// run about twice, and the scratch traffic falls to three doubles per block.
+// The back-substitution writes the normalised eigenvector straight to its
+// column of Z when asked to (a second call after the vector is accepted).
+// ------------------------------------------------------------------------
+#ifndef CK_K
+#define CK_K 4
+#endif
+
+// One lane's checkpoints; element j of each array at [j * 32].
+struct r1c_ck {
+  double *S;   // s entering block j (s = -lambda for j = 0)
+  double *I;   // stationary value SI of row j*CK_K (0 for j = 0)
+  double *P;   // p entering the highest row of block j that the progressive
+               // sweep processed
+};
+
+struct r1c_state {
+  int r;
+  double mingma;
+  bool sawnan, slowA, slowB;   // NaN seen; stationary / progressive sweep
+                               // used the NaN-safe formulas
+};
+
+// Stationary sweep (rows 1..r2-1) of one lane with checkpoints, rows read
+// in register chunks of MR3_U (next chunk loaded before the current one is
+// computed).  SLOW selects the NaN-safe formulas.  Returns whether a NaN
+// calls for the NaN-safe rerun; sr1 = SI of row r1-1 (0 for r1 = 1),
+// silast = SI of row r2-1.
+template <bool SLOW>
+static __device__ __noinline__ bool dv_r1c_statio(double lambda, const double2 *__restrict__ P,
+                                           const double2 *__restrict__ Q, int ps, double pivmin,
+                                           int r1, int r2, double *__restrict__ ckS,
+                                           double *__restrict__ ckI, int *neg1o, double *sr1o,
+                                           double *silasto) {
+  constexpr int U = MR3_U;
+  static_assert(CK_K % U == 0, "chunks must not straddle checkpoint blocks");
+  const int last = r2 - 1;
+  int neg1 = 0;
+  double s = 0.0 - lambda, siv = 0.0, sr1 = 0.0;
+  bool sawnan = false;
+  if (last >= 1) {
+    double2 cp[U], cq[U], np_[U], nq[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int i = d_imin(1 + u, last);
+      cp[u] = P[(size_t)(i - 1) * ps];
+      cq[u] = Q[(size_t)(i - 1) * ps];
+    }
+    for (int i0 = 1; i0 <= last; i0 += U) {
+      if (((i0 - 1) & (CK_K - 1)) == 0) {
+        const int j = (i0 - 1) / CK_K;
+        ckS[(size_t)j * 32] = s;
+        ckI[(size_t)j * 32] = siv;
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int i = d_imin(i0 + U + u, last);
+        np_[u] = P[(size_t)(i - 1) * ps];
+        nq[u] = Q[(size_t)(i - 1) * ps];
+        if (MR3_PF && i0 + u + MR3_PF <= last) {
+          pf_l1(&P[(size_t)(i0 + u + MR3_PF - 1) * ps]);
+          pf_l1(&Q[(size_t)(i0 + u + MR3_PF - 1) * ps]);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int i = i0 + u;
+        if (i <= last) {
+          double dplus = cp[u].x + s;
+          if (SLOW && fabs(dplus) < pivmin) dplus = -pivmin;
+          const double lp = cq[u].y / dplus;
+          if (i <= r1 - 1) neg1 += (dplus < 0.0);
+          double si = s * lp * cq[u].x;
+          if (SLOW && lp == 0.0) si = cp[u].y;
+          s = si - lambda;
+          siv = si;
+          if (i == r1 - 1) {
+            sr1 = si;
+            if (!SLOW && isnan(s)) sawnan = true;
+          }
+        }
+      }
+      if (sawnan) break;
+#pragma unroll
+      for (int u = 0; u < U; u++) { cp[u] = np_[u]; cq[u] = nq[u]; }
+    }
+  }
+  if (!SLOW && !sawnan) sawnan = isnan(s);
+  *neg1o = neg1;
+  *sr1o = sr1;
+  *silasto = siv;
+  return !SLOW && sawnan;
+}
+
+// Progressive sweep (rows n-1..r1) with the twist search of r1..r2, for the
+// whole warp: the lanes sweep the blocks by absolute index from the largest
+// N-1 down to the smallest R1, each lane on its own rows, so the per-lane
+// checkpoint rows stay aligned.  The twist search needs the stationary SI of
+// row i-1 at row i: in search mode a block's SI values are recomputed from
+// its stationary checkpoint first.  Returns P(R1-1).
+template <bool SLOW>
+static __device__ __noinline__ double dv_r1c_progr(bool active, int n, double lambda,
+                                            const double2 *__restrict__ P,
+                                            const double2 *__restrict__ Q, int ps, double pivmin,
+                                            int r1, int r2, bool slowA, const double *__restrict__ ckS,
+                                            const double *__restrict__ ckI, double *__restrict__ ckP,
+                                            double silast, int *neg2o, int *rbest_o, double *best_o,
+                                            bool *have_o) {
+  const double eps = MR3_EPS;
+  int neg2 = 0, rbest = 0;
+  double p = 0.0, best = 0.0;
+  bool have = false;
+  const int top = n - 1;
+  if (active) {
+    p = P[(size_t)(n - 1) * ps].x - lambda;   // P(n-1)
+    if (r2 == n && n > r1) {                  // candidate r = n
+      double c = silast + p;
+      if (c == 0.0) c = eps * silast;
+      best = c; rbest = n; have = true;
+    }
+  }
+  const bool work = active && top >= r1;
+  const bool search = r2 > r1;
+  const int topw = __reduce_max_sync(0xffffffffu, work ? top : 0);
+  const int r1w = __reduce_min_sync(0xffffffffu, work ? r1 : 0x7fffffff);
+  if (topw >= 1) {
+    for (int jb = (topw - 1) / CK_K; jb >= (r1w - 1) / CK_K; jb--) {
+      const int base = jb * CK_K + 1;
+      const int hi = d_imin(base + CK_K - 1, top), lo = d_imax(base, r1);
+      const bool bw = work && lo <= hi;
+      // this block's rows, loaded before any arithmetic
+      double2 pp[CK_K];
+#pragma unroll
+      for (int u = 0; u < CK_K; u++) {
+        if (bw) pp[u] = P[(size_t)(d_imax(d_imin(base + u, hi), lo) - 1) * ps];
+      }
+      if (bw && base - 1 >= r1)
+        for (int i = d_imax(base - CK_K, r1); i <= base - 1; i++) {
+          pf_l1(&P[(size_t)(i - 1) * ps]);
+          pf_l1(&Q[(size_t)(i - 1) * ps]);
+        }
+      double sia[CK_K];
+      if (bw && search) {
+        // SI of rows base-1 .. base+CK_K-2 (those of twist candidates only)
+        sia[0] = ckI[(size_t)jb * 32];
+        double s = ckS[(size_t)jb * 32];
+        const int rmax = d_imin(hi - 1, r2 - 1);
+#pragma unroll
+        for (int u = 1; u < CK_K; u++) {
+          const int i = base + u - 1;
+          if (i <= rmax) {
+            const double2 a = pp[u - 1];
+            const double2 q = Q[(size_t)(i - 1) * ps];
+            double dplus = a.x + s;
+            if (slowA && fabs(dplus) < pivmin) dplus = -pivmin;
+            const double lp = q.y / dplus;
+            double si = s * lp * q.x;
+            if (slowA && lp == 0.0) si = a.y;
+            s = si - lambda;
+            sia[u] = si;
+          }
+        }
+      }
+      if (bw) ckP[(size_t)jb * 32] = p;
+#pragma unroll
+      for (int u = CK_K - 1; u >= 0; u--) {
+        const int i = base + u;
+        if (bw && i >= lo && i <= hi) {
+          double dminus = pp[u].y + p;
+          if (SLOW && fabs(dminus) < pivmin) dminus = -pivmin;
+          const double tmp = pp[u].x / dminus;
+          neg2 += (dminus < 0.0);
+          double pn = p * tmp - lambda;
+          if (SLOW && tmp == 0.0) pn = pp[u].x - lambda;
+          p = pn;
+          if (i > r1 && i <= r2) {        // candidate r = i: S(i-1) + P(i-1)
+            const double sprev = sia[u];
+            double c = sprev + p;
+            if (c == 0.0) c = eps * sprev;
+            if (!have || fabs(c) < fabs(best)) { best = c; rbest = i; have = true; }
+          }
+        }
+      }
+    }
+  }
+  *neg2o = neg2;
+  *rbest_o = rbest;
+  *best_o = best;
+  *have_o = have;
+  return p;
+}
+
+// The two factorisation sweeps and the twist choice of dlar1v (as
+// dv_r1v_factor), for the whole warp.
+static __device__ __noinline__ void dv_r1c_factor(bool active, int n, double lambda,
+                                           const double2 *__restrict__ P,
+                                           const double2 *__restrict__ Q, int ps, double pivmin,
+                                           bool wantnc, int r_in, r1c_ck ck, int *negcnt,
+                                           r1c_state *st) {
+  const double eps = MR3_EPS;
+  int r1 = 1, r2 = n, neg1 = 0, neg2 = 0, rbest = 0;
+  if (r_in != 0) { r1 = r_in; r2 = r_in; }
+  bool sawnan1 = false;
+  double sr1 = 0.0, silast = 0.0;
+  if (active) {
+    sawnan1 = dv_r1c_statio<false>(lambda, P, Q, ps, pivmin, r1, r2, ck.S, ck.I, &neg1, &sr1, &silast);
+    // odr1v.f:199-205: rerun with the NaN-safe formulas
+    if (sawnan1) dv_r1c_statio<true>(lambda, P, Q, ps, pivmin, r1, r2, ck.S, ck.I, &neg1, &sr1, &silast);
+  }
+  double best = 0.0;
+  bool have = false;
+  double pr1 = dv_r1c_progr<false>(active, n, lambda, P, Q, ps, pivmin, r1, r2, sawnan1, ck.S, ck.I,
+                                   ck.P, silast, &neg2, &rbest, &best, &have);
+  bool sawnan2 = active && isnan(pr1);
+  if (__any_sync(0xffffffffu, sawnan2)) {
+    // odr1v.f:234-250: the progressive sweep again with the NaN-safe
+    // formulas (the stationary checkpoints are unchanged)
+    int n2b = 0, rbb = 0;
+    double bb = 0.0;
+    bool hb = false;
+    double pb = dv_r1c_progr<true>(sawnan2, n, lambda, P, Q, ps, pivmin, r1, r2, sawnan1, ck.S, ck.I,
+                                   ck.P, silast, &n2b, &rbb, &bb, &hb);
+    if (sawnan2) { pr1 = pb; neg2 = n2b; rbest = rbb; best = bb; have = hb; }
+  }
+  if (!active) return;
+  double mg = sr1 + pr1;
+  if (mg < 0.0) neg1++;
+  *negcnt = wantnc ? neg1 + neg2 : -1;
+  if (fabs(mg) == 0.0) mg = eps * sr1;
+  int r = r1;
+  if (have && fabs(best) <= fabs(mg)) { mg = best; r = rbest; }
+  st->mingma = mg;
+  st->r = r;
+  st->sawnan = sawnan1 || sawnan2;
+  st->slowA = sawnan1;
+  st->slowB = sawnan2;
+}
+
+// Back-substitution of dlar1v (as dv_r1v_solve) for one lane, on its own
+// rows only (no lock-step: a localised eigenvector costs its support, not
+// the span of its warp's twist indices), with the factors recomputed block
+// by block from the checkpoints: upward from the twist, LPLUS of a block
+// from its stationary checkpoint; downward, UMINUS from its progressive
+// checkpoint.  With zout (the lane's column of Z at the block's first row)
+// the normalised z (times nv) of the rows in the support is written there;
+// rows outside the support are not touched.
+static __device__ __noinline__ void dv_r1c_solve(int n, double lambda, const double2 *__restrict__ P,
+                                          const double2 *__restrict__ Q, int ps, double pivmin,
+                                          double gaptol, int r, bool slow, bool slowA, bool slowB,
+                                          const double *__restrict__ ckS,
+                                          const double *__restrict__ ckP, double mingma,
+                                          double *zout, double nv, dlar1v_out *o) {
+  int is1 = 1, is2 = n;
+  double ztz = 1.0;
+  if (zout) zout[r - 1] = 1.0 * nv;
+  // upward solve: i = r-1 .. 1
+  {
+    double zp = 1.0, zpp = 0.0;   // z(i+1), z(i+2)
+    bool go = r - 1 >= 1;
+    for (int jb = (r - 2) / CK_K; go && jb >= 0; jb--) {
+      const int base = jb * CK_K + 1;
+      const int hi = d_imin(base + CK_K - 1, r - 1);
+      double lpa[CK_K], lda[CK_K];
+      double s = ckS[(size_t)jb * 32];
+#pragma unroll
+      for (int u = 0; u < CK_K; u++) {
+        const int i = base + u;
+        if (i <= hi) {
+          const double2 pp = P[(size_t)(i - 1) * ps];
+          const double2 q = Q[(size_t)(i - 1) * ps];
+          double dplus = pp.x + s;
+          if (slowA && fabs(dplus) < pivmin) dplus = -pivmin;
+          const double lp = q.y / dplus;
+          double si = s * lp * q.x;
+          if (slowA && lp == 0.0) si = pp.y;
+          s = si - lambda;
+          lpa[u] = lp;
+          lda[u] = q.y;
+        }
+      }
+      if (base > 1)
+        for (int i = d_imax(base - CK_K, 1); i <= base - 1; i++) {
+          pf_l1(&P[(size_t)(i - 1) * ps]);
+          pf_l1(&Q[(size_t)(i - 1) * ps]);
+        }
+#pragma unroll
+      for (int u = CK_K - 1; u >= 0; u--) {
+        const int i = base + u;
+        if (go && i <= hi) {
+          const double ldi = lda[u];
+          double zi;
+          if (!slow) zi = -(lpa[u] * zp);
+          else if (zp == 0.0) zi = -(Q[(size_t)i * ps].y / ldi) * zpp;
+          else zi = -(lpa[u] * zp);
+          if ((fabs(zi) + fabs(zp)) * fabs(ldi) < gaptol) {
+            is1 = i + 1;
+            go = false;
+          } else {
+            ztz = ztz + zi * zi;
+            if (zout) zout[i - 1] = zi * nv;
+            zpp = zp;
+            zp = zi;
+          }
+        }
+      }
+    }
+  }
+  // downward solve: i = r .. n-1, z(i+1) from z(i)
+  {
+    double zc = 1.0, zcp = 0.0;   // z(i), z(i-1)
+    bool go = r <= n - 1;
+    for (int jb = (r - 1) / CK_K; go && jb <= (n - 2) / CK_K; jb++) {
+      const int base = jb * CK_K + 1;
+      const int lo = d_imax(base, r), hi = d_imin(base + CK_K - 1, n - 1);
+      double uma[CK_K], lda[CK_K];
+      double p = ckP[(size_t)jb * 32];
+#pragma unroll
+      for (int u = CK_K - 1; u >= 0; u--) {
+        const int i = base + u;
+        if (i >= lo && i <= hi) {
+          const double2 pp = P[(size_t)(i - 1) * ps];
+          const double2 q = Q[(size_t)(i - 1) * ps];
+          double dminus = pp.y + p;
+          if (slowB && fabs(dminus) < pivmin) dminus = -pivmin;
+          const double tmp = pp.x / dminus;
+          uma[u] = q.x * tmp;
+          lda[u] = q.y;
+          double pn = p * tmp - lambda;
+          if (slowB && tmp == 0.0) pn = pp.x - lambda;
+          p = pn;
+        }
+      }
+      if (base + CK_K <= n - 1)
+        for (int i = base + CK_K; i <= d_imin(base + 2 * CK_K - 1, n - 1); i++) {
+          pf_l1(&P[(size_t)(i - 1) * ps]);
+          pf_l1(&Q[(size_t)(i - 1) * ps]);
+        }
+#pragma unroll
+      for (int u = 0; u < CK_K; u++) {
+        const int i = base + u;
+        if (go && i >= lo && i <= hi) {
+          const double ldi = lda[u];
+          double zn;
+          if (!slow) zn = -(uma[u] * zc);
+          else if (zc == 0.0) zn = -(Q[(size_t)(i - 2) * ps].y / ldi) * zcp;
+          else zn = -(uma[u] * zc);
+          if ((fabs(zc) + fabs(zn)) * fabs(ldi) < gaptol) {
+            is2 = i;
+            go = false;
+          } else {
+            ztz = ztz + zn * zn;
+            if (zout) zout[i] = zn * nv;
+            zcp = zc;
+            zc = zn;
+          }
+        }
+      }
+    }
+  }
+  o->r = r;
+  o->mingma = mingma;
+  o->isupp1 = is1;
+  o->isupp2 = is2;
+  o->ztz = ztz;
+  const double tmp = 1.0 / ztz;
+  o->nrminv = sqrt(tmp);
+  o->resid = fabs(mingma) * o->nrminv;
+  o->rqcorr = mingma * tmp;
+  o->sawnan = slow;
 }
 
 // dlarrf, LAPACK 3.2.2 with NOFAIL (SRC/LAPACK/odrrf.f:140-378), one thread.

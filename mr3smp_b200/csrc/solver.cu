@@ -1441,15 +1441,16 @@ __global__ void k_group_tasks(int ncl, const ClusterDev *cl, ClsScratch xs, SngC
 // k_sng_bisect serves between rounds.  So no lane waits for another lane's
 // extra iterations, and the warps stay full in every round.
 //
-// Each warp owns scratch of 2 x nmax x 32 doubles laid out [array][row]
-// [lane]: the lanes sweep the rows by absolute index, so every scratch
-// access is one coalesced 256-byte row.  Consecutive records of a list
-// mostly share a block; a warp whose lanes hold blocks of different sizes
-// sweeps the largest.  Finished eigenvectors leave through a shared-memory
-// transpose, so the Z columns are written in coalesced rows.
+// A lane's dlar1v keeps only checkpoints (dv_r1c_*): each warp owns scratch
+// of 3 x (nmax/CK_K + 1) x 32 doubles laid out [array][block][lane], and the
+// lanes sweep the blocks by absolute index, so a checkpoint access is one
+// coalesced 256-byte row.  Consecutive records of a list mostly share a
+// block; a warp whose lanes hold blocks of different sizes sweeps the
+// largest.  An accepted eigenvector is recomputed once more and written by
+// its lane straight to its column of Z; the warp zeroes the rows outside the
+// support in coalesced rows.
 // ------------------------------------------------------------------------
 #define SNG_WARPS 8
-#define SNG_TILE_LD 33
 #define SNG_ROUNDS (MR3_MAXITER + 1)   // MAXITER loop calls and the step-2 call
 enum { SF_USEDBS = 1, SF_USEDRQ = 2, SF_NEEDBS = 4, SF_STEP2 = 8 };
 
@@ -1579,16 +1580,18 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, const ProbDev *prob
             const int *Zindex, SngState *sst, const int *act0, const int *act1,
             unsigned char *flag, SngCounters *sc, double *scratch, long long nmax,
             unsigned long long *stats) {
-  extern __shared__ double sm_tile[];
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  double *tile = sm_tile + (threadIdx.x >> 5) * 32 * SNG_TILE_LD;
   const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-  double *X = scratch + gw * 2 * nmax * 32 + lane;
-  double *Y = X + nmax * 32;
+  const long long nck = nmax / CK_K + 1;   // checkpoint blocks per lane
+  r1c_ck ck;
+  ck.S = scratch + gw * 3 * nck * 32 + lane;
+  ck.I = ck.S + nck * 32;
+  ck.P = ck.I + nck * 32;
   const int *Ain = in ? act1 : act0;
   const int nin = sc->nin;
   const double rqtol = 2.0 * MR3_EPS;
+  __shared__ SngState sm_st[SNG_WARPS * 32];
   unsigned long long w_r1v = 0, w_sweep = 0, w_chunks = 0;
   for (;;) {
     int base = 0;
@@ -1600,42 +1603,54 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, const ProbDev *prob
     // pointers) and do no work
     const int j = active ? base + lane : base;
     const int idx = FIRST ? j : Ain[j];
-    const SngDev S = sng[idx];
-    const ClusterDev C = cl[S.cl];
-    const BlockDev &B = blocks[C.blk];
-    const ProbDev *p = &probs[B.prob];
-    const int nb = B.nbl;
-    const double pivmin = p->pivmin;
+    const int s = sng[idx].slot;
+    int nb;
+    double pivmin, lam_call, gaptol;
     const double2 *P, *Q;
-    int ps;
-    own_rrr(C, B, RP, RQ, arena, &P, &Q, &ps);
-    const int s = S.slot;
-    SngState st;
-    if (FIRST) {
-      st.lambda = Wsh[s]; st.wsh = st.lambda; st.werr = Werr[s];
-      st.left = st.lambda - st.werr; st.right = st.lambda + st.werr;
-      // the reference compares the eigenvalue index with the block's first
-      // and last row (SRC/process_singleton.c:142-157); W slots and rows of a
-      // problem start at the same offset, so the same comparison is s == row
-      const double lgap = (s == B.ibgn) ? MR3_EPS * fmax(fabs(st.left), fabs(st.right)) : S.lgap;
-      const double rgap = (s == B.iend) ? MR3_EPS * fmax(fabs(st.left), fabs(st.right)) : Wgap[s];
-      st.gap = fmin(lgap, rgap);
-      st.gaptol = (s == B.ibgn || s == B.iend) ? 0.0 : st.gap * MR3_EPS;
-      st.bstres = 0.0; st.bstw = 0.0; st.resid = 0.0;
-      st.r = 0; st.k = 1; st.flags = 0; st.pad = 0;
-    } else {
-      st = sst[idx];
+    int ps, r_in;
+    bool usedBS;
+    {
+      // the loop state waits in shared memory while the sweeps run, so that
+      // they have the registers to themselves
+      const SngDev S = sng[idx];
+      const ClusterDev C = cl[S.cl];
+      const BlockDev &B = blocks[C.blk];
+      nb = B.nbl;
+      pivmin = probs[B.prob].pivmin;
+      own_rrr(C, B, RP, RQ, arena, &P, &Q, &ps);
+      SngState st;
+      if (FIRST) {
+        st.lambda = Wsh[s]; st.wsh = st.lambda; st.werr = Werr[s];
+        st.left = st.lambda - st.werr; st.right = st.lambda + st.werr;
+        // the reference compares the eigenvalue index with the block's first
+        // and last row (SRC/process_singleton.c:142-157); W slots and rows of
+        // a problem start at the same offset, so the same comparison is s == row
+        const double lgap = (s == B.ibgn) ? MR3_EPS * fmax(fabs(st.left), fabs(st.right)) : S.lgap;
+        const double rgap = (s == B.iend) ? MR3_EPS * fmax(fabs(st.left), fabs(st.right)) : Wgap[s];
+        st.gap = fmin(lgap, rgap);
+        st.gaptol = (s == B.ibgn || s == B.iend) ? 0.0 : st.gap * MR3_EPS;
+        st.bstres = 0.0; st.bstw = 0.0; st.resid = 0.0;
+        st.r = 0; st.k = 1; st.flags = 0; st.pad = 0;
+      } else {
+        st = sst[idx];
+      }
+      sm_st[threadIdx.x] = st;
+      usedBS = (st.flags & SF_USEDBS) != 0;
+      lam_call = (st.flags & SF_STEP2) ? st.bstw : st.lambda;
+      r_in = st.r;
+      gaptol = st.gaptol;
     }
-    const bool step2 = (st.flags & SF_STEP2) != 0;
-    const bool usedBS = (st.flags & SF_USEDBS) != 0;
-    const double lam_call = step2 ? st.bstw : st.lambda;
-    r1v_state rs;
-    rs.r = 0; rs.mingma = 0.0; rs.sawnan = false;
+    r1c_state rs;
+    rs.r = 0; rs.mingma = 0.0; rs.sawnan = false; rs.slowA = false; rs.slowB = false;
     int negc = 0;
-    dv_r1v_factor(active, nb, lam_call, P, Q, ps, pivmin, !usedBS, st.r, X, Y, &negc, &rs);
+    dv_r1c_factor(active, nb, lam_call, P, Q, ps, pivmin, !usedBS, r_in, ck, &negc, &rs);
     dlar1v_out o;
     o.isupp1 = 1; o.isupp2 = nb; o.nrminv = 0.0; o.r = 0; o.resid = 0.0; o.rqcorr = 0.0;
-    dv_r1v_solve(active, nb, Q, ps, st.gaptol, X, Y, rs, &o);
+    if (active)
+      dv_r1c_solve(nb, lam_call, P, Q, ps, pivmin, gaptol, rs.r, rs.sawnan, rs.slowA, rs.slowB,
+                   ck.S, ck.P, rs.mingma, nullptr, 0.0, &o);
+    SngState st = sm_st[threadIdx.x];
+    const bool step2 = (st.flags & SF_STEP2) != 0;
     const int nb_sweep = __reduce_max_sync(full, active ? nb : 0);
     if (lane == 0) { w_chunks++; w_sweep += nb_sweep; }
     bool done = false, tobs = false;
@@ -1683,51 +1698,39 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, const ProbDev *prob
     // finished eigenvectors out
     const unsigned fin = __ballot_sync(full, done);
     if (!fin) continue;
+    const ClusterDev &Cf = cl[sng[idx].cl];
+    const BlockDev &B = blocks[Cf.blk];
+    const ProbDev *p = &probs[B.prob];
     const int bl0 = B.ibgn - p->off;   // block's first row inside the problem
     int zind = 0;
     if (done) {
       Wsh[s] = st.lambda;
       Werr[s] = st.werr;
       Wgap[s] = st.gap;
-      W[s] = st.lambda + C.sigma;
+      W[s] = st.lambda + Cf.sigma;
       zind = Zindex[s];
       p->Zsupp[2 * (size_t)zind] = o.isupp1 + bl0;
       p->Zsupp[2 * (size_t)zind + 1] = o.isupp2 + bl0;
     }
+    // the accepted vector: z of the support again, normalised, straight to
+    // the lane's column of Z (the same operations as the solve above)
     double *const Zp = p->Z;
     const int ldz = p->ldz, np = p->n;
-    const int a1 = o.isupp1, a2 = o.isupp2, rr = o.r;
-    const double nv = o.nrminv;
-    const int nbw = __reduce_max_sync(full, done ? nb : 0);
-    for (int k0 = 1; k0 <= nbw; k0 += 32) {
-#pragma unroll 4
-      for (int jj = 0; jj < 32; jj++) {
-        const int kk = k0 + jj;
-        double val = 0.0;
-        if (done && kk <= nb && kk >= a1 && kk <= a2) val = dv_zget(X, Y, rr, kk) * nv;
-        tile[jj * SNG_TILE_LD + lane] = val;
-      }
-      __syncwarp();
-      for (unsigned m = fin; m; m &= m - 1) {
-        const int v = __ffs(m) - 1;
-        const int zc = __shfl_sync(full, zind, v);
-        const int b0 = __shfl_sync(full, bl0, v), nbv = __shfl_sync(full, nb, v);
-        const int ldv = __shfl_sync(full, ldz, v);
-        double *Zv = (double *)__shfl_sync(full, (unsigned long long)Zp, v);
-        if (k0 + lane <= nbv) Zv[(size_t)zc * ldv + b0 + k0 - 1 + lane] = tile[lane * SNG_TILE_LD + v];
-      }
-      __syncwarp();
+    if (done) {
+      dlar1v_out o2;
+      dv_r1c_solve(nb, lam_call, P, Q, ps, pivmin, st.gaptol, rs.r, rs.sawnan, rs.slowA, rs.slowB,
+                   ck.S, ck.P, rs.mingma, Zp + (size_t)zind * ldz + bl0, o.nrminv, &o2);
     }
-    // rows of the problem outside this block are zero
+    // rows of the column outside the support (and outside the block) are zero
+    const int z1 = bl0 + o.isupp1 - 1, z2 = bl0 + o.isupp2;   // support rows [z1, z2)
     for (unsigned m = fin; m; m &= m - 1) {
       const int v = __ffs(m) - 1;
-      const int npv = __shfl_sync(full, np, v), nbv = __shfl_sync(full, nb, v);
-      if (npv <= nbv) continue;
-      const int zc = __shfl_sync(full, zind, v), b0 = __shfl_sync(full, bl0, v);
+      const int npv = __shfl_sync(full, np, v), zc = __shfl_sync(full, zind, v);
+      const int a = __shfl_sync(full, z1, v), b = __shfl_sync(full, z2, v);
       const int ldv = __shfl_sync(full, ldz, v);
       double *Zc = (double *)__shfl_sync(full, (unsigned long long)Zp, v) + (size_t)zc * ldv;
-      for (int row = lane; row < b0; row += 32) Zc[row] = 0.0;
-      for (int row = b0 + nbv + lane; row < npv; row += 32) Zc[row] = 0.0;
+      for (int row = lane; row < a; row += 32) Zc[row] = 0.0;
+      for (int row = b + lane; row < npv; row += 32) Zc[row] = 0.0;
     }
     __syncwarp();
   }
@@ -2090,13 +2093,8 @@ extern "C" int mr3_cuda_ctx_create(int device, mr3_cuda_ctx **out) {
     mr3_cuda_ctx_destroy(c);
     return MR3_EMISC;
   }
-  cudaFuncSetAttribute(k_sng_round<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       SNG_WARPS * 32 * SNG_TILE_LD * (int)sizeof(double));
-  cudaFuncSetAttribute(k_sng_round<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       SNG_WARPS * 32 * SNG_TILE_LD * (int)sizeof(double));
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &nb, k_sng_round<false>, SNG_WARPS * 32, SNG_WARPS * 32 * SNG_TILE_LD * sizeof(double)) ==
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_sng_round<false>, SNG_WARPS * 32, 0) ==
           cudaSuccess &&
       nb > 0)
     c->sng_ctas_per_sm = nb;
@@ -2429,8 +2427,8 @@ extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *s
     if (c->h_sc->n_unit > 0)
       LAUNCH(k_unitvec, c->h_sc->n_unit, 256, c->unit_list, c->sc, c->probs, c->blocks, c->iblk,
              c->Zindex);
-    // singleton scratch: 2 x nmax x 32 doubles per persistent warp
-    const size_t per_warp = 2ull * (size_t)nmaxV * 32ull;
+    // singleton scratch: the checkpoints of 32 lanes per persistent warp
+    const size_t per_warp = 3ull * ((size_t)nmaxV / CK_K + 1) * 32ull;
     const size_t budget = (size_t)8 << 30;   // bytes
     // persistent warps: no more than can be resident at once
     const size_t resident = (size_t)c->nsm * (size_t)c->sng_ctas_per_sm * SNG_WARPS;
@@ -2477,7 +2475,7 @@ extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *s
         const int nsng = c->h_sc->n_sng;
         const int ctas_all = (int)(nwarps / SNG_WARPS);
         const int ctas_first = std::min(ctas_all, (nsng + 32 * SNG_WARPS - 1) / (32 * SNG_WARPS));
-        const size_t smem = SNG_WARPS * 32 * SNG_TILE_LD * sizeof(double);
+        const size_t smem = 0;
         const int bis_ctas = c->nsm * 4;
         const int nblk = (nsng + LIST_T - 1) / LIST_T;
         for (int rd = 0; rd < SNG_ROUNDS; rd++) {

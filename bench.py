@@ -148,6 +148,93 @@ def cpu_reference(problems, budget_s: float, check: bool = True):
     return pairs / el, info
 
 
+SERVE_SIZES = (64, 256, 1024, 4096, 16384)
+SERVE_PROBS = (0.4, 0.3, 0.2, 0.08, 0.02)
+
+
+def run_serving(M, wl, rate: float, count: int, seed: int):
+    """Poisson stream of independent requests through the serving API.
+
+    Sizes n in SERVE_SIZES with SERVE_PROBS, D, E ~ U(-1,1), range
+    alternating A and I (il = 1, iu = ceil(n/10)), results to host memory.
+    Latency = arrival to result ready (queueing in the client included)."""
+    import threading
+    rng = np.random.default_rng(seed)
+    ns = rng.choice(SERVE_SIZES, size=count, p=SERVE_PROBS)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=count))
+    reqs = []
+    for k, n in enumerate(ns):
+        D, E = wl.uniform(int(n), seed=seed * 100003 + k)
+        if k % 2 == 0:
+            reqs.append(dict(jobz="V", range="A", D=D, E=E))
+        else:
+            reqs.append(dict(jobz="V", range="I", D=D, E=E, il=1, iu=-(-int(n) // 10)))
+    S = M.Server(pinned=True)
+    # page-locked result buffers, recycled per request shape
+    pool = {}
+    plock = threading.Lock()
+
+    def shape(p):
+        return (len(p["D"]), p["range"], p.get("iu", 0))
+
+    for n in SERVE_SIZES:   # warm-up: workspaces of both workers, one buffer set each
+        D, E = wl.uniform(n, seed=1)
+        for p in (dict(jobz="V", range="A", D=D, E=E),
+                  dict(jobz="V", range="I", D=D, E=E, il=1, iu=-(-n // 10))):
+            (info, m, arr), _ = S.poll(S.submit(p), wait=True, raw=True)
+            pool.setdefault(shape(p), []).append(arr)
+    lat = [None] * count
+    pairs = [0] * count
+    sub = [None] * count
+    done_t = [0.0] * count
+    ready = threading.Semaphore(0)
+
+    def poller():
+        for k in range(count):
+            ready.acquire()
+            t, t_arr, t_sub = sub[k]
+            (info, m, arr), l = S.poll(t, wait=True, raw=True)
+            done_t[k] = time.perf_counter()
+            lat[k] = (t_sub - t_arr) * 1e3 + l
+            pairs[k] = m if info == 0 else 0
+            with plock:
+                pool.setdefault(shape(reqs[k]), []).append(arr)
+
+    th = threading.Thread(target=poller)
+    th.start()
+    t0 = time.perf_counter()
+    for k in range(count):
+        ta = t0 + arrivals[k]
+        d = ta - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        with plock:
+            free = pool.get(shape(reqs[k]))
+            arr = free.pop() if free else None
+        ts = time.perf_counter()
+        sub[k] = (S.submit(reqs[k], arr), ta, ts)
+        ready.release()
+    th.join()
+    st = S.stats()
+    S.close()
+    el = max(done_t) - t0
+    lat_a = np.array(lat)
+    by_n = {}
+    for n in SERVE_SIZES:
+        sel = lat_a[ns == n]
+        if len(sel):
+            by_n[str(n)] = {"count": int(len(sel)), "p50_ms": float(np.percentile(sel, 50)),
+                            "p99_ms": float(np.percentile(sel, 99))}
+    return {"rate_per_s": rate, "requests": count, "p50_ms": float(np.percentile(lat_a, 50)),
+            "p99_ms": float(np.percentile(lat_a, 99)), "mean_ms": float(lat_a.mean()),
+            "by_n": by_n,
+            "eigenpairs_per_s": float(sum(pairs) / el), "requests_per_s": count / el,
+            "batches": st["batches"],
+            "mix": "n in {64,256,1024,4096,16384} w.p. {.4,.3,.2,.08,.02}; range A/I alternating "
+                   "(I: il=1, iu=ceil(n/10)); D,E U(-1,1); results to host memory",
+            "api": "mr3_server_submit/poll (C ABI)"}
+
+
 def _workload(args):
     return (f"mixed batch: {args.count} tridiagonals, n log-uniform [32,{args.nmax}], "
             "25% 1-2-1, D,E uniform(-1,1), jobz=V range=A")
@@ -202,6 +289,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--serve-rate", type=float, default=40.0)
+    ap.add_argument("--serve-count", type=int, default=400)
+    ap.add_argument("--no-serve", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -397,6 +487,10 @@ def main():
                "steps": args.e2e_steps}
         del keep, hp
 
+    serving = None
+    if rank == 0 and not args.no_serve:
+        serving = run_serving(M, wl, args.serve_rate, args.serve_count, args.seed)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         _, cpu = cpu_reference(problems, args.cpu_seconds)
@@ -419,7 +513,7 @@ def main():
                          f"{zbytes / 1e9:.1f} GB of Z"},
         "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "roofline": roof,
         "roofline_hbm": roof_hbm, "fp64_peaks": {"fma_tflops": fma_tflops, "div_gops": div_gops},
-        "percall": percall, "cpu_baseline": cpu,
+        "percall": percall, "serving": serving, "cpu_baseline": cpu,
         "kernels_ms_per_step": {k: v[0] / args.steps for k, v in
                                 sorted(kern.items(), key=lambda kv: -kv[1][0])},
         "work_counters": dict(zip(groups, ctr)),

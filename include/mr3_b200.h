@@ -59,6 +59,29 @@ int mr3_batched(int nprob, mr3_host_prob *probs);
  * (a cudaStream_t or NULL). */
 int mr3_batched_device(int nprob, mr3_cuda_prob *probs, void *stream);
 
+/* Serving (no counterpart in the reference, which answers one call at a
+ * time; SRC/mrrr.c:87-296 is the per-request computation).  A server takes
+ * a stream of independent requests and solves them in batches as they
+ * arrive: one worker thread per size class (n <= 2048, and larger) takes
+ * the oldest queued requests of its class that fit its share of the device
+ * memory budget (budget_bytes; 0 = 120 GB) and solves them in one pass.
+ * Results are those of a call alone.
+ *
+ * mr3_server_submit: the request (an mr3_host_prob as for mr3_batched) and
+ * its arrays must stay valid and untouched until poll reports it done.
+ * Returns a ticket >= 1, or -1 bad arguments, -2 request larger than its
+ * class's budget, -3 server stopping, -4 out of host memory.
+ * mr3_server_poll: 1 done (req->info, req->m, ... are set), 0 pending,
+ * -1 unknown ticket; wait = 1 blocks until done; latency_ms (or NULL)
+ * receives the submit-to-done time.
+ * mr3_server_destroy finishes every queued request, then stops. */
+typedef struct mr3_server mr3_server;
+int  mr3_server_create(int device, size_t budget_bytes, mr3_server **out);
+long long mr3_server_submit(mr3_server *s, mr3_host_prob *req);
+int  mr3_server_poll(mr3_server *s, long long ticket, int wait, double *latency_ms);
+int  mr3_server_stats(mr3_server *s, long long *submitted, long long *solved, long long *batches);
+void mr3_server_destroy(mr3_server *s);
+
 /* Kernels launched by the calling thread's last solve (diagnostics). */
 long long mr3_last_launches(void);
 

@@ -77,6 +77,9 @@ int  mr3_cuda_copy2d(mr3_cuda_ctx *ctx, void *dst, size_t dpitch, const void *sr
                      size_t spitch, size_t width, size_t height, int dir);
 int  mr3_cuda_sync(mr3_cuda_ctx *ctx);
 
+/* Makes the context's device current for the calling thread. */
+int  mr3_cuda_set_device(mr3_cuda_ctx *ctx);
+
 /* Second stream of the context for copies that overlap the solves, and the
  * events that order the two.  stream: MR3_STREAM_MAIN (the stream of the
  * copies above and of solves given stream NULL) or MR3_STREAM_COPY.

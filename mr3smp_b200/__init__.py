@@ -268,6 +268,121 @@ class Solver:
         return kern, counters
 
 
+def _host_request(pb: dict, pinned: bool = False, arrays=None):
+    """Build an HostProb for one problem dict; returns (struct, arrays kept
+    alive).  ``arrays`` (D, E, W, Z, Zsupp of a finished request of the same
+    shape, see Server.poll(raw=True)) are reused instead of new buffers."""
+    def alloc(n, dtype):
+        if arrays is not None:
+            return alloc.pool.pop(0)
+        if pinned:
+            import torch
+            t = torch.empty(max(n, 1), dtype=torch.float64 if dtype == np.float64 else torch.int32,
+                            pin_memory=True)
+            return t.numpy()
+        return np.zeros(max(n, 1), dtype=dtype)
+    if arrays is not None:
+        alloc.pool = list(arrays[:5])
+    n = int(len(pb["D"]))
+    D = alloc(n, np.float64)
+    D[:n] = pb["D"]
+    E = alloc(n, np.float64)
+    E[:] = 0.0
+    E[: min(n, len(pb["E"]))] = np.asarray(pb["E"], dtype=np.float64)[:n]
+    jz, rg = pb["jobz"], pb["range"]
+    il, iu = int(pb.get("il", 1)), int(pb.get("iu", 1))
+    want_z = jz[0] in "Vv"
+    W = alloc(n, np.float64)
+    Z = alloc(_ncols(jz, rg, n, il, iu) * n if want_z else 1, np.float64)
+    Zs = alloc(2 * n, np.int32)
+    h = HostProb()
+    h.jobz, h.range, h.n, h.il, h.iu = jz[0].encode(), rg[0].encode(), n, il, iu
+    h.tryrac, h.ldz = int(pb.get("tryrac", 0)), n
+    h.vl, h.vu = float(pb.get("vl", 0.0)), float(pb.get("vu", 0.0))
+    h.D, h.E, h.W = D.ctypes.data_as(_pd), E.ctypes.data_as(_pd), W.ctypes.data_as(_pd)
+    h.Z, h.Zsupp = Z.ctypes.data_as(_pd), Zs.ctypes.data_as(_pi)
+    return h, (D, E, W, Z, Zs, n, jz)
+
+
+def _host_result(h, keep) -> dict:
+    D, E, W, Z, Zs, n, jz = keep
+    m = h.m if h.info == 0 else 0
+    out = dict(info=h.info, m=m, W=W[:m].copy(), D=D[:n].copy(), E=E[:n].copy(), vl=h.vl_out,
+               vu=h.vu_out, il=h.il_out, iu=h.iu_out, tryrac=h.tryrac_out)
+    if jz[0] in "Vv":
+        out["Z"] = Z[: n * m].reshape(m, n).T.copy() if m > 0 else np.zeros((n, 0))
+        out["Zsupp"] = Zs[: 2 * m].copy()
+    return out
+
+
+class Server:
+    """Serving handle (mr3_server_*): requests solved in batches as they arrive.
+
+    ``submit(problem)`` takes a problem dict as :func:`mrrr_batched` does and
+    returns a ticket; ``poll(ticket, wait)`` returns ``(result, latency_ms)``
+    once the request is done (``(None, None)`` while pending).  Results are
+    those of a call alone.
+    """
+
+    def __init__(self, device: int = 0, budget_bytes: int = 0, pinned: bool = False):
+        L = lib()
+        L.mr3_server_create.restype = C.c_int
+        L.mr3_server_create.argtypes = [C.c_int, C.c_size_t, C.POINTER(C.c_void_p)]
+        L.mr3_server_submit.restype = C.c_longlong
+        L.mr3_server_submit.argtypes = [C.c_void_p, C.POINTER(HostProb)]
+        L.mr3_server_poll.restype = C.c_int
+        L.mr3_server_poll.argtypes = [C.c_void_p, C.c_longlong, C.c_int, C.POINTER(C.c_double)]
+        L.mr3_server_stats.restype = C.c_int
+        L.mr3_server_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong),
+                                       C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+        L.mr3_server_destroy.argtypes = [C.c_void_p]
+        self._L = L
+        self._pinned = pinned
+        self._h = C.c_void_p()
+        rc = L.mr3_server_create(device, budget_bytes, C.byref(self._h))
+        if rc != 0:
+            raise MR3Error(f"mr3_server_create failed ({rc})")
+        self._live = {}
+
+    def submit(self, problem: dict, arrays=None) -> int:
+        h, keep = _host_request(problem, self._pinned, arrays)
+        t = self._L.mr3_server_submit(self._h, C.byref(h))
+        if t < 1:
+            raise MR3Error(f"mr3_server_submit refused the request ({t})")
+        self._live[t] = (h, keep)
+        return t
+
+    def poll(self, ticket: int, wait: bool = True, raw: bool = False):
+        """(result dict, latency ms), or with raw=True ((info, m, arrays),
+        latency ms) where arrays can be passed to submit() again."""
+        lat = C.c_double(0.0)
+        rc = self._L.mr3_server_poll(self._h, ticket, 1 if wait else 0, C.byref(lat))
+        if rc < 0:
+            raise MR3Error(f"unknown ticket {ticket}")
+        if rc == 0:
+            return None, None
+        h, keep = self._live.pop(ticket)
+        if raw:
+            return (h.info, h.m, keep[:5]), lat.value
+        return _host_result(h, keep), lat.value
+
+    def stats(self):
+        a, b, c = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        self._L.mr3_server_stats(self._h, C.byref(a), C.byref(b), C.byref(c))
+        return {"submitted": a.value, "solved": b.value, "batches": c.value}
+
+    def close(self):
+        if self._h:
+            self._L.mr3_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def device_batch(host_problems, device: str = "cuda", with_z: bool = True):
     """Lay out a list of (D, E) numpy pairs on the device for batched solves.
 

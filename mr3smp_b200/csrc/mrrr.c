@@ -105,11 +105,12 @@ static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 #define PIPE_CHUNK_BYTES ((size_t)40 << 30)
 #define PIPE_MAX_CHUNKS 16
 
-int mr3_batched(int nprob, mr3_host_prob *hp)
+/* One batched solve of host problems on a given context (the body of
+ * mr3_batched, also used by the serving workers, which own their contexts). */
+__attribute__((visibility("hidden"))) int mr3__batched_on(mr3_cuda_ctx *ctx, int nprob, mr3_host_prob *hp)
 {
-  int i, c, slot, rc = MR3_OK, worst = 0, nchunk = 1;
+  int i, c, rc = MR3_OK, worst = 0, nchunk = 1;
   int cbeg[PIPE_MAX_CHUNKS + 1];
-  mr3_cuda_ctx *ctx;
   mr3_cuda_prob *dp;
   size_t nrow = 0, nzs = 0, ztot = 0, zmax = 0, small, pipe_min, pipe_chunk;
   size_t *zb, *orow, *ozs;
@@ -166,9 +167,7 @@ int mr3_batched(int nprob, mr3_host_prob *hp)
     for (i = cbeg[c]; i < cbeg[c + 1]; i++) z += zb[i];
     if (z > zmax) zmax = z;
   }
-  slot = pool_acquire();
-  if (slot < 0) { free(dp); free(zb); return MR3_EMISC; }
-  ctx = g_pool[slot].ctx;
+  if (!ctx) { free(dp); free(zb); return MR3_EMISC; }
   /* device layout of the small arrays, mirrored by the staging buffer:
    * D | E | W (nrow doubles each) | Zsupp (nzs ints) */
   small = 3 * nrow * sizeof(double) + nzs * sizeof(int);
@@ -220,7 +219,15 @@ int mr3_batched(int nprob, mr3_host_prob *hp)
       mr3_host_prob *h = &hp[i];
       mr3_cuda_prob *q = &dp[i];
       if (q->jobz != MR3_JOB_V || q->info != MR3_OK || q->m <= 0) continue;
-      if (mr3_cuda_copy2d_on(ctx, MR3_STREAM_COPY, h->Z, (size_t)h->ldz * sizeof(double), q->Z,
+      /* one contiguous copy when the caller's Z has no padding between
+       * columns (a pitched copy into pageable memory goes column by column) */
+      if (h->ldz == q->ldz) {
+        if (mr3_cuda_copy_on(ctx, MR3_STREAM_COPY, h->Z, q->Z,
+                             (size_t)h->ldz * (size_t)q->m * sizeof(double), 1) != MR3_OK) {
+          rc = MR3_EMISC;
+          goto done;
+        }
+      } else if (mr3_cuda_copy2d_on(ctx, MR3_STREAM_COPY, h->Z, (size_t)h->ldz * sizeof(double), q->Z,
                              (size_t)q->ldz * sizeof(double), (size_t)h->n * sizeof(double),
                              (size_t)q->m, 1) != MR3_OK) {
         rc = MR3_EMISC;
@@ -255,7 +262,6 @@ int mr3_batched(int nprob, mr3_host_prob *hp)
   }
 done:
   if (rc != MR3_OK) mr3_cuda_sync_all(ctx);
-  pool_release(slot);
   for (i = 0; i < nprob; i++) {
     if (rc != MR3_OK) hp[i].info = dp[i].jobz < 0 ? MR3_EARG : MR3_EMISC;
     if (hp[i].info > worst) worst = hp[i].info;
@@ -263,6 +269,17 @@ done:
   free(dp);
   free(zb);
   return worst;
+}
+
+int mr3_batched(int nprob, mr3_host_prob *hp)
+{
+  int rc, slot;
+  if (nprob <= 0) return 0;
+  slot = pool_acquire();
+  if (slot < 0) return MR3_EMISC;
+  rc = mr3__batched_on(g_pool[slot].ctx, nprob, hp);
+  pool_release(slot);
+  return rc;
 }
 
 int mr3_batched_device(int nprob, mr3_cuda_prob *probs, void *stream)

@@ -2175,6 +2175,11 @@ extern "C" int mr3_cuda_sync(mr3_cuda_ctx *c) {
   return MR3_OK;
 }
 
+extern "C" int mr3_cuda_set_device(mr3_cuda_ctx *c) {
+  if (!c) return MR3_EMISC;
+  return cudaSetDevice(c->device) == cudaSuccess ? MR3_OK : MR3_EMISC;
+}
+
 static cudaStream_t ctx_stream(mr3_cuda_ctx *c, int which) {
   return which == MR3_STREAM_COPY ? c->aux : c->own;
 }

@@ -121,3 +121,32 @@ def residual_orth(D, E, W, Z):
     G = Z.T @ Z
     orth = np.abs(G - np.eye(m)).max() / (n * eps)
     return float(res), float(orth)
+
+
+def residual_orth_torch(D, E, W, Z, device="cuda", chunk=4096):
+    """residual_orth on the GPU (torch, fp64) for large problems: the same
+    two scaled quantities; Z may be a host array (n x m) or a torch tensor."""
+    import torch
+    n = len(D)
+    eps = np.finfo(np.float64).eps
+    Zt = torch.as_tensor(Z, device=device, dtype=torch.float64)
+    m = Zt.shape[1]
+    if m == 0:
+        return 0.0, 0.0
+    d = torch.as_tensor(np.asarray(D, dtype=np.float64), device=device)
+    e = torch.as_tensor(np.asarray(E[: n - 1], dtype=np.float64), device=device)
+    w = torch.as_tensor(np.asarray(W, dtype=np.float64), device=device)
+    tn = max(float(d.abs().max()), float(e.abs().max()) if n > 1 else 0.0) or 1.0
+    res = 0.0
+    for c0 in range(0, m, chunk):
+        Zc = Zt[:, c0:c0 + chunk]
+        TZ = d[:, None] * Zc
+        TZ[:-1] += e[:, None] * Zc[1:]
+        TZ[1:] += e[:, None] * Zc[:-1]
+        res = max(res, float((TZ - Zc * w[None, c0:c0 + chunk]).abs().max()))
+    orth = 0.0
+    for c0 in range(0, m, chunk):
+        G = Zt[:, c0:c0 + chunk].T @ Zt
+        G[:, c0:c0 + chunk] -= torch.eye(G.shape[0], device=device, dtype=torch.float64)
+        orth = max(orth, float(G.abs().max()))
+    return res / (n * eps * tn), orth / (n * eps)

@@ -64,3 +64,11 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(M, "_lib", None)
     with pytest.raises(M.MR3Error):
         M.lib()
+
+
+def test_server_create_fails_cleanly_without_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(M.MR3Error):
+        M.Server()

@@ -393,11 +393,19 @@ def main():
         avg_ms = tms / max(tcnt, 1)
         per_launch = divs / max(tcnt, 1)
         achieved = per_launch / (avg_ms * 1e-3) * 1e-9
+        traffic = None
+        if tname == "k_sng_round":
+            # DRAM bytes per dlar1v row of the round kernels, measured with ncu
+            # (dram__bytes_read.sum + dram__bytes_write.sum) on a 256-problem
+            # mixed batch (n <= 1024), scaled by this run's dlar1v rows
+            traffic = {"bytes_per_launch": 28.1 * ctr[4][2] / max(tcnt, 1),
+                       "source": "ncu on a 256-problem mixed batch: 28.1 B per dlar1v row, "
+                                 "scaled by the live dlar1v-row counter"}
         roof = {"bound": "fp64-div", "kernel": tname, "achieved": achieved,
                 "peak": div_gops, "unit": "Gdiv/s",
                 "frac": (achieved / div_gops) if div_gops else None,
                 "peak_source": "measured in-run (independent IEEE double divisions)",
-                "traffic": None, "avg_launch_ms": avg_ms, "launches": tcnt,
+                "traffic": traffic, "avg_launch_ms": avg_ms, "launches": tcnt,
                 "algorithmic_divisions_per_launch": per_launch}
     hbm = peaks.get("hbm_gbs")
     roof_hbm = {"bound": "hbm", "what": "Z written per step / step time", "achieved":

@@ -46,6 +46,27 @@ def _dist():
     return ws, rank, local
 
 
+def rank_batch(wl, count: int, seed: int, nmax: int, rank: int):
+    """This rank's share of the job: an independent batch seeded seed + rank
+    (problems are independent; ranks exchange nothing)."""
+    return wl.mixed_batch(count, seed=seed + rank, nmax=nmax)
+
+
+def job_throughput(dist, device, ms_total: float, steps: int, pairs_per_step: int):
+    """Whole-job eigenpairs/s: the eigenpairs of all ranks over the slowest
+    rank's time.  Returns (value, ms_per_step)."""
+    import torch
+    ms, pairs = float(ms_total), float(pairs_per_step)
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        p = torch.tensor([pairs], dtype=torch.float64, device=device)
+        dist.all_reduce(p, op=dist.ReduceOp.SUM)
+        ms, pairs = float(t.item()), float(p.item())
+    ms_per_step = ms / steps
+    return pairs / (ms_per_step * 1e-3), ms_per_step
+
+
 def _stratified(ns, count):
     """Indices of `count` problems spread evenly over the batch sorted by n."""
     order = np.argsort(np.asarray(ns), kind="stable")
@@ -311,7 +332,7 @@ def main():
     peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
 
     # workload: this rank's batch
-    batch = wl.mixed_batch(args.count, seed=args.seed + rank, nmax=args.nmax)
+    batch = rank_batch(wl, args.count, args.seed, args.nmax, rank)
     problems = [(D, E) for D, E, _ in batch]
     ns = [len(D) for D, E in problems]
     pairs_per_step = int(sum(ns))
@@ -353,13 +374,7 @@ def main():
     clocks = _clocks_stop(cproc, cpath)
     kern, ctr = S.profile_read()
     S.profile(False)
-    ms_max = ms
-    if dist:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    ms_per_step = ms_max / args.steps
-    value = ws * pairs_per_step / (ms_per_step * 1e-3)
+    value, ms_per_step = job_throughput(dist, "cuda", ms, args.steps, pairs_per_step)
 
     # roofline: the dominant kernel, algorithmic divisions per second
     div_gops = fma_tflops = None
@@ -489,7 +504,10 @@ def main():
         for _ in range(args.e2e_steps):
             e2e_step()
         el = (time.perf_counter() - t0) / args.e2e_steps
+        # measured on rank 0 (its page-locked copy of the batch); with N ranks the
+        # job figure is N times rank 0's, the ranks' batches being alike
         e2e = {"value": ws * pairs_per_step / el, "unit": "eigenpairs/s",
+               "measured_on": "rank 0" if ws > 1 else "the only rank",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "ms_per_step": el * 1e3, "api": "mr3_batched (C ABI), pinned host buffers",
                "steps": args.e2e_steps}

@@ -385,11 +385,10 @@ def main():
     if L.mr3_cuda_fp64_peaks(local, ctypes.byref(a), ctypes.byref(b)) == 0:
         fma_tflops, div_gops = a.value, b.value
     groups = M.Solver.KERNEL_GROUPS
-    # kernel family -> (counter group, divisions per counted unit); the two
-    # instantiations of the singleton round kernel are one family
+    # kernel family -> (counter group, divisions per counted unit)
     fam = {}
     for k, (kms, kc) in kern.items():
-        f = "k_sng_round" if k.startswith("k_sng_round") else k
+        f = k.split("<")[0]   # the instantiations of one template are one family
         a_, b_ = fam.get(f, (0.0, 0))
         fam[f] = (a_ + kms, b_ + kc)
     kmap = {"k_bisect": (0, [1, 0, 0, 0]), "k_refine_root": (1, [0, 1, 0, 0]),

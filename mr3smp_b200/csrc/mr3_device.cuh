@@ -133,6 +133,50 @@ static __device__ __noinline__ int dv_bisect_one(int n, const double2 *__restric
   return 0;
 }
 
+// dv_bisect_one by a group of L lanes (L = 4..32; groups independent): the
+// midpoints of the next log2(L) steps form a binary tree that follows from
+// the current interval; lane t of the group counts at node max(t,1) (its
+// interval computed along the node's path with the loop's operations), then
+// the group walks the tree, clamping each count to the walk's (na, nb) and
+// applying the loop's convergence test after each step, as the sequential
+// loop does.  The same sequence of intervals; log2(L) steps per count.
+static __device__ __noinline__ int dv_bisect_tree(int L, int n, const double2 *__restrict__ tp,
+                                           double pivmin, double abstol, double reltol, int itmax,
+                                           int j, double *a_, double *b_, int na, int nb,
+                                           int *iters) {
+  const int lane = threadIdx.x & 31;
+  const int t = lane & (L - 1), g0 = lane - t, depth = 31 - __clz(L);
+  const unsigned gm = ((L == 32) ? 0xffffffffu : ((1u << L) - 1u)) << g0;
+  const int node_t = t == 0 ? 1 : t;
+  double a = *a_, b = *b_;
+  int it = 0, done = itmax < 1, conv = 0;
+  while (!done) {
+    double l = a, r = b;
+    for (int k = 30 - __clz(node_t); k >= 0; k--) {
+      const double m = 0.5 * (l + r);
+      if ((node_t >> k) & 1) l = m; else r = m;
+    }
+    const int raw = dv_count_bisect(n, tp, pivmin, 0.5 * (l + r));
+    int node = 1;
+    for (int d = 0; d < depth; d++) {
+      const int cv = __shfl_sync(gm, raw, g0 + node);
+      if (!done) {
+        const double c = 0.5 * (a + b);
+        const int cnt = d_imin(nb, d_imax(na, cv));
+        if (j <= cnt) { b = c; nb = cnt; node = 2 * node; } else { a = c; na = cnt; node = 2 * node + 1; }
+        it++;
+        const double w = fabs(b - a), tt = fmax(fabs(b), fabs(a));
+        if (w < fmax(fmax(abstol, pivmin), reltol * tt) || na >= nb) { done = 1; conv = 1; }
+        else if (it >= itmax) done = 1;
+      }
+    }
+  }
+  *a_ = a;
+  *b_ = b;
+  *iters = it;
+  return conv;
+}
+
 // dlaneg (SRC/LAPACK/odneg.f:98-163) on packed rows P[(i)*ps]; r is 1-based.
 // U > 1: rows are read in chunks of U with the next chunk's loads issued
 // ahead of the current chunk's arithmetic (see the dlar1v sweeps below),
@@ -343,8 +387,9 @@ static __device__ __noinline__ int dv_dlarrb_one(int n, const double2 *__restric
 }
 
 // dv_dlarrb_one for one interval per group of L lanes (L = 4, 8, 16 or 32,
-// the same for the whole warp; every lane calls it, the lanes of a group
-// with the same arguments, and they get the same results).  The bisection
+// the same for the whole warp; every lane of a group calls it with the same
+// arguments and gets the same results; groups are independent, a group may
+// skip the call).  The bisection
 // midpoints of the next log2(L) steps form a binary tree whose nodes follow
 // from the current interval alone: lane t of the group evaluates the count
 // at node max(t,1) (heap numbering, computed along the node's path with the
@@ -358,11 +403,11 @@ static __device__ __noinline__ int dv_dlarrb_tree(int L, int n, const double2 *_
                                            double lgap_in, double rtol1, double rtol2,
                                            double pivmin, int maxitr, int r, double *w,
                                            double *werr, int *ncount) {
-  const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int t = lane & (L - 1), g0 = lane - t, half = L >> 1;
   const int depth = 31 - __clz(L);
-  const unsigned gbits = (L == 32) ? full : ((1u << L) - 1u);
+  const unsigned gbits = (L == 32) ? 0xffffffffu : ((1u << L) - 1u);
+  const unsigned full = gbits << g0;   // the group's lanes: groups run independently
   const double mnwdth = 2.0 * pivmin;
   double left = *w - *werr, right = *w + *werr;
   double gap = fmin(first ? rgap_own : lgap_in, rgap_own);
@@ -1231,6 +1276,59 @@ static __device__ __noinline__ void dv_r1c_solve(int n, double lambda, const dou
   o->sawnan = slow;
 }
 
+// The factorisation L+ D+ L+^T = L D L^T - sigma I of dlarrf
+// (SRC/LAPACK/odrrf.f:226-252) for one shift: DPLUS into dp[i*os], LPLUS
+// into lp[i*os]; returns max |DPLUS|, sawnan when a pivot was replaced by
+// -pivmin.  The running pivot stays in a register (it is written out, never
+// read back) and the rows are read in chunks of MR3_U issued one chunk
+// ahead of the arithmetic.
+static __device__ __forceinline__ double rrf_sweep(int n, const double2 *__restrict__ P,
+                                                   const double2 *__restrict__ Q, int ps,
+                                                   double sig, double pivmin, double *dp,
+                                                   double *lp, int os, bool *sawnan) {
+  constexpr int U = MR3_U;
+  double s = -sig;
+  double d = P[0].x + s;
+  if (fabs(d) < pivmin) { d = -pivmin; *sawnan = true; }
+  dp[0] = d;
+  double mx = fabs(d);
+  const int last = n - 2;   // rows i = 0..n-2 produce LPLUS(i), DPLUS(i+1)
+  if (last >= 0) {
+    double2 cq[U], nq[U];
+    double cp[U], np_[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int i = d_imin(u, last);
+      cq[u] = Q[(size_t)i * ps];
+      cp[u] = P[(size_t)(i + 1) * ps].x;
+    }
+    for (int i0 = 0; i0 <= last; i0 += U) {
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int i = d_imin(i0 + U + u, last);
+        nq[u] = Q[(size_t)i * ps];
+        np_[u] = P[(size_t)(i + 1) * ps].x;
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int i = i0 + u;
+        if (i <= last) {
+          const double l = cq[u].y / d;
+          lp[(size_t)i * os] = l;
+          s = s * l * cq[u].x - sig;
+          d = cp[u] + s;
+          if (fabs(d) < pivmin) { d = -pivmin; *sawnan = true; }
+          dp[(size_t)(i + 1) * os] = d;
+          mx = fmax(mx, fabs(d));
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) { cq[u] = nq[u]; cp[u] = np_[u]; }
+    }
+  }
+  return mx;
+}
+
 // dlarrf, LAPACK 3.2.2 with NOFAIL (SRC/LAPACK/odrrf.f:140-378), one thread.
 // Parent rows: d = P[i].x, l = Q[i].x, ld = Q[i].y.  w/wgap/werr point at the
 // cluster's first eigenvalue (CLSTRT = 1, CLEND = clend).  dplus, lplus: out;
@@ -1270,35 +1368,11 @@ static __device__ __noinline__ double dv_dlarrf(int n, const double2 *__restrict
     bool sawnan1 = false, sawnan2 = false;
     ldelta = fmin(ldmax, ldelta);
     rdelta = fmin(rdmax, rdelta);
-    double s = -lsigma;
-    dplus(0) = P[0].x + s;
-    if (fabs(dplus(0)) < pivmin) { dplus(0) = -pivmin; sawnan1 = true; }
-    max1 = fabs(dplus(0));
-    for (int i = 0; i < n - 1; i++) {
-      const double2 q = Q[(size_t)i * ps];
-      lplus(i) = q.y / dplus(i);
-      s = s * lplus(i) * q.x - lsigma;
-      double dp = P[(size_t)(i + 1) * ps].x + s;
-      if (fabs(dp) < pivmin) { dp = -pivmin; sawnan1 = true; }
-      dplus(i + 1) = dp;
-      max1 = fmax(max1, fabs(dp));
-    }
+    max1 = rrf_sweep(n, P, Q, ps, lsigma, pivmin, dp_, lp_, os, &sawnan1);
     sawnan1 = sawnan1 || isnan(max1);
     if (forcer || (max1 <= growthbound && !sawnan1)) { sigma = lsigma; shift = 1; break; }
 
-    s = -rsigma;
-    work(0) = P[0].x + s;
-    if (fabs(work(0)) < pivmin) { work(0) = -pivmin; sawnan2 = true; }
-    max2 = fabs(work(0));
-    for (int i = 0; i < n - 1; i++) {
-      const double2 q = Q[(size_t)i * ps];
-      work(n + i) = q.y / work(i);
-      s = s * work(n + i) * q.x - rsigma;
-      double dp = P[(size_t)(i + 1) * ps].x + s;
-      if (fabs(dp) < pivmin) { dp = -pivmin; sawnan2 = true; }
-      work(i + 1) = dp;
-      max2 = fmax(max2, fabs(dp));
-    }
+    max2 = rrf_sweep(n, P, Q, ps, rsigma, pivmin, wk_, wk_ + (size_t)n * os, os, &sawnan2);
     sawnan2 = sawnan2 || isnan(max2);
     if (forcer || (max2 <= growthbound && !sawnan2)) { sigma = rsigma; shift = 2; break; }
 

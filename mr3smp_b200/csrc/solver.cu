@@ -502,12 +502,37 @@ __device__ __forceinline__ unsigned long long bisect_body(int g, const ProbDev *
   return (unsigned long long)it * (unsigned long long)B->nbl;
 }
 
+// TREE = false: a thread per eigenvalue (L = 1).  The two forms are separate
+// instantiations so that the thread form keeps its own register budget.
+template <bool TREE>
 __global__ void __launch_bounds__(128)
-k_bisect(int N, const ProbDev *probs, const BlockDev *blocks, const int *blk_of_row,
+k_bisect(int N, int L, const ProbDev *probs, const BlockDev *blocks, const int *blk_of_row,
          const double2 *TP, double *Wt, double *Et, int *It, Tol tol, unsigned long long *stats) {
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   unsigned long long work = 0;
-  if (g < N) work = bisect_body(g, probs, blocks, blk_of_row, TP, Wt, Et, It, tol);
+  if (!TREE) {
+    if (gt < N) work = bisect_body((int)gt, probs, blocks, blk_of_row, TP, Wt, Et, It, tol);
+  } else if (gt / L < N) {
+    // L lanes per eigenvalue (few eigenvalues: single large problems)
+    const int g = (int)(gt / L);
+    const BlockDev *B = &blocks[blk_of_row[g]];
+    const ProbDev *p = &probs[B->prob];
+    const int k = g - B->ibgn;
+    if (!(p->trivial || p->jobz == MR3_JOB_C || p->status) &&
+        !(B->nbl < 2 || B->mbl <= 0 || B->none || k >= B->nab2 - B->nab1)) {
+      const int j = B->nab1 + 1 + k;
+      double a = B->gl3, b = B->gu3;
+      int itc = 0;
+      dv_bisect_tree(L, B->nbl, TP + B->ibgn, p->pivmin, B->atoli, tol.bsrtol, B->itmax2, j, &a, &b,
+                     B->nab1, B->nab2, &itc);
+      if ((gt % L) == 0) {
+        Wt[g] = 0.5 * (a + b);
+        Et[g] = 0.5 * fabs(a - b);
+        It[g] = j;
+        work = (unsigned long long)itc * (unsigned long long)B->nbl;
+      }
+    }
+  }
   stat_add(stats, KID_BISECT * 4 + 0, work);
 }
 
@@ -772,13 +797,42 @@ __device__ __forceinline__ unsigned long long refine_root_body(int s, const Prob
   return (unsigned long long)nc * (unsigned long long)B->nbl;
 }
 
+template <bool TREE>
 __global__ void __launch_bounds__(128)
-k_refine_root(int N, const ProbDev *probs, const BlockDev *blocks, const int *iblk,
+k_refine_root(int N, int L, const ProbDev *probs, const BlockDev *blocks, const int *iblk,
               const double2 *RP, double *W, double *Werr, const double *Wgap, Tol tol,
               unsigned long long *stats) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   unsigned long long work = 0;
-  if (s < N) work = refine_root_body(s, probs, blocks, iblk, RP, W, Werr, Wgap, tol);
+  if (!TREE) {
+    if (gt < N) work = refine_root_body((int)gt, probs, blocks, iblk, RP, W, Werr, Wgap, tol);
+  } else if (gt / L < N) {
+    // L lanes per eigenvalue (few eigenvalues: single large problems)
+    const int s = (int)(gt / L);
+    const bool ok = iblk[s] >= 0;
+    const BlockDev *B = ok ? &blocks[iblk[s]] : nullptr;
+    const ProbDev *p = ok ? &probs[B->prob] : nullptr;
+    if (ok && !p->status && B->nbl >= 2) {
+      const bool onlyW = (p->jobz == MR3_JOB_N);
+      const int II = s - B->wbgn + 1;
+      const int i = B->ilow + II - 1;
+      double w = W[s] - B->sigma;
+      double werr = Werr[s] + fabs(w) * MR3_EPS;
+      const double rgap = Wgap[s];
+      const double lgap = (II > 1) ? Wgap[s - 1] : rgap;
+      const int maxitr = dv_itmax(B->spdiam + p->pivmin, p->pivmin);
+      const double rtol1 = onlyW ? 4.0 * MR3_EPS : tol.rtol1;
+      const double rtol2 = onlyW ? 4.0 * MR3_EPS : tol.rtol2;
+      int nc = 0;
+      dv_dlarrb_tree(L, B->nbl, RP + B->ibgn, 1, i, II == 1, II > 1, rgap, lgap, rtol1, rtol2,
+                     p->pivmin, maxitr, B->nbl, &w, &werr, &nc);
+      if ((gt % L) == 0) {
+        W[s] = w;
+        Werr[s] = werr;
+        work = (unsigned long long)nc * (unsigned long long)B->nbl;
+      }
+    }
+  }
   stat_add(stats, KID_REFROOT * 4 + 1, work);
 }
 
@@ -1105,15 +1159,20 @@ __device__ __forceinline__ void own_rrr(const ClusterDev &C, const BlockDev &B, 
 // (dlarrb with RQtol, SRC/process_cluster.c:170-195), one thread per end.
 // Both calls see a zero right gap, so their convergence test does not depend
 // on any other gap and the two ends are independent.
+template <bool TREE>
 __global__ void __launch_bounds__(128)
-k_cl_ext(int ncl, const ClusterDev *cl, const ProbDev *probs, const BlockDev *blocks,
+k_cl_ext(int ncl, int L, const ClusterDev *cl, const ProbDev *probs, const BlockDev *blocks,
          const double2 *RP, const double2 *RQ, const double *arena_prev, const double *Wsh,
          const double *Werr, const int *Windex, double *xw, double *xe, Tol tol,
          unsigned long long *stats) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  // L lanes per cluster end (L = 1: a thread; L >= 4: dv_dlarrb_tree, for
+  // launches with few clusters, where the sequential steps are the cost)
+  const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const bool valid = gt / L < 2LL * ncl;
+  const int t = valid ? (int)(gt / L) : 2 * ncl - 1;   // spare lanes mirror the last end
   const int w = t >> 1;
   unsigned long long work = 0;
-  if (w < ncl) {
+  {
     const ClusterDev C = cl[w];
     const BlockDev &B = blocks[C.blk];
     const ProbDev *p = &probs[B.prob];
@@ -1126,11 +1185,19 @@ k_cl_ext(int ncl, const ClusterDev *cl, const ProbDev *probs, const BlockDev *bl
     const int maxitr = dv_itmax(C.bl_spdiam + p->pivmin, p->pivmin);
     double wv = Wsh[sx], ev = Werr[sx];
     int nc = 0;
-    dv_dlarrb_one<MR3_U>(nb, Pp, ps, i, 1, II > 1, 0.0, 0.0, tol.rqtol, tol.rqtol, p->pivmin, maxitr, nb,
-                  &wv, &ev, &nc);
-    xw[t] = wv;
-    xe[t] = ev;
-    work = (unsigned long long)nc * nb;
+    if (!TREE) {
+      if (valid)
+        dv_dlarrb_one<MR3_U>(nb, Pp, ps, i, 1, II > 1, 0.0, 0.0, tol.rqtol, tol.rqtol, p->pivmin,
+                             maxitr, nb, &wv, &ev, &nc);
+    } else {
+      dv_dlarrb_tree(L, nb, Pp, ps, i, 1, II > 1, 0.0, 0.0, tol.rqtol, tol.rqtol, p->pivmin, maxitr,
+                     nb, &wv, &ev, &nc);
+    }
+    if (valid && (gt % L) == 0) {
+      xw[t] = wv;
+      xe[t] = ev;
+      work = (unsigned long long)nc * nb;
+    }
   }
   stat_add(stats, KID_NEWRRR * 4 + 1, work);
 }
@@ -1174,7 +1241,8 @@ k_cl_rrf(int ncl, ClusterDev *cl, const ProbDev *probs, const BlockDev *blocks, 
 // (SRC/process_cluster.c:212-218) and pack the new representations' rows;
 // one CTA per sibling group, rows of the group's members interleaved.
 __global__ void k_cl_pack(int ncl, const ClusterDev *cl, const BlockDev *blocks, double *arena_cur,
-                          double *Wsh, double *Werr, int *cl_of_slot, int *lvl_of_slot, int level) {
+                          double *Wsh, double *Werr, int *cl_of_slot, int *lvl_of_slot, int level,
+                          int *rl, int *rl_n) {
   for (int w = blockIdx.x; w < ncl; w += gridDim.x) {
     const ClusterDev L0 = cl[w];
     if (L0.g != 0) continue;   // the group's first member packs the group
@@ -1195,6 +1263,13 @@ __global__ void k_cl_pack(int ncl, const ClusterDev *cl, const BlockDev *blocks,
         Werr[k] += f;
         cl_of_slot[k] = w + m;
         lvl_of_slot[k] = level;
+        // the level's refinement list (warp-aggregated, neighbours stay together)
+        const unsigned am = __activemask();
+        const int lead = __ffs(am) - 1, lane = threadIdx.x & 31;
+        int o = 0;
+        if (lane == lead) o = atomicAdd(rl_n, __popc(am));
+        o = __shfl_sync(am, o, lead);
+        rl[o + __popc(am & ((1u << lane) - 1u))] = k;
       }
     }
     for (long long idx = threadIdx.x; idx < nG; idx += blockDim.x) {
@@ -1239,16 +1314,61 @@ __device__ __forceinline__ unsigned long long refine_cl_body(
   return (unsigned long long)nc * (unsigned long long)B.nbl;
 }
 
+// Lanes per interval for a launch of `items` independent dlarrb intervals:
+// a thread each when they fill the GPU, else groups of 4..32 lanes running
+// the tree bisection (the same intervals, fewer sequential sweeps).
+__host__ __device__ __forceinline__ int tree_lanes(long long items, long long lanes,
+                                                   int maxL = 32) {
+  if (maxL < 4) return 1;
+  int L = maxL > 32 ? 32 : maxL;
+  while (L > 4 && items * L > lanes) L >>= 1;
+  return items * L > lanes ? 1 : L;
+}
+
+template <bool TREE>
 __global__ void __launch_bounds__(128)
-k_refine_cl(int N, const ClusterDev *cl, const ProbDev *probs, const BlockDev *blocks,
-            const double *arena_cur, double *Wsh, double *Werr, const double *Wgap,
-            const int *Windex, const int *cl_of_slot, const int *lvl_of_slot, int level, Tol tol,
-            unsigned long long *stats) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
+k_refine_cl(const int *rl, const int *rl_n, const ClusterDev *cl, const ProbDev *probs,
+            const BlockDev *blocks, const double *arena_cur, double *Wsh, double *Werr,
+            const double *Wgap, const int *Windex, const int *cl_of_slot, const int *lvl_of_slot,
+            int level, Tol tol, long long lanes, int tree_max, unsigned long long *stats) {
+  const int cnt = *rl_n;
   unsigned long long work = 0;
-  if (s < N)
-    work = refine_cl_body(s, cl, probs, blocks, arena_cur, Wsh, Werr, Wgap, Windex, cl_of_slot,
-                          lvl_of_slot, level, tol);
+  const int L0 = cnt > 0 ? tree_lanes(cnt, lanes, tree_max) : 1;
+  if (cnt > 0 && (L0 > 1) == TREE) {   // the other instantiation has the other form
+    const int L = L0;
+    const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long per = ((long long)gridDim.x * blockDim.x) / L;
+    for (long long b0 = 0; b0 < cnt; b0 += per) {
+      const long long it = b0 + gt / L;
+      const bool valid = it < cnt;
+      const int s = rl[valid ? it : cnt - 1];
+      if (!TREE) {
+        if (valid)
+          work += refine_cl_body(s, cl, probs, blocks, arena_cur, Wsh, Werr, Wgap, Windex,
+                                 cl_of_slot, lvl_of_slot, level, tol);
+        continue;
+      }
+      const ClusterDev C = cl[cl_of_slot[s]];
+      const BlockDev &B = blocks[C.blk];
+      const ProbDev *p = &probs[B.prob];
+      const int pidx = Windex[C.begin], i = Windex[s], II = i - (pidx - 1);
+      const double2 *P, *Q;
+      int ps;
+      own_rrr(C, B, nullptr, nullptr, arena_cur, &P, &Q, &ps);
+      const double rgap = Wgap[s];
+      const double lgap = (II > 1) ? Wgap[s - 1] : rgap;
+      const int maxitr = dv_itmax(C.bl_spdiam + p->pivmin, p->pivmin);
+      double w = Wsh[s], e = Werr[s];
+      int nc = 0;
+      dv_dlarrb_tree(L, B.nbl, P, ps, i, i == pidx, II > 1, rgap, lgap, tol.rtol1, tol.rtol2,
+                     p->pivmin, maxitr, B.nbl, &w, &e, &nc);
+      if (valid && (gt % L) == 0) {
+        Wsh[s] = w;
+        Werr[s] = e;
+        work += (unsigned long long)nc * (unsigned long long)B.nbl;
+      }
+    }
+  }
   stat_add(stats, KID_REFCL * 4 + 1, work);
 }
 
@@ -1924,6 +2044,7 @@ struct mr3_cuda_ctx {
   SngDev *sng = nullptr;
   SngState *sst = nullptr;
   int *act[2] = {nullptr, nullptr}, *bsl = nullptr, *sbcnt = nullptr;
+  int *rl = nullptr, *rl_n = nullptr;       // a level's cluster eigenvalues to refine
   unsigned char *sflag = nullptr;
   LevelCounters *lc = nullptr;
   SngCounters *sc = nullptr;
@@ -2047,6 +2168,7 @@ static int ensure_rows(mr3_cuda_ctx *c, size_t N, size_t P) {
     CK(regrow(&c->act[0], n), "act0");
     CK(regrow(&c->act[1], n), "act1");
     CK(regrow(&c->bsl, n), "bsl");
+    CK(regrow(&c->rl, n), "rl");
     CK(regrow(&c->sflag, n), "sflag");
     CK(regrow(&c->sbcnt, 2 * (n / LIST_T + 1)), "sbcnt");
     c->capN = n;
@@ -2085,6 +2207,7 @@ extern "C" int mr3_cuda_ctx_create(int device, mr3_cuda_ctx **out) {
       cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc((void **)&c->lc, 2 * sizeof(LevelCounters)) != cudaSuccess ||
       cudaMalloc((void **)&c->sc, sizeof(SngCounters)) != cudaSuccess ||
+      cudaMalloc((void **)&c->rl_n, sizeof(int)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_lc, 2 * sizeof(LevelCounters)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_sc, sizeof(SngCounters)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_const, sizeof(double)) != cudaSuccess ||
@@ -2112,7 +2235,7 @@ extern "C" void mr3_cuda_ctx_destroy(mr3_cuda_ctx *c) {
                  c->prob_of_slot, c->cl_of_slot, c->lvl_of_slot, c->unit_list, c->flag, c->tmp2,
                  c->D, c->E, c->E2, c->Wt, c->Et, c->W, c->Werr, c->Wgap, c->Wcopy, c->Wsh,
                  c->Dt, c->Lt, c->Wout, c->gers, c->TP, c->TPc, c->RP, c->RQ, c->rec0, c->rec1,
-                 c->cl[0], c->cl[1], c->sng, c->sst, c->act[0], c->act[1], c->bsl, c->sflag, c->sbcnt, c->lc, c->sc, c->scratch, c->arena[0],
+                 c->cl[0], c->cl[1], c->sng, c->sst, c->act[0], c->act[1], c->bsl, c->sflag, c->sbcnt, c->rl, c->rl_n, c->lc, c->sc, c->scratch, c->arena[0],
                  c->cls_ns, c->cls_soff, c->cls_cbase, c->cls_abase,
                  c->arena[1], (void *)c->Din, (void *)c->Ein, c->Wp, c->Dp, c->Ep};
   for (void *q : dev)
@@ -2309,6 +2432,10 @@ static SortRec *merge_sort(mr3_cuda_ctx *c, cudaStream_t st, int N, int mmax, in
 extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *stream) {
   if (!c) return MR3_EMISC;
   cudaStream_t st = stream ? (cudaStream_t)stream : c->own;
+  // MR3_TREE_LANES caps the lanes per bisection interval (1: a thread each);
+  // tests use it to run both forms on small problems
+  int tree_max = 32;
+  if (const char *ev = getenv("MR3_TREE_LANES")) tree_max = atoi(ev);
   c->launches = 0;
   c->err[0] = 0;
   CK(cudaSetDevice(c->device), "cudaSetDevice");
@@ -2402,15 +2529,29 @@ extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *s
          c->gers, c->TP, c->TPc, tol);
   LAUNCH(k_blocks, L, MR3_THREADS, c->probs, c->blocks, c->D, c->E, c->gers, c->TP, tol);
   unsigned long long *stats = c->prof ? c->stats : nullptr;
-  LAUNCH(k_bisect, gN128, 128, NN, c->probs, c->blocks, c->blk_of_row, c->TP, c->Wt, c->Et, c->It,
-         tol, stats);
+  {
+    const int Lb = tree_lanes(NN, (long long)c->nsm * 2048, tree_max);
+    if (Lb == 1)
+      LAUNCH(k_bisect<false>, gN128, 128, NN, 1, c->probs, c->blocks, c->blk_of_row, c->TP, c->Wt,
+             c->Et, c->It, tol, stats);
+    else
+      LAUNCH(k_bisect<true>, (int)(((long long)NN * Lb + 127) / 128), 128, NN, Lb, c->probs,
+             c->blocks, c->blk_of_row, c->TP, c->Wt, c->Et, c->It, tol, stats);
+  }
   LAUNCH(k_compact, L, MR3_THREADS, c->probs, c->blocks, c->D, c->Wt, c->Et, c->It, c->W, c->Werr,
          c->Windex, c->iblk, c->Wcopy);
   LAUNCH(k_gaps_init, gN, 256, NN, c->probs, c->blocks, c->iblk, c->W, c->Werr, c->Wgap);
   LAUNCH(k_root, L, MR3_THREADS, c->probs, c->blocks, c->D, c->E, c->TP, c->Dt, c->Lt, c->W,
          c->Werr, c->Wgap, c->RP, c->RQ);
-  LAUNCH(k_refine_root, gN128, 128, NN, c->probs, c->blocks, c->iblk, c->RP, c->W, c->Werr,
-         c->Wgap, tol, stats);
+  {
+    const int Lr = tree_lanes(NN, (long long)c->nsm * 2048, tree_max);
+    if (Lr == 1)
+      LAUNCH(k_refine_root<false>, gN128, 128, NN, 1, c->probs, c->blocks, c->iblk, c->RP, c->W,
+             c->Werr, c->Wgap, tol, stats);
+    else
+      LAUNCH(k_refine_root<true>, (int)(((long long)NN * Lr + 127) / 128), 128, NN, Lr, c->probs,
+             c->blocks, c->iblk, c->RP, c->W, c->Werr, c->Wgap, tol, stats);
+  }
   LAUNCH(k_gaps_root, gN, 256, NN, c->probs, c->blocks, c->iblk, c->W, c->Werr, c->Wgap);
   LAUNCH(k_discard, (L + 127) / 128, 128, c->probs, L, c->blocks, c->W, c->Werr, c->Wgap,
          c->Windex, c->iblk, c->Wcopy);
@@ -2447,19 +2588,34 @@ extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *s
     const int DEPTH_CAP = 512;
     ClsScratch xs;
     xs.ns = c->cls_ns; xs.soff = c->cls_soff; xs.cbase = c->cls_cbase; xs.abase = c->cls_abase;
+    const long long lanes = (long long)c->nsm * 2048;   // lanes a launch can keep busy
     for (int level = 0; ncl > 0; level++) {
       if (level >= DEPTH_CAP) { snprintf(c->err, sizeof(c->err), "representation tree too deep"); return MR3_EMISC; }
       const int cur = level & 1, nxt = cur ^ 1;
       const int gW = (ncl * 32 + MR3_THREADS - 1) / MR3_THREADS;
       if (level > 0) {
-        LAUNCH(k_cl_ext, (2 * ncl + 127) / 128, 128, ncl, c->cl[cur], c->probs, c->blocks, c->RP,
-               c->RQ, c->arena[nxt], c->Wsh, c->Werr, c->Windex, c->Wt, c->Et, tol, stats);
+        const int Lx = tree_lanes(2LL * ncl, lanes, tree_max);
+        if (Lx == 1)
+          LAUNCH(k_cl_ext<false>, (int)((2LL * ncl + 127) / 128), 128, ncl, 1, c->cl[cur], c->probs,
+                 c->blocks, c->RP, c->RQ, c->arena[nxt], c->Wsh, c->Werr, c->Windex, c->Wt, c->Et,
+                 tol, stats);
+        else
+          LAUNCH(k_cl_ext<true>, (int)((2LL * ncl * Lx + 127) / 128), 128, ncl, Lx, c->cl[cur],
+                 c->probs, c->blocks, c->RP, c->RQ, c->arena[nxt], c->Wsh, c->Werr, c->Windex, c->Wt,
+                 c->Et, tol, stats);
         LAUNCH(k_cl_rrf, (ncl + 127) / 128, 128, ncl, c->cl[cur], c->probs, c->blocks, c->RP, c->RQ,
                c->arena[nxt], c->arena[cur], c->Wt, c->Et, c->Wsh, c->Werr, c->Wgap, stats);
+        CK(cudaMemsetAsync(c->rl_n, 0, sizeof(int), st), "rl_n");
         LAUNCH(k_cl_pack, std::min(ncl, 65535 * 16), 256, ncl, c->cl[cur], c->blocks, c->arena[cur],
-               c->Wsh, c->Werr, c->cl_of_slot, c->lvl_of_slot, level);
-        LAUNCH(k_refine_cl, gN128, 128, NN, c->cl[cur], c->probs, c->blocks, c->arena[cur], c->Wsh,
-               c->Werr, c->Wgap, c->Windex, c->cl_of_slot, c->lvl_of_slot, level, tol, stats);
+               c->Wsh, c->Werr, c->cl_of_slot, c->lvl_of_slot, level, c->rl, c->rl_n);
+        // both forms are launched; the one that does not match the list's
+        // length returns at once (the length is known on the device only)
+        LAUNCH(k_refine_cl<false>, gN128, 128, c->rl, c->rl_n, c->cl[cur], c->probs, c->blocks,
+               c->arena[cur], c->Wsh, c->Werr, c->Wgap, c->Windex, c->cl_of_slot, c->lvl_of_slot,
+               level, tol, lanes, tree_max, stats);
+        LAUNCH(k_refine_cl<true>, (int)(lanes / 128), 128, c->rl, c->rl_n, c->cl[cur], c->probs,
+               c->blocks, c->arena[cur], c->Wsh, c->Werr, c->Wgap, c->Windex, c->cl_of_slot,
+               c->lvl_of_slot, level, tol, lanes, tree_max, stats);
         LAUNCH(k_gaps_cl, gN, 256, NN, c->cl[cur], c->Wsh, c->Werr, c->Wgap, c->W, c->cl_of_slot,
                c->lvl_of_slot, level);
       }

@@ -14,8 +14,18 @@ pytestmark = pytest.mark.gpu
 CASES, GOLD = load_golden()
 
 
+@pytest.fixture(params=["tree", "thread"])
+def bisection_form(request, monkeypatch):
+    """Small problems take the lane-group (tree) form of the bisection
+    kernels; MR3_TREE_LANES=1 forces the thread-per-interval form that large
+    batches take, so both forms are checked against the oracle."""
+    if request.param == "thread":
+        monkeypatch.setenv("MR3_TREE_LANES", "1")
+    return request.param
+
+
 @pytest.mark.parametrize("case", small_zoo(), ids=lambda c: c[0])
-def test_gpu_equals_oracle_small(case):
+def test_gpu_equals_oracle_small(case, bisection_form):
     name, D, E, jz, rg, kw = case
     g = M.mrrr(jz, rg, D, E, **kw)
     o = oracle.mrrr(jz, rg, D, E, **kw)
@@ -24,7 +34,7 @@ def test_gpu_equals_oracle_small(case):
 
 
 @pytest.mark.parametrize("case", medium_zoo(), ids=lambda c: c[0])
-def test_gpu_equals_oracle_medium(case):
+def test_gpu_equals_oracle_medium(case, bisection_form):
     name, D, E, jz, rg, kw = case
     g = M.mrrr(jz, rg, D, E, **kw)
     o = oracle.mrrr(jz, rg, D, E, **kw)

@@ -63,6 +63,16 @@ void mr3_cuda_ctx_destroy(mr3_cuda_ctx *ctx);
  * returns after the results (m, info, ...) have been copied to probs. */
 int  mr3_cuda_solve(mr3_cuda_ctx *ctx, int nprob, mr3_cuda_prob *probs, void *stream);
 
+/* mr3_cuda_solve with a report of finished eigenvectors: done(user, list,
+ * count) is called on the calling thread, during the solve, with the
+ * indices (into probs) of problems whose Z columns are all written in device
+ * memory, so that their copies can start while the rest is solved.  A
+ * problem is reported again if its columns were reordered afterwards (the
+ * rare order fix-up of sort_eigenpairs); the last report holds. */
+typedef void (*mr3_cuda_done_fn)(void *user, const int *probs, int count);
+int  mr3_cuda_solve_cb(mr3_cuda_ctx *ctx, int nprob, mr3_cuda_prob *probs, void *stream,
+                       mr3_cuda_done_fn done, void *user);
+
 /* Grow-only device buffer `slot` (0..MR3_CUDA_WS_SLOTS-1) of this context,
  * at least `bytes` long and 256-byte aligned; NULL on allocation failure.
  * Its contents do not survive a call that grows it. */

@@ -1031,24 +1031,32 @@ static __device__ __noinline__ double dv_r1c_progr(bool active, int n, double la
   const int topw = __reduce_max_sync(0xffffffffu, work ? top : 0);
   const int r1w = __reduce_min_sync(0xffffffffu, work ? r1 : 0x7fffffff);
   if (topw >= 1) {
-    for (int jb = (topw - 1) / CK_K; jb >= (r1w - 1) / CK_K; jb--) {
+    const int jtop = (topw - 1) / CK_K, jbot = (r1w - 1) / CK_K;
+    // a block's rows (P; Q for the search's stationary recompute) are
+    // loaded one block ahead of its arithmetic
+    double2 cp[CK_K], cq[CK_K], np_[CK_K], nq[CK_K];
+    auto load = [&](int jb, double2 *bp, double2 *bq) {
+      const int base = jb * CK_K + 1;
+      const int hi = d_imin(base + CK_K - 1, top), lo = d_imax(base, r1);
+      if (work && lo <= hi) {
+#pragma unroll
+        for (int u = 0; u < CK_K; u++) {
+          const int i = d_imax(d_imin(base + u, hi), lo);
+          bp[u] = P[(size_t)(i - 1) * ps];
+          if (search) bq[u] = Q[(size_t)(i - 1) * ps];
+        }
+      }
+    };
+    load(jtop, cp, cq);
+    for (int jb = jtop; jb >= jbot; jb--) {
+      if (jb - 1 >= jbot) load(jb - 1, np_, nq);
       const int base = jb * CK_K + 1;
       const int hi = d_imin(base + CK_K - 1, top), lo = d_imax(base, r1);
       const bool bw = work && lo <= hi;
-      // this block's rows, loaded before any arithmetic
-      double2 pp[CK_K];
-#pragma unroll
-      for (int u = 0; u < CK_K; u++) {
-        if (bw) pp[u] = P[(size_t)(d_imax(d_imin(base + u, hi), lo) - 1) * ps];
-      }
-      if (bw && base - 1 >= r1)
-        for (int i = d_imax(base - CK_K, r1); i <= base - 1; i++) {
-          pf_l1(&P[(size_t)(i - 1) * ps]);
-          pf_l1(&Q[(size_t)(i - 1) * ps]);
-        }
       double sia[CK_K];
       if (bw && search) {
-        // SI of rows base-1 .. base+CK_K-2 (those of twist candidates only)
+        // SI of rows base-1 .. base+CK_K-2 (those of twist candidates only);
+        // in search mode r1 = 1, so the block's rows were loaded unclamped
         sia[0] = ckI[(size_t)jb * 32];
         double s = ckS[(size_t)jb * 32];
         const int rmax = d_imin(hi - 1, r2 - 1);
@@ -1056,13 +1064,11 @@ static __device__ __noinline__ double dv_r1c_progr(bool active, int n, double la
         for (int u = 1; u < CK_K; u++) {
           const int i = base + u - 1;
           if (i <= rmax) {
-            const double2 a = pp[u - 1];
-            const double2 q = Q[(size_t)(i - 1) * ps];
-            double dplus = a.x + s;
+            double dplus = cp[u - 1].x + s;
             if (slowA && fabs(dplus) < pivmin) dplus = -pivmin;
-            const double lp = q.y / dplus;
-            double si = s * lp * q.x;
-            if (slowA && lp == 0.0) si = a.y;
+            const double lp = cq[u - 1].y / dplus;
+            double si = s * lp * cq[u - 1].x;
+            if (slowA && lp == 0.0) si = cp[u - 1].y;
             s = si - lambda;
             sia[u] = si;
           }
@@ -1073,12 +1079,12 @@ static __device__ __noinline__ double dv_r1c_progr(bool active, int n, double la
       for (int u = CK_K - 1; u >= 0; u--) {
         const int i = base + u;
         if (bw && i >= lo && i <= hi) {
-          double dminus = pp[u].y + p;
+          double dminus = cp[u].y + p;
           if (SLOW && fabs(dminus) < pivmin) dminus = -pivmin;
-          const double tmp = pp[u].x / dminus;
+          const double tmp = cp[u].x / dminus;
           neg2 += (dminus < 0.0);
           double pn = p * tmp - lambda;
-          if (SLOW && tmp == 0.0) pn = pp[u].x - lambda;
+          if (SLOW && tmp == 0.0) pn = cp[u].x - lambda;
           p = pn;
           if (i > r1 && i <= r2) {        // candidate r = i: S(i-1) + P(i-1)
             const double sprev = sia[u];
@@ -1088,6 +1094,8 @@ static __device__ __noinline__ double dv_r1c_progr(bool active, int n, double la
           }
         }
       }
+#pragma unroll
+      for (int u = 0; u < CK_K; u++) { cp[u] = np_[u]; cq[u] = nq[u]; }
     }
   }
   *neg2o = neg2;

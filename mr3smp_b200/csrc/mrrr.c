@@ -107,6 +107,42 @@ static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 /* One batched solve of host problems on a given context (the body of
  * mr3_batched, also used by the serving workers, which own their contexts). */
+/* Z of one problem to the caller's array, on the copy stream. */
+static int copy_z(mr3_cuda_ctx *ctx, const mr3_host_prob *h, const mr3_cuda_prob *q, int m)
+{
+  if (h->ldz == q->ldz)
+    return mr3_cuda_copy_on(ctx, MR3_STREAM_COPY, h->Z, q->Z,
+                            (size_t)h->ldz * (size_t)m * sizeof(double), 1);
+  return mr3_cuda_copy2d_on(ctx, MR3_STREAM_COPY, h->Z, (size_t)h->ldz * sizeof(double), q->Z,
+                            (size_t)q->ldz * sizeof(double), (size_t)h->n * sizeof(double),
+                            (size_t)m, 1);
+}
+
+/* Eigenvector copies started while the solve goes on: the solver reports
+ * problems whose Z columns are complete (mr3_cuda_solve_cb). */
+typedef struct {
+  mr3_cuda_ctx *ctx;
+  mr3_host_prob *hp;
+  mr3_cuda_prob *dp;
+  char *copied;
+  int rc;
+} early_copy;
+
+static void on_done(void *user, const int *probs, int count)
+{
+  early_copy *e = (early_copy *)user;
+  int t;
+  for (t = 0; t < count; t++) {
+    const int i = probs[t];
+    const mr3_host_prob *h = &e->hp[i];
+    const mr3_cuda_prob *q = &e->dp[i];
+    /* range V: the column count is known only at the end */
+    if (q->jobz != MR3_JOB_V || q->range == MR3_RANGE_V) continue;
+    if (copy_z(e->ctx, h, q, ncols_of(h, q->jobz, q->range)) != MR3_OK) e->rc = MR3_EMISC;
+    e->copied[i] = 1;
+  }
+}
+
 __attribute__((visibility("hidden"))) int mr3__batched_on(mr3_cuda_ctx *ctx, int nprob, mr3_host_prob *hp)
 {
   int i, c, rc = MR3_OK, worst = 0, nchunk = 1;
@@ -114,13 +150,16 @@ __attribute__((visibility("hidden"))) int mr3__batched_on(mr3_cuda_ctx *ctx, int
   mr3_cuda_prob *dp;
   size_t nrow = 0, nzs = 0, ztot = 0, zmax = 0, small, pipe_min, pipe_chunk;
   size_t *zb, *orow, *ozs;
+  char *copied;
+  early_copy ec;
   char *base, *stage;
   double *dD, *dE, *dW, *dZb[2] = {NULL, NULL};
   int *dZs;
   if (nprob <= 0) return 0;
   dp = (mr3_cuda_prob *)calloc((size_t)nprob, sizeof(mr3_cuda_prob));
   zb = (size_t *)calloc(3 * (size_t)nprob, sizeof(size_t));
-  if (!dp || !zb) { free(dp); free(zb); return MR3_EMISC; }
+  copied = (char *)calloc((size_t)nprob, 1);
+  if (!dp || !zb || !copied) { free(dp); free(zb); free(copied); return MR3_EMISC; }
   orow = zb + nprob;
   ozs = orow + nprob;
   for (i = 0; i < nprob; i++) {
@@ -167,7 +206,7 @@ __attribute__((visibility("hidden"))) int mr3__batched_on(mr3_cuda_ctx *ctx, int
     for (i = cbeg[c]; i < cbeg[c + 1]; i++) z += zb[i];
     if (z > zmax) zmax = z;
   }
-  if (!ctx) { free(dp); free(zb); return MR3_EMISC; }
+  if (!ctx) { free(dp); free(zb); free(copied); return MR3_EMISC; }
   /* device layout of the small arrays, mirrored by the staging buffer:
    * D | E | W (nrow doubles each) | Zsupp (nzs ints) */
   small = 3 * nrow * sizeof(double) + nzs * sizeof(int);
@@ -210,26 +249,23 @@ __attribute__((visibility("hidden"))) int mr3__batched_on(mr3_cuda_ctx *ctx, int
       rc = MR3_EMISC;
       goto done;
     }
-    if (mr3_cuda_solve(ctx, cbeg[c + 1] - cbeg[c], dp + cbeg[c], NULL) != MR3_OK ||
-        mr3_cuda_event(ctx, 2, MR3_STREAM_MAIN, MR3_STREAM_COPY) != MR3_OK) {
+    ec.ctx = ctx;
+    ec.hp = hp + cbeg[c];
+    ec.dp = dp + cbeg[c];
+    ec.copied = copied + cbeg[c];
+    ec.rc = MR3_OK;
+    if (mr3_cuda_solve_cb(ctx, cbeg[c + 1] - cbeg[c], dp + cbeg[c], NULL, on_done, &ec) != MR3_OK ||
+        ec.rc != MR3_OK || mr3_cuda_event(ctx, 2, MR3_STREAM_MAIN, MR3_STREAM_COPY) != MR3_OK) {
       rc = MR3_EMISC;
       goto done;
     }
     for (i = cbeg[c]; i < cbeg[c + 1]; i++) {
       mr3_host_prob *h = &hp[i];
       mr3_cuda_prob *q = &dp[i];
-      if (q->jobz != MR3_JOB_V || q->info != MR3_OK || q->m <= 0) continue;
+      if (q->jobz != MR3_JOB_V || q->info != MR3_OK || q->m <= 0 || copied[i]) continue;
       /* one contiguous copy when the caller's Z has no padding between
        * columns (a pitched copy into pageable memory goes column by column) */
-      if (h->ldz == q->ldz) {
-        if (mr3_cuda_copy_on(ctx, MR3_STREAM_COPY, h->Z, q->Z,
-                             (size_t)h->ldz * (size_t)q->m * sizeof(double), 1) != MR3_OK) {
-          rc = MR3_EMISC;
-          goto done;
-        }
-      } else if (mr3_cuda_copy2d_on(ctx, MR3_STREAM_COPY, h->Z, (size_t)h->ldz * sizeof(double), q->Z,
-                             (size_t)q->ldz * sizeof(double), (size_t)h->n * sizeof(double),
-                             (size_t)q->m, 1) != MR3_OK) {
+      if (copy_z(ctx, h, q, q->m) != MR3_OK) {
         rc = MR3_EMISC;
         goto done;
       }
@@ -268,6 +304,7 @@ done:
   }
   free(dp);
   free(zb);
+  free(copied);
   return worst;
 }
 

@@ -41,6 +41,7 @@ struct ProbDev {
   int *Zsupp;
   // state and outputs
   int status, m, nvals, nsplit, irange, nwl, nwu, il_out, iu_out, tryrac_out, trivial;
+  int zleft;                    // eigenvector columns not yet written
   double scale, pivmin, spdiam, tnorm, gl, gu, wl, wu, wlu, wul, vl_out, vu_out, split;
 };
 
@@ -88,7 +89,13 @@ struct SngCounters {
   int act_n[2], act_next[2];   // round lists: entries, next entry to take
   int bs_n, bs_next, err, nin; // bisection list; err: a list outlived the
                                // rounds; nin: entries of this round's list
+  int done_n, pad2;            // problems whose eigenvectors are all written
 };
+
+// A problem's last eigenvector column is written: list the problem.
+__device__ __forceinline__ void column_done(ProbDev *p, int prob, SngCounters *sc, int *done_list) {
+  if (atomicSub(&p->zleft, 1) == 1) done_list[atomicAdd(&sc->done_n, 1)] = prob;
+}
 
 struct Tol {
   double rtol1, rtol2, bsrtol, rqtol;
@@ -555,7 +562,10 @@ k_compact(ProbDev *probs, BlockDev *blocks, const double *D, double *Wt, double 
     blocks[off + b].wbgn = off + base;
     base += max(blocks[off + b].mbl, 0);
   }
-  if (tid == 0) p->m = total;
+  if (tid == 0) {
+    p->m = total;
+    p->zleft = (p->jobz == MR3_JOB_V) ? total : 0;
+  }
   __syncthreads();
   const int lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
   for (int b = wid; b < ns; b += nw) {
@@ -1534,9 +1544,19 @@ k_classify(int ncl, const ClusterDev *cl, const BlockDev *blocks, const double *
 
 // Per sibling group (led by the member with g == 0): reserve the group's
 // singleton records contiguously, so that consecutive records share a block
-// (and the size of their sweeps).
-__global__ void k_group_tasks(int ncl, const ClusterDev *cl, ClsScratch xs, SngCounters *sc,
-                              LevelCounters *lcn, int cap) {
+// (and the size of their sweeps).  The level's list is ordered by block size,
+// largest first (16 log2 buckets): a round's costliest chunks start first
+// and the small ones fill in behind them.  PASS 0 counts per bucket, PASS 1
+// reserves inside the buckets laid out by k_bucket_scan.
+#define SNG_BUCKETS 16
+__device__ __forceinline__ int size_bucket(int nb) {
+  const int b = 31 - __clz(nb > 0 ? nb : 1);
+  return b < SNG_BUCKETS ? b : SNG_BUCKETS - 1;
+}
+
+template <int PASS>
+__global__ void k_group_tasks(int ncl, const ClusterDev *cl, const BlockDev *blocks, ClsScratch xs,
+                              SngCounters *sc, int *bk, LevelCounters *lcn, int cap) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= ncl) return;
   const ClusterDev C = cl[w];
@@ -1544,10 +1564,26 @@ __global__ void k_group_tasks(int ncl, const ClusterDev *cl, ClsScratch xs, SngC
   int tot = 0;
   for (int m = 0; m < C.G; m++) tot += xs.ns[w + m];
   if (tot == 0) return;
-  const int base = atomicAdd(&sc->n_sng, tot);
+  const int b = size_bucket(blocks[C.blk].nbl);
+  if (PASS == 0) {
+    atomicAdd(&bk[b], tot);
+    atomicAdd(&sc->n_sng, tot);
+    return;
+  }
+  const int base = bk[SNG_BUCKETS + b] + atomicAdd(&bk[2 * SNG_BUCKETS + b], tot);
   if (base + tot > cap) { atomicOr(&lcn->err, 1); return; }
   int o = base;
   for (int m = 0; m < C.G; m++) { xs.soff[w + m] = o; o += xs.ns[w + m]; }
+}
+
+// bk[0..15]: counts per bucket; bk[16..31]: first record of each bucket,
+// largest blocks first; bk[32..47]: fill counters (zeroed with the counts).
+__global__ void k_bucket_scan(int *bk) {
+  int run = 0;
+  for (int b = SNG_BUCKETS - 1; b >= 0; b--) {
+    bk[SNG_BUCKETS + b] = run;
+    run += bk[b];
+  }
 }
 
 // ------------------------------------------------------------------------
@@ -1694,12 +1730,12 @@ __global__ void __launch_bounds__(256) k_list_scatter(int first, const SngCounte
 
 template <bool FIRST>
 __global__ void __launch_bounds__(SNG_WARPS * 32, 2)
-k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, const ProbDev *probs,
+k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
             const BlockDev *blocks, const double2 *RP, const double2 *RQ, const double *arena,
             double *W, double *Wsh, double *Werr, double *Wgap, const int *Windex,
             const int *Zindex, SngState *sst, const int *act0, const int *act1,
             unsigned char *flag, SngCounters *sc, double *scratch, long long nmax,
-            unsigned long long *stats) {
+            int *done_list, unsigned long long *stats) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
@@ -1820,7 +1856,7 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, const ProbDev *prob
     if (!fin) continue;
     const ClusterDev &Cf = cl[sng[idx].cl];
     const BlockDev &B = blocks[Cf.blk];
-    const ProbDev *p = &probs[B.prob];
+    ProbDev *p = &probs[B.prob];
     const int bl0 = B.ibgn - p->off;   // block's first row inside the problem
     int zind = 0;
     if (done) {
@@ -1853,6 +1889,10 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, const ProbDev *prob
       for (int row = b + lane; row < npv; row += 32) Zc[row] = 0.0;
     }
     __syncwarp();
+    if (done) {   // this lane's column is complete (its zero rows included)
+      __threadfence();
+      column_done(p, B.prob, sc, done_list);
+    }
   }
   stat_add(stats, KID_SNG * 4 + 2, w_r1v);
   // diagnostics: warp-level row sweeps and warp chunks
@@ -1918,20 +1958,24 @@ k_sng_bisect(int out, const SngDev *sng, const ClusterDev *cl, const ProbDev *pr
 }
 
 // Unit vectors of 1x1 blocks (SRC/process_singleton.c:125-133).
-__global__ void k_unitvec(const int *list, const SngCounters *sc, const ProbDev *probs,
-                          const BlockDev *blocks, const int *iblk, const int *Zindex) {
+__global__ void k_unitvec(const int *list, SngCounters *sc, ProbDev *probs,
+                          const BlockDev *blocks, const int *iblk, const int *Zindex,
+                          int *done_list) {
   int t = blockIdx.x;
   if (t >= sc->n_unit) return;
   int s = list[t];
   const BlockDev &B = blocks[iblk[s]];
-  const ProbDev *p = &probs[B.prob];
+  ProbDev *p = &probs[B.prob];
   int zind = Zindex[s];
   double *Zc = p->Z + (size_t)zind * (size_t)p->ldz;
   int row0 = B.ibgn - p->off;
   for (int row = threadIdx.x; row < p->n; row += blockDim.x) Zc[row] = (row == row0) ? 1.0 : 0.0;
+  __syncthreads();
   if (threadIdx.x == 0) {
     p->Zsupp[2 * (size_t)zind] = row0 + 1;
     p->Zsupp[2 * (size_t)zind + 1] = row0 + 1;
+    __threadfence();
+    column_done(p, B.prob, sc, done_list);
   }
 }
 
@@ -2045,6 +2089,9 @@ struct mr3_cuda_ctx {
   SngState *sst = nullptr;
   int *act[2] = {nullptr, nullptr}, *bsl = nullptr, *sbcnt = nullptr;
   int *rl = nullptr, *rl_n = nullptr;       // a level's cluster eigenvalues to refine
+  int *sbk = nullptr;                       // singleton size buckets (3 x 16)
+  int *done_list = nullptr;                 // problems whose eigenvectors are complete
+  std::vector<int> h_done;
   unsigned char *sflag = nullptr;
   LevelCounters *lc = nullptr;
   SngCounters *sc = nullptr;
@@ -2177,6 +2224,7 @@ static int ensure_rows(mr3_cuda_ctx *c, size_t N, size_t P) {
     size_t p = std::max(P, c->capP + c->capP / 2);
     CK(regrow(&c->probs, p), "probs");
     CK(regrow(&c->flag, p), "flag");
+    CK(regrow(&c->done_list, p), "done_list");
     CK(regrow(&c->Din, p), "Din");
     CK(regrow(&c->Ein, p), "Ein");
     CK(regrow(&c->Wp, p), "Wp");
@@ -2208,6 +2256,7 @@ extern "C" int mr3_cuda_ctx_create(int device, mr3_cuda_ctx **out) {
       cudaMalloc((void **)&c->lc, 2 * sizeof(LevelCounters)) != cudaSuccess ||
       cudaMalloc((void **)&c->sc, sizeof(SngCounters)) != cudaSuccess ||
       cudaMalloc((void **)&c->rl_n, sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void **)&c->sbk, 3 * SNG_BUCKETS * sizeof(int)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_lc, 2 * sizeof(LevelCounters)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_sc, sizeof(SngCounters)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_const, sizeof(double)) != cudaSuccess ||
@@ -2235,7 +2284,7 @@ extern "C" void mr3_cuda_ctx_destroy(mr3_cuda_ctx *c) {
                  c->prob_of_slot, c->cl_of_slot, c->lvl_of_slot, c->unit_list, c->flag, c->tmp2,
                  c->D, c->E, c->E2, c->Wt, c->Et, c->W, c->Werr, c->Wgap, c->Wcopy, c->Wsh,
                  c->Dt, c->Lt, c->Wout, c->gers, c->TP, c->TPc, c->RP, c->RQ, c->rec0, c->rec1,
-                 c->cl[0], c->cl[1], c->sng, c->sst, c->act[0], c->act[1], c->bsl, c->sflag, c->sbcnt, c->rl, c->rl_n, c->lc, c->sc, c->scratch, c->arena[0],
+                 c->cl[0], c->cl[1], c->sng, c->sst, c->act[0], c->act[1], c->bsl, c->sflag, c->sbcnt, c->rl, c->rl_n, c->sbk, c->done_list, c->lc, c->sc, c->scratch, c->arena[0],
                  c->cls_ns, c->cls_soff, c->cls_cbase, c->cls_abase,
                  c->arena[1], (void *)c->Din, (void *)c->Ein, c->Wp, c->Dp, c->Ep};
   for (void *q : dev)
@@ -2430,6 +2479,11 @@ static SortRec *merge_sort(mr3_cuda_ctx *c, cudaStream_t st, int N, int mmax, in
 }
 
 extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *stream) {
+  return mr3_cuda_solve_cb(c, P, pr, stream, nullptr, nullptr);
+}
+
+extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *stream,
+                                 mr3_cuda_done_fn done_fn, void *user) {
   if (!c) return MR3_EMISC;
   cudaStream_t st = stream ? (cudaStream_t)stream : c->own;
   // MR3_TREE_LANES caps the lanes per bisection interval (1: a thread each);
@@ -2491,6 +2545,21 @@ extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *s
   const int L = nlive;
   int rc = ensure_rows(c, N, (size_t)L);
   if (rc != MR3_OK) return rc;
+  // problems whose eigenvectors are complete, reported to done_fn at the
+  // host's syncs (the kernels that wrote them have finished)
+  int reported = 0;
+  auto report_done = [&]() -> int {
+    if (!done_fn || c->h_sc->done_n <= reported) return MR3_OK;
+    const int cnt = c->h_sc->done_n - reported;
+    c->h_done.resize(cnt);
+    CK(cudaMemcpyAsync(c->h_done.data(), c->done_list + reported, cnt * sizeof(int),
+                       cudaMemcpyDeviceToHost, st), "done d2h");
+    CK(cudaStreamSynchronize(st), "done sync");
+    for (int t = 0; t < cnt; t++) c->h_done[t] = idx[c->h_done[t]];
+    done_fn(user, c->h_done.data(), cnt);
+    reported = c->h_sc->done_n;
+    return MR3_OK;
+  };
   const int NN = (int)N;
   {
     int o = 0;
@@ -2572,7 +2641,7 @@ extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *s
     CK(cudaStreamSynchronize(st), "level0 sync");
     if (c->h_sc->n_unit > 0)
       LAUNCH(k_unitvec, c->h_sc->n_unit, 256, c->unit_list, c->sc, c->probs, c->blocks, c->iblk,
-             c->Zindex);
+             c->Zindex, c->done_list);
     // singleton scratch: the checkpoints of 32 lanes per persistent warp
     const size_t per_warp = 3ull * ((size_t)nmaxV / CK_K + 1) * 32ull;
     const size_t budget = (size_t)8 << 30;   // bytes
@@ -2623,13 +2692,19 @@ extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *s
       CK(cudaMemsetAsync(&c->sc->n_sng, 0, sizeof(int), st), "scn");
       LAUNCH(k_classify<0>, gW, MR3_THREADS, ncl, c->cl[cur], c->blocks, c->Wsh, c->Wgap,
              c->cl[nxt], c->sng, &c->lc[nxt], xs, NN);
-      LAUNCH(k_group_tasks, (ncl + 127) / 128, 128, ncl, c->cl[cur], xs, c->sc, &c->lc[nxt], NN);
+      CK(cudaMemsetAsync(c->sbk, 0, 3 * SNG_BUCKETS * sizeof(int), st), "sbk");
+      LAUNCH(k_group_tasks<0>, (ncl + 127) / 128, 128, ncl, c->cl[cur], c->blocks, xs, c->sc, c->sbk,
+             &c->lc[nxt], NN);
+      LAUNCH(k_bucket_scan, 1, 1, c->sbk);
+      LAUNCH(k_group_tasks<1>, (ncl + 127) / 128, 128, ncl, c->cl[cur], c->blocks, xs, c->sc, c->sbk,
+             &c->lc[nxt], NN);
       LAUNCH(k_classify<1>, gW, MR3_THREADS, ncl, c->cl[cur], c->blocks, c->Wsh, c->Wgap,
              c->cl[nxt], c->sng, &c->lc[nxt], xs, NN);
       CK(cudaMemcpyAsync(c->h_lc, &c->lc[nxt], sizeof(LevelCounters), cudaMemcpyDeviceToHost, st), "lcn d2h");
       CK(cudaMemcpyAsync(c->h_sc, c->sc, sizeof(SngCounters), cudaMemcpyDeviceToHost, st), "sc d2h");
       CK(cudaStreamSynchronize(st), "level sync");
       if (c->h_lc->err) { snprintf(c->err, sizeof(c->err), "queue overflow"); return MR3_EMISC; }
+      if ((rc = report_done()) != MR3_OK) return rc;
       if (c->h_sc->err) { snprintf(c->err, sizeof(c->err), "singleton rounds exhausted"); return MR3_EMISC; }
       if (c->h_sc->n_sng > 0) {
         // the level's singletons in rounds (see k_sng_round)
@@ -2646,12 +2721,12 @@ extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *s
             LAUNCH_SMEM(k_sng_round<true>, ctas_first, SNG_WARPS * 32, smem, in, c->sng,
                         c->cl[cur], c->probs, c->blocks, c->RP, c->RQ, c->arena[cur], c->W, c->Wsh,
                         c->Werr, c->Wgap, c->Windex, c->Zindex, c->sst, c->act[0], c->act[1],
-                        c->sflag, c->sc, c->scratch, (long long)nmaxV, stats);
+                        c->sflag, c->sc, c->scratch, (long long)nmaxV, c->done_list, stats);
           else
             LAUNCH_SMEM(k_sng_round<false>, ctas_all, SNG_WARPS * 32, smem, in, c->sng,
                         c->cl[cur], c->probs, c->blocks, c->RP, c->RQ, c->arena[cur], c->W, c->Wsh,
                         c->Werr, c->Wgap, c->Windex, c->Zindex, c->sst, c->act[0], c->act[1],
-                        c->sflag, c->sc, c->scratch, (long long)nmaxV, stats);
+                        c->sflag, c->sc, c->scratch, (long long)nmaxV, c->done_list, stats);
           LAUNCH(k_list_count, nblk, 256, c->sc, c->sflag, c->sbcnt);
           LAUNCH(k_list_scan, 1, 1024, nblk, c->sc, c->sbcnt, in ^ 1, last);
           LAUNCH(k_list_scatter, nblk, 256, rd == 0, c->sc, c->sflag, c->sbcnt, c->act[0],
@@ -2674,6 +2749,7 @@ extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *s
     CK(cudaMemcpyAsync(c->h_sc, c->sc, sizeof(SngCounters), cudaMemcpyDeviceToHost, st), "sc end");
     CK(cudaStreamSynchronize(st), "rounds sync");
     if (c->h_sc->err) { snprintf(c->err, sizeof(c->err), "singleton rounds exhausted"); return MR3_EMISC; }
+    if ((rc = report_done()) != MR3_OK) return rc;
   }
 
   // ---- post-processing (SRC/mrrr.c:262-285)
@@ -2721,6 +2797,13 @@ extern "C" int mr3_cuda_solve(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void *s
                              colsz * sizeof(double), cudaMemcpyDeviceToDevice, st), "perm scatter");
         CK(cudaStreamSynchronize(st), "perm done");
         cudaFree(tmp);
+      }
+      // columns were reordered: report these problems again
+      if (done_fn) {
+        c->h_done.clear();
+        for (int k = 0; k < L; k++)
+          if (c->h_flag[k]) c->h_done.push_back(idx[k]);
+        if (!c->h_done.empty()) done_fn(user, c->h_done.data(), (int)c->h_done.size());
       }
     }
   }

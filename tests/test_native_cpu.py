@@ -21,6 +21,7 @@ def declared_functions():
             continue
         txt = open(os.path.join(INC, f)).read()
         txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+        txt = re.sub(r"^\s*typedef[^;]*;", "", txt, flags=re.M | re.S)   # function-pointer types
         for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][\w ]*?[\s\*]+(\w+)\s*\(", txt, re.M):
             if m.group(1) not in ("if", "for", "while", "sizeof", "return"):
                 names.add(m.group(1))

@@ -63,13 +63,16 @@ void mr3_cuda_ctx_destroy(mr3_cuda_ctx *ctx);
  * returns after the results (m, info, ...) have been copied to probs. */
 int  mr3_cuda_solve(mr3_cuda_ctx *ctx, int nprob, mr3_cuda_prob *probs, void *stream);
 
-/* mr3_cuda_solve with a report of finished eigenvectors: done(user, list,
- * count) is called on the calling thread, during the solve, with the
- * indices (into probs) of problems whose Z columns are all written in device
- * memory, so that their copies can start while the rest is solved.  A
- * problem is reported again if its columns were reordered afterwards (the
- * rare order fix-up of sort_eigenpairs); the last report holds. */
-typedef void (*mr3_cuda_done_fn)(void *user, const int *probs, int count);
+/* mr3_cuda_solve with a report of finished eigenvectors: done(user, probs,
+ * col0, ncols, count) is called on the calling thread, during the solve,
+ * with `count` column ranges: columns col0[t] .. col0[t]+ncols[t]-1 of
+ * problem probs[t] (an index into probs) are written in device memory, so
+ * that their copies can start while the rest is solved.  Columns come in
+ * tiles of 256, for problems with jobz V and range A or I.  Columns are
+ * reported again if they were reordered afterwards (the rare order fix-up
+ * of sort_eigenpairs); the last report holds. */
+typedef void (*mr3_cuda_done_fn)(void *user, const int *probs, const int *col0, const int *ncols,
+                                 int count);
 int  mr3_cuda_solve_cb(mr3_cuda_ctx *ctx, int nprob, mr3_cuda_prob *probs, void *stream,
                        mr3_cuda_done_fn done, void *user);
 

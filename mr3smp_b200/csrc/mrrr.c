@@ -105,44 +105,46 @@ static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 #define PIPE_CHUNK_BYTES ((size_t)40 << 30)
 #define PIPE_MAX_CHUNKS 16
 
-/* One batched solve of host problems on a given context (the body of
- * mr3_batched, also used by the serving workers, which own their contexts). */
-/* Z of one problem to the caller's array, on the copy stream. */
-static int copy_z(mr3_cuda_ctx *ctx, const mr3_host_prob *h, const mr3_cuda_prob *q, int m)
+/* Columns c0 .. c0+m-1 of one problem's Z to the caller's array, on the
+ * copy stream: one contiguous copy when the caller's Z has no padding
+ * between columns (a pitched copy into pageable memory goes column by
+ * column). */
+static int copy_z(mr3_cuda_ctx *ctx, const mr3_host_prob *h, const mr3_cuda_prob *q, int c0, int m)
 {
+  double *dst = h->Z + (size_t)c0 * (size_t)h->ldz;
+  const double *src = q->Z + (size_t)c0 * (size_t)q->ldz;
   if (h->ldz == q->ldz)
-    return mr3_cuda_copy_on(ctx, MR3_STREAM_COPY, h->Z, q->Z,
+    return mr3_cuda_copy_on(ctx, MR3_STREAM_COPY, dst, src,
                             (size_t)h->ldz * (size_t)m * sizeof(double), 1);
-  return mr3_cuda_copy2d_on(ctx, MR3_STREAM_COPY, h->Z, (size_t)h->ldz * sizeof(double), q->Z,
+  return mr3_cuda_copy2d_on(ctx, MR3_STREAM_COPY, dst, (size_t)h->ldz * sizeof(double), src,
                             (size_t)q->ldz * sizeof(double), (size_t)h->n * sizeof(double),
                             (size_t)m, 1);
 }
 
 /* Eigenvector copies started while the solve goes on: the solver reports
- * problems whose Z columns are complete (mr3_cuda_solve_cb). */
+ * column tiles whose Z columns are complete (mr3_cuda_solve_cb). */
 typedef struct {
   mr3_cuda_ctx *ctx;
   mr3_host_prob *hp;
   mr3_cuda_prob *dp;
-  char *copied;
+  int *copied;   /* columns copied so far, per problem */
   int rc;
 } early_copy;
 
-static void on_done(void *user, const int *probs, int count)
+static void on_done(void *user, const int *probs, const int *col0, const int *ncols, int count)
 {
   early_copy *e = (early_copy *)user;
   int t;
   for (t = 0; t < count; t++) {
     const int i = probs[t];
-    const mr3_host_prob *h = &e->hp[i];
-    const mr3_cuda_prob *q = &e->dp[i];
-    /* range V: the column count is known only at the end */
-    if (q->jobz != MR3_JOB_V || q->range == MR3_RANGE_V) continue;
-    if (copy_z(e->ctx, h, q, ncols_of(h, q->jobz, q->range)) != MR3_OK) e->rc = MR3_EMISC;
-    e->copied[i] = 1;
+    if (e->dp[i].jobz != MR3_JOB_V || ncols[t] <= 0) continue;
+    if (copy_z(e->ctx, &e->hp[i], &e->dp[i], col0[t], ncols[t]) != MR3_OK) e->rc = MR3_EMISC;
+    e->copied[i] += ncols[t];
   }
 }
 
+/* One batched solve of host problems on a given context (the body of
+ * mr3_batched, also used by the serving workers, which own their contexts). */
 __attribute__((visibility("hidden"))) int mr3__batched_on(mr3_cuda_ctx *ctx, int nprob, mr3_host_prob *hp)
 {
   int i, c, rc = MR3_OK, worst = 0, nchunk = 1;
@@ -150,7 +152,7 @@ __attribute__((visibility("hidden"))) int mr3__batched_on(mr3_cuda_ctx *ctx, int
   mr3_cuda_prob *dp;
   size_t nrow = 0, nzs = 0, ztot = 0, zmax = 0, small, pipe_min, pipe_chunk;
   size_t *zb, *orow, *ozs;
-  char *copied;
+  int *copied;
   early_copy ec;
   char *base, *stage;
   double *dD, *dE, *dW, *dZb[2] = {NULL, NULL};
@@ -158,7 +160,7 @@ __attribute__((visibility("hidden"))) int mr3__batched_on(mr3_cuda_ctx *ctx, int
   if (nprob <= 0) return 0;
   dp = (mr3_cuda_prob *)calloc((size_t)nprob, sizeof(mr3_cuda_prob));
   zb = (size_t *)calloc(3 * (size_t)nprob, sizeof(size_t));
-  copied = (char *)calloc((size_t)nprob, 1);
+  copied = (int *)calloc((size_t)nprob, sizeof(int));
   if (!dp || !zb || !copied) { free(dp); free(zb); free(copied); return MR3_EMISC; }
   orow = zb + nprob;
   ozs = orow + nprob;
@@ -262,10 +264,9 @@ __attribute__((visibility("hidden"))) int mr3__batched_on(mr3_cuda_ctx *ctx, int
     for (i = cbeg[c]; i < cbeg[c + 1]; i++) {
       mr3_host_prob *h = &hp[i];
       mr3_cuda_prob *q = &dp[i];
-      if (q->jobz != MR3_JOB_V || q->info != MR3_OK || q->m <= 0 || copied[i]) continue;
-      /* one contiguous copy when the caller's Z has no padding between
-       * columns (a pitched copy into pageable memory goes column by column) */
-      if (copy_z(ctx, h, q, q->m) != MR3_OK) {
+      /* the columns that were not all copied during the solve */
+      if (q->jobz != MR3_JOB_V || q->info != MR3_OK || q->m <= 0 || copied[i] >= q->m) continue;
+      if (copy_z(ctx, h, q, 0, q->m) != MR3_OK) {
         rc = MR3_EMISC;
         goto done;
       }

@@ -42,6 +42,7 @@ struct ProbDev {
   // state and outputs
   int status, m, nvals, nsplit, irange, nwl, nwu, il_out, iu_out, tryrac_out, trivial;
   int zleft;                    // eigenvector columns not yet written
+  int tbase;                    // first column tile in the tile counters (-1: none)
   double scale, pivmin, spdiam, tnorm, gl, gu, wl, wu, wlu, wul, vl_out, vu_out, split;
 };
 
@@ -89,12 +90,39 @@ struct SngCounters {
   int act_n[2], act_next[2];   // round lists: entries, next entry to take
   int bs_n, bs_next, err, nin; // bisection list; err: a list outlived the
                                // rounds; nin: entries of this round's list
-  int done_n, pad2;            // problems whose eigenvectors are all written
+  int done_n, done_exp;        // finished column tiles: listed, exported to the host
 };
 
-// A problem's last eigenvector column is written: list the problem.
-__device__ __forceinline__ void column_done(ProbDev *p, int prob, SngCounters *sc, int *done_list) {
-  if (atomicSub(&p->zleft, 1) == 1) done_list[atomicAdd(&sc->done_n, 1)] = prob;
+// Output column zind of a problem is written.  Columns are counted in tiles
+// of ZT_COLS; a tile whose last column is written is listed as
+// (problem, tile), so that its copy can start while the solve goes on.
+#define ZT_COLS 256
+__device__ __forceinline__ void column_done(ProbDev *p, int prob, int zind, SngCounters *sc,
+                                            int2 *done_list, int *tile_left) {
+  atomicSub(&p->zleft, 1);
+  if (p->tbase < 0) return;
+  const int t = zind / ZT_COLS;
+  if (atomicSub(&tile_left[p->tbase + t], 1) == 1)
+    done_list[atomicAdd(&sc->done_n, 1)] = make_int2(prob, t);
+}
+
+// The level and singleton counters (hlc, hsc), and the column tiles listed
+// since the last export (hdone, with their count so far in *hsnap), written
+// by the SMs straight into pinned host memory; null targets are skipped.
+// A copy-engine transfer would queue behind the eigenvector copies of
+// finished tiles that the caller may have started meanwhile.
+__global__ void k_export(const LevelCounters *lc, LevelCounters *hlc, SngCounters *sc,
+                         SngCounters *hsc, const int2 *done_list, int2 *hdone, int *hsnap) {
+  const int t = threadIdx.x, from = sc->done_exp, to = sc->done_n;
+  if (t == 0) {
+    if (hlc) *hlc = *lc;
+    if (hsc) *hsc = *sc;
+    if (hsnap) *hsnap = to;
+  }
+  if (hdone)
+    for (int i = from + t; i < to; i += blockDim.x) hdone[i] = done_list[i];
+  __syncthreads();
+  if (t == 0 && hdone) sc->done_exp = to;
 }
 
 struct Tol {
@@ -549,7 +577,7 @@ k_bisect(int N, int L, const ProbDev *probs, const BlockDev *blocks, const int *
 // ------------------------------------------------------------------------
 __global__ void __launch_bounds__(MR3_THREADS)
 k_compact(ProbDev *probs, BlockDev *blocks, const double *D, double *Wt, double *Et, int *It,
-          double *W, double *Werr, int *Windex, int *iblk, double *Wcopy) {
+          double *W, double *Werr, int *Windex, int *iblk, double *Wcopy, int *tile_left) {
   __shared__ int sint[64];
   ProbDev *p = &probs[blockIdx.x];
   if (p->trivial || p->jobz == MR3_JOB_C) return;
@@ -565,7 +593,14 @@ k_compact(ProbDev *probs, BlockDev *blocks, const double *D, double *Wt, double 
   if (tid == 0) {
     p->m = total;
     p->zleft = (p->jobz == MR3_JOB_V) ? total : 0;
+    // the host sized the tiles for iu-il+1 (range I) or n (range A) columns
+    if (total != (p->range == MR3_RANGE_I ? p->iu - p->il + 1 : p->n)) p->tbase = -1;
   }
+  __syncthreads();
+  // column tiles of ZT_COLS output columns, each counting its unwritten columns
+  if (p->tbase >= 0 && p->jobz == MR3_JOB_V)
+    for (int t = tid; t * ZT_COLS < total; t += nt)
+      tile_left[p->tbase + t] = min(ZT_COLS, total - t * ZT_COLS);
   __syncthreads();
   const int lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
   for (int b = wid; b < ns; b += nw) {
@@ -1735,7 +1770,7 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
             double *W, double *Wsh, double *Werr, double *Wgap, const int *Windex,
             const int *Zindex, SngState *sst, const int *act0, const int *act1,
             unsigned char *flag, SngCounters *sc, double *scratch, long long nmax,
-            int *done_list, unsigned long long *stats) {
+            int2 *done_list, int *tile_left, unsigned long long *stats) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
@@ -1891,7 +1926,7 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
     __syncwarp();
     if (done) {   // this lane's column is complete (its zero rows included)
       __threadfence();
-      column_done(p, B.prob, sc, done_list);
+      column_done(p, B.prob, zind, sc, done_list, tile_left);
     }
   }
   stat_add(stats, KID_SNG * 4 + 2, w_r1v);
@@ -1960,7 +1995,7 @@ k_sng_bisect(int out, const SngDev *sng, const ClusterDev *cl, const ProbDev *pr
 // Unit vectors of 1x1 blocks (SRC/process_singleton.c:125-133).
 __global__ void k_unitvec(const int *list, SngCounters *sc, ProbDev *probs,
                           const BlockDev *blocks, const int *iblk, const int *Zindex,
-                          int *done_list) {
+                          int2 *done_list, int *tile_left) {
   int t = blockIdx.x;
   if (t >= sc->n_unit) return;
   int s = list[t];
@@ -1975,7 +2010,7 @@ __global__ void k_unitvec(const int *list, SngCounters *sc, ProbDev *probs,
     p->Zsupp[2 * (size_t)zind] = row0 + 1;
     p->Zsupp[2 * (size_t)zind + 1] = row0 + 1;
     __threadfence();
-    column_done(p, B.prob, sc, done_list);
+    column_done(p, B.prob, zind, sc, done_list, tile_left);
   }
 }
 
@@ -2090,8 +2125,14 @@ struct mr3_cuda_ctx {
   int *act[2] = {nullptr, nullptr}, *bsl = nullptr, *sbcnt = nullptr;
   int *rl = nullptr, *rl_n = nullptr;       // a level's cluster eigenvalues to refine
   int *sbk = nullptr;                       // singleton size buckets (3 x 16)
-  int *done_list = nullptr;                 // problems whose eigenvectors are complete
-  std::vector<int> h_done;
+  int2 *done_list = nullptr;                // finished column tiles (problem, tile)
+  int *tile_left = nullptr;                 // unwritten columns of each tile
+  size_t capTiles = 0;
+  int2 *h_done = nullptr, *d_hdone = nullptr;   // pinned copy of done_list (host, device view)
+  int *h_snap = nullptr, *d_hsnap = nullptr;    // done_n after each singleton round
+  cudaEvent_t rev[SNG_ROUNDS] = {};             // and the rounds' completion
+  std::vector<int2> h_runs;
+  std::vector<int> h_dprob, h_dcol, h_dcnt;
   unsigned char *sflag = nullptr;
   LevelCounters *lc = nullptr;
   SngCounters *sc = nullptr;
@@ -2101,8 +2142,8 @@ struct mr3_cuda_ctx {
   // pinned host mirrors
   ProbDev *h_probs = nullptr;
   void **h_ptrs = nullptr;
-  LevelCounters *h_lc = nullptr;
-  SngCounters *h_sc = nullptr;
+  LevelCounters *h_lc = nullptr, *d_hlc = nullptr;   // host pointer, device view
+  SngCounters *h_sc = nullptr, *d_hsc = nullptr;
   int *h_flag = nullptr;
   double *h_const = nullptr;   // {1.0}
   int *h_iconst = nullptr;     // {1, 1}
@@ -2224,7 +2265,7 @@ static int ensure_rows(mr3_cuda_ctx *c, size_t N, size_t P) {
     size_t p = std::max(P, c->capP + c->capP / 2);
     CK(regrow(&c->probs, p), "probs");
     CK(regrow(&c->flag, p), "flag");
-    CK(regrow(&c->done_list, p), "done_list");
+
     CK(regrow(&c->Din, p), "Din");
     CK(regrow(&c->Ein, p), "Ein");
     CK(regrow(&c->Wp, p), "Wp");
@@ -2251,6 +2292,8 @@ extern "C" int mr3_cuda_ctx_create(int device, mr3_cuda_ctx **out) {
   bool evok = true;
   for (int i = 0; i < MR3_CUDA_EVENTS; i++)
     evok = evok && cudaEventCreateWithFlags(&c->xev[i], cudaEventDisableTiming) == cudaSuccess;
+  for (int i = 0; i < SNG_ROUNDS; i++)
+    evok = evok && cudaEventCreateWithFlags(&c->rev[i], cudaEventDisableTiming) == cudaSuccess;
   if (!evok || cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc((void **)&c->lc, 2 * sizeof(LevelCounters)) != cudaSuccess ||
@@ -2259,9 +2302,13 @@ extern "C" int mr3_cuda_ctx_create(int device, mr3_cuda_ctx **out) {
       cudaMalloc((void **)&c->sbk, 3 * SNG_BUCKETS * sizeof(int)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_lc, 2 * sizeof(LevelCounters)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_sc, sizeof(SngCounters)) != cudaSuccess ||
+      cudaMallocHost((void **)&c->h_snap, SNG_ROUNDS * sizeof(int)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_const, sizeof(double)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_iconst, 2 * sizeof(int)) != cudaSuccess ||
-      cudaMalloc((void **)&c->stats, KID_COUNT * 4 * sizeof(unsigned long long)) != cudaSuccess) {
+      cudaMalloc((void **)&c->stats, KID_COUNT * 4 * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaHostGetDevicePointer((void **)&c->d_hlc, c->h_lc, 0) != cudaSuccess ||
+      cudaHostGetDevicePointer((void **)&c->d_hsc, c->h_sc, 0) != cudaSuccess ||
+      cudaHostGetDevicePointer((void **)&c->d_hsnap, c->h_snap, 0) != cudaSuccess) {
     mr3_cuda_ctx_destroy(c);
     return MR3_EMISC;
   }
@@ -2284,20 +2331,23 @@ extern "C" void mr3_cuda_ctx_destroy(mr3_cuda_ctx *c) {
                  c->prob_of_slot, c->cl_of_slot, c->lvl_of_slot, c->unit_list, c->flag, c->tmp2,
                  c->D, c->E, c->E2, c->Wt, c->Et, c->W, c->Werr, c->Wgap, c->Wcopy, c->Wsh,
                  c->Dt, c->Lt, c->Wout, c->gers, c->TP, c->TPc, c->RP, c->RQ, c->rec0, c->rec1,
-                 c->cl[0], c->cl[1], c->sng, c->sst, c->act[0], c->act[1], c->bsl, c->sflag, c->sbcnt, c->rl, c->rl_n, c->sbk, c->done_list, c->lc, c->sc, c->scratch, c->arena[0],
+                 c->cl[0], c->cl[1], c->sng, c->sst, c->act[0], c->act[1], c->bsl, c->sflag, c->sbcnt, c->rl, c->rl_n, c->sbk, c->done_list, c->tile_left, c->lc, c->sc, c->scratch, c->arena[0],
                  c->cls_ns, c->cls_soff, c->cls_cbase, c->cls_abase,
                  c->arena[1], (void *)c->Din, (void *)c->Ein, c->Wp, c->Dp, c->Ep};
   for (void *q : dev)
     if (q) cudaFree(q);
   for (int i = 0; i < MR3_CUDA_WS_SLOTS; i++)
     if (c->ws[i]) cudaFree(c->ws[i]);
-  void *host[] = {c->h_probs, c->h_ptrs, c->h_lc, c->h_sc, c->h_flag, c->h_const, c->h_iconst};
+  void *host[] = {c->h_probs, c->h_ptrs, c->h_lc, c->h_sc, c->h_flag, c->h_const, c->h_iconst,
+                  c->h_done, c->h_snap};
   for (void *q : host)
     if (q) cudaFreeHost(q);
   if (c->stats) cudaFree(c->stats);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
   for (int i = 0; i < MR3_CUDA_EVENTS; i++)
     if (c->xev[i]) cudaEventDestroy(c->xev[i]);
+  for (int i = 0; i < SNG_ROUNDS; i++)
+    if (c->rev[i]) cudaEventDestroy(c->rev[i]);
   if (c->hws) cudaFreeHost(c->hws);
   if (c->aux) cudaStreamDestroy(c->aux);
   if (c->own) cudaStreamDestroy(c->own);
@@ -2545,28 +2595,82 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
   const int L = nlive;
   int rc = ensure_rows(c, N, (size_t)L);
   if (rc != MR3_OK) return rc;
-  // problems whose eigenvectors are complete, reported to done_fn at the
+  // column tiles of the problems whose column count is known up front
+  // (jobz V, range A or I); finished tiles are reported to done_fn at the
   // host's syncs (the kernels that wrote them have finished)
+  std::vector<int> mest(L, 0);
+  size_t ntiles = 0;
+  for (int k = 0; k < L; k++) {
+    const mr3_cuda_prob &q = pr[idx[k]];
+    if (q.jobz == MR3_JOB_V && q.range != MR3_RANGE_V)
+      mest[k] = q.range == MR3_RANGE_I ? q.iu - q.il + 1 : q.n;
+    ntiles += (mest[k] + ZT_COLS - 1) / ZT_COLS;
+  }
+  if (done_fn && ntiles > c->capTiles) {
+    CK(cudaStreamSynchronize(st), "tiles sync");
+    CK(regrow(&c->tile_left, ntiles), "tile_left");
+    CK(regrow(&c->done_list, ntiles), "done_list");
+    if (c->h_done) cudaFreeHost(c->h_done);
+    c->h_done = nullptr;
+    CK(cudaMallocHost((void **)&c->h_done, ntiles * sizeof(int2)), "h_done");
+    CK(cudaHostGetDevicePointer((void **)&c->d_hdone, c->h_done, 0), "h_done view");
+    c->capTiles = ntiles;
+  }
+  const bool tiles = done_fn && ntiles > 0;
   int reported = 0;
-  auto report_done = [&]() -> int {
-    if (!done_fn || c->h_sc->done_n <= reported) return MR3_OK;
-    const int cnt = c->h_sc->done_n - reported;
-    c->h_done.resize(cnt);
-    CK(cudaMemcpyAsync(c->h_done.data(), c->done_list + reported, cnt * sizeof(int),
-                       cudaMemcpyDeviceToHost, st), "done d2h");
-    CK(cudaStreamSynchronize(st), "done sync");
-    for (int t = 0; t < cnt; t++) c->h_done[t] = idx[c->h_done[t]];
-    done_fn(user, c->h_done.data(), cnt);
-    reported = c->h_sc->done_n;
+  auto report_upto = [&](int upto) -> int {
+    if (!tiles || upto <= reported) return MR3_OK;
+    // the new tiles in (problem, tile) order, adjacent tiles of a problem
+    // merged into one range
+    c->h_runs.assign(c->h_done + reported, c->h_done + upto);
+    std::sort(c->h_runs.begin(), c->h_runs.end(), [](int2 a, int2 b) {
+      return a.x != b.x ? a.x < b.x : a.y < b.y;
+    });
+    c->h_dprob.clear();
+    c->h_dcol.clear();
+    c->h_dcnt.clear();
+    for (size_t t = 0; t < c->h_runs.size();) {
+      size_t u = t + 1;
+      while (u < c->h_runs.size() && c->h_runs[u].x == c->h_runs[t].x &&
+             c->h_runs[u].y == c->h_runs[u - 1].y + 1)
+        u++;
+      const int k = c->h_runs[t].x, c0 = c->h_runs[t].y * ZT_COLS;
+      c->h_dprob.push_back(idx[k]);
+      c->h_dcol.push_back(c0);
+      c->h_dcnt.push_back(std::min((c->h_runs[u - 1].y + 1) * ZT_COLS, mest[k]) - c0);
+      t = u;
+    }
+    done_fn(user, c->h_dprob.data(), c->h_dcol.data(), c->h_dcnt.data(), (int)c->h_dprob.size());
+    reported = upto;
+    return MR3_OK;
+  };
+  auto report_done = [&]() -> int { return report_upto(c->h_sc->done_n); };
+  // singleton rounds whose finished tiles are exported but not yet reported
+  int npend = 0;
+  // the counters (and the tiles finished since the last export) go to the
+  // host through k_export; the host waits for it, reporting the tiles of
+  // the rounds before it as they complete
+  auto sync_counters = [&](LevelCounters *lc, const char *what) -> int {
+    LAUNCH(k_export, 1, 256, lc, lc ? c->d_hlc : nullptr, c->sc, c->d_hsc, c->done_list,
+           tiles ? c->d_hdone : nullptr, nullptr);
+    for (int i = 0; i < npend; i++) {
+      CK(cudaEventSynchronize(c->rev[i]), "round event");
+      int rc2 = report_upto(c->h_snap[i]);
+      if (rc2 != MR3_OK) return rc2;
+    }
+    npend = 0;
+    CK(cudaStreamSynchronize(st), what);
     return MR3_OK;
   };
   const int NN = (int)N;
   {
-    int o = 0;
+    int o = 0, tb = 0;
     for (int k = 0; k < L; k++) {
       const mr3_cuda_prob &q = pr[idx[k]];
       ProbDev &h = c->h_probs[k];
       memset(&h, 0, sizeof(ProbDev));
+      h.tbase = (done_fn && mest[k] > 0) ? tb : -1;
+      if (h.tbase >= 0) tb += (mest[k] + ZT_COLS - 1) / ZT_COLS;
       h.n = q.n; h.off = o; h.jobz = q.jobz; h.range = q.range; h.il = q.il; h.iu = q.iu;
       h.tryrac = q.tryrac; h.ldz = q.ldz; h.vl = q.vl; h.vu = q.vu; h.Z = q.Z; h.Zsupp = q.Zsupp;
       h.scale = 1.0;
@@ -2608,7 +2712,7 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
              c->blocks, c->blk_of_row, c->TP, c->Wt, c->Et, c->It, tol, stats);
   }
   LAUNCH(k_compact, L, MR3_THREADS, c->probs, c->blocks, c->D, c->Wt, c->Et, c->It, c->W, c->Werr,
-         c->Windex, c->iblk, c->Wcopy);
+         c->Windex, c->iblk, c->Wcopy, c->tile_left);
   LAUNCH(k_gaps_init, gN, 256, NN, c->probs, c->blocks, c->iblk, c->W, c->Werr, c->Wgap);
   LAUNCH(k_root, L, MR3_THREADS, c->probs, c->blocks, c->D, c->E, c->TP, c->Dt, c->Lt, c->W,
          c->Werr, c->Wgap, c->RP, c->RQ);
@@ -2636,12 +2740,10 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
     CK(cudaMemsetAsync(c->lvl_of_slot, 0xff, N * sizeof(int), st), "lvl");
     LAUNCH(k_level0, L, MR3_THREADS, c->probs, c->blocks, c->E, c->gers, c->W, c->Werr, c->Wsh,
            c->cl[0], &c->lc[0], c->sc, c->unit_list);
-    CK(cudaMemcpyAsync(c->h_lc, c->lc, sizeof(LevelCounters), cudaMemcpyDeviceToHost, st), "lc0");
-    CK(cudaMemcpyAsync(c->h_sc, c->sc, sizeof(SngCounters), cudaMemcpyDeviceToHost, st), "sc0");
-    CK(cudaStreamSynchronize(st), "level0 sync");
+    if ((rc = sync_counters(c->lc, "level0 sync")) != MR3_OK) return rc;
     if (c->h_sc->n_unit > 0)
       LAUNCH(k_unitvec, c->h_sc->n_unit, 256, c->unit_list, c->sc, c->probs, c->blocks, c->iblk,
-             c->Zindex, c->done_list);
+             c->Zindex, c->done_list, c->tile_left);
     // singleton scratch: the checkpoints of 32 lanes per persistent warp
     const size_t per_warp = 3ull * ((size_t)nmaxV / CK_K + 1) * 32ull;
     const size_t budget = (size_t)8 << 30;   // bytes
@@ -2700,9 +2802,7 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
              &c->lc[nxt], NN);
       LAUNCH(k_classify<1>, gW, MR3_THREADS, ncl, c->cl[cur], c->blocks, c->Wsh, c->Wgap,
              c->cl[nxt], c->sng, &c->lc[nxt], xs, NN);
-      CK(cudaMemcpyAsync(c->h_lc, &c->lc[nxt], sizeof(LevelCounters), cudaMemcpyDeviceToHost, st), "lcn d2h");
-      CK(cudaMemcpyAsync(c->h_sc, c->sc, sizeof(SngCounters), cudaMemcpyDeviceToHost, st), "sc d2h");
-      CK(cudaStreamSynchronize(st), "level sync");
+      if ((rc = sync_counters(&c->lc[nxt], "level sync")) != MR3_OK) return rc;
       if (c->h_lc->err) { snprintf(c->err, sizeof(c->err), "queue overflow"); return MR3_EMISC; }
       if ((rc = report_done()) != MR3_OK) return rc;
       if (c->h_sc->err) { snprintf(c->err, sizeof(c->err), "singleton rounds exhausted"); return MR3_EMISC; }
@@ -2721,12 +2821,20 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
             LAUNCH_SMEM(k_sng_round<true>, ctas_first, SNG_WARPS * 32, smem, in, c->sng,
                         c->cl[cur], c->probs, c->blocks, c->RP, c->RQ, c->arena[cur], c->W, c->Wsh,
                         c->Werr, c->Wgap, c->Windex, c->Zindex, c->sst, c->act[0], c->act[1],
-                        c->sflag, c->sc, c->scratch, (long long)nmaxV, c->done_list, stats);
+                        c->sflag, c->sc, c->scratch, (long long)nmaxV, c->done_list, c->tile_left,
+                        stats);
           else
             LAUNCH_SMEM(k_sng_round<false>, ctas_all, SNG_WARPS * 32, smem, in, c->sng,
                         c->cl[cur], c->probs, c->blocks, c->RP, c->RQ, c->arena[cur], c->W, c->Wsh,
                         c->Werr, c->Wgap, c->Windex, c->Zindex, c->sst, c->act[0], c->act[1],
-                        c->sflag, c->sc, c->scratch, (long long)nmaxV, c->done_list, stats);
+                        c->sflag, c->sc, c->scratch, (long long)nmaxV, c->done_list, c->tile_left,
+                        stats);
+          if (tiles) {
+            LAUNCH(k_export, 1, 256, nullptr, nullptr, c->sc, nullptr, c->done_list, c->d_hdone,
+                   c->d_hsnap + npend);
+            CK(cudaEventRecord(c->rev[npend], st), "round record");
+            npend++;
+          }
           LAUNCH(k_list_count, nblk, 256, c->sc, c->sflag, c->sbcnt);
           LAUNCH(k_list_scan, 1, 1024, nblk, c->sc, c->sbcnt, in ^ 1, last);
           LAUNCH(k_list_scatter, nblk, 256, rd == 0, c->sc, c->sflag, c->sbcnt, c->act[0],
@@ -2746,8 +2854,7 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
         c->capArena[nxt] = nsz;
       }
     }
-    CK(cudaMemcpyAsync(c->h_sc, c->sc, sizeof(SngCounters), cudaMemcpyDeviceToHost, st), "sc end");
-    CK(cudaStreamSynchronize(st), "rounds sync");
+    if ((rc = sync_counters(nullptr, "rounds sync")) != MR3_OK) return rc;
     if (c->h_sc->err) { snprintf(c->err, sizeof(c->err), "singleton rounds exhausted"); return MR3_EMISC; }
     if ((rc = report_done()) != MR3_OK) return rc;
   }
@@ -2798,12 +2905,20 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
         CK(cudaStreamSynchronize(st), "perm done");
         cudaFree(tmp);
       }
-      // columns were reordered: report these problems again
+      // columns were reordered: report these problems' columns again
       if (done_fn) {
-        c->h_done.clear();
+        c->h_dprob.clear();
+        c->h_dcol.clear();
+        c->h_dcnt.clear();
         for (int k = 0; k < L; k++)
-          if (c->h_flag[k]) c->h_done.push_back(idx[k]);
-        if (!c->h_done.empty()) done_fn(user, c->h_done.data(), (int)c->h_done.size());
+          if (c->h_flag[k] && c->h_probs[k].m > 0) {
+            c->h_dprob.push_back(idx[k]);
+            c->h_dcol.push_back(0);
+            c->h_dcnt.push_back(c->h_probs[k].m);
+          }
+        if (!c->h_dprob.empty())
+          done_fn(user, c->h_dprob.data(), c->h_dcol.data(), c->h_dcnt.data(),
+                  (int)c->h_dprob.size());
       }
     }
   }

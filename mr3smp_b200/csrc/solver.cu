@@ -1798,6 +1798,7 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
     int nb;
     double pivmin, lam_call, gaptol;
     const double2 *P, *Q;
+    double *zcol;   // the eigenvector's column of Z at the block's first row
     int ps, r_in;
     bool usedBS;
     {
@@ -1807,7 +1808,9 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
       const ClusterDev C = cl[S.cl];
       const BlockDev &B = blocks[C.blk];
       nb = B.nbl;
-      pivmin = probs[B.prob].pivmin;
+      const ProbDev *pd = &probs[B.prob];
+      pivmin = pd->pivmin;
+      zcol = pd->Z + (size_t)Zindex[s] * pd->ldz + (B.ibgn - pd->off);
       own_rrr(C, B, RP, RQ, arena, &P, &Q, &ps);
       SngState st;
       if (FIRST) {
@@ -1837,9 +1840,11 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
     dv_r1c_factor(active, nb, lam_call, P, Q, ps, pivmin, !usedBS, r_in, ck, &negc, &rs);
     dlar1v_out o;
     o.isupp1 = 1; o.isupp2 = nb; o.nrminv = 0.0; o.r = 0; o.resid = 0.0; o.rqcorr = 0.0;
+    // z of the support goes to the column unscaled; an accepted vector is
+    // scaled below (z * nrminv, the reference's dscal after dlar1v)
     if (active)
       dv_r1c_solve(nb, lam_call, P, Q, ps, pivmin, gaptol, rs.r, rs.sawnan, rs.slowA, rs.slowB,
-                   ck.S, ck.P, rs.mingma, nullptr, 0.0, &o);
+                   ck.S, ck.P, rs.mingma, zcol, 1.0, &o);
     SngState st = sm_st[threadIdx.x];
     const bool step2 = (st.flags & SF_STEP2) != 0;
     const int nb_sweep = __reduce_max_sync(full, active ? nb : 0);
@@ -1903,24 +1908,21 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
       p->Zsupp[2 * (size_t)zind] = o.isupp1 + bl0;
       p->Zsupp[2 * (size_t)zind + 1] = o.isupp2 + bl0;
     }
-    // the accepted vector: z of the support again, normalised, straight to
-    // the lane's column of Z (the same operations as the solve above)
-    double *const Zp = p->Z;
+    // the accepted vectors, one column at a time by the whole warp: the
+    // support scaled by nrminv, the rows outside the support (and outside
+    // the block) zero
     const int ldz = p->ldz, np = p->n;
-    if (done) {
-      dlar1v_out o2;
-      dv_r1c_solve(nb, lam_call, P, Q, ps, pivmin, st.gaptol, rs.r, rs.sawnan, rs.slowA, rs.slowB,
-                   ck.S, ck.P, rs.mingma, Zp + (size_t)zind * ldz + bl0, o.nrminv, &o2);
-    }
-    // rows of the column outside the support (and outside the block) are zero
     const int z1 = bl0 + o.isupp1 - 1, z2 = bl0 + o.isupp2;   // support rows [z1, z2)
+    __syncwarp();
     for (unsigned m = fin; m; m &= m - 1) {
       const int v = __ffs(m) - 1;
       const int npv = __shfl_sync(full, np, v), zc = __shfl_sync(full, zind, v);
       const int a = __shfl_sync(full, z1, v), b = __shfl_sync(full, z2, v);
       const int ldv = __shfl_sync(full, ldz, v);
-      double *Zc = (double *)__shfl_sync(full, (unsigned long long)Zp, v) + (size_t)zc * ldv;
+      const double nv = __shfl_sync(full, o.nrminv, v);
+      double *Zc = (double *)__shfl_sync(full, (unsigned long long)p->Z, v) + (size_t)zc * ldv;
       for (int row = lane; row < a; row += 32) Zc[row] = 0.0;
+      for (int row = a + lane; row < b; row += 32) Zc[row] = Zc[row] * nv;
       for (int row = b + lane; row < npv; row += 32) Zc[row] = 0.0;
     }
     __syncwarp();

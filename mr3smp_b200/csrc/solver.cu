@@ -2103,6 +2103,8 @@ struct mr3_cuda_ctx {
   int sng_ctas_per_sm = 2;                  // resident k_sng_round CTAs per SM
   cudaStream_t own = nullptr;
   cudaStream_t aux = nullptr;               // copies that overlap the solves
+  cudaStream_t rnd = nullptr;               // a level's singleton rounds
+  cudaEvent_t rnd_done = nullptr;           // and their end
   cudaEvent_t xev[MR3_CUDA_EVENTS] = {nullptr};
   void *hws = nullptr;                      // page-locked staging buffer
   size_t hws_cap = 0;
@@ -2298,6 +2300,8 @@ extern "C" int mr3_cuda_ctx_create(int device, mr3_cuda_ctx **out) {
     evok = evok && cudaEventCreateWithFlags(&c->rev[i], cudaEventDisableTiming) == cudaSuccess;
   if (!evok || cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->rnd, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->rnd_done, cudaEventDisableTiming) != cudaSuccess ||
       cudaMalloc((void **)&c->lc, 2 * sizeof(LevelCounters)) != cudaSuccess ||
       cudaMalloc((void **)&c->sc, sizeof(SngCounters)) != cudaSuccess ||
       cudaMalloc((void **)&c->rl_n, sizeof(int)) != cudaSuccess ||
@@ -2352,6 +2356,8 @@ extern "C" void mr3_cuda_ctx_destroy(mr3_cuda_ctx *c) {
     if (c->rev[i]) cudaEventDestroy(c->rev[i]);
   if (c->hws) cudaFreeHost(c->hws);
   if (c->aux) cudaStreamDestroy(c->aux);
+  if (c->rnd) cudaStreamDestroy(c->rnd);
+  if (c->rnd_done) cudaEventDestroy(c->rnd_done);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
 }
@@ -2546,6 +2552,8 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
   c->err[0] = 0;
   CK(cudaSetDevice(c->device), "cudaSetDevice");
   if (P <= 0) return MR3_OK;
+  // rounds of an earlier solve that ended early (an error) finish first
+  CK(cudaStreamWaitEvent(st, c->rnd_done, 0), "rounds wait");
 
   // ---- host-side triage: invalid and trivial problems
   size_t N = 0;
@@ -2762,6 +2770,7 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
     ClsScratch xs;
     xs.ns = c->cls_ns; xs.soff = c->cls_soff; xs.cbase = c->cls_cbase; xs.abase = c->cls_abase;
     const long long lanes = (long long)c->nsm * 2048;   // lanes a launch can keep busy
+    bool rounds_pending = false;
     for (int level = 0; ncl > 0; level++) {
       if (level >= DEPTH_CAP) { snprintf(c->err, sizeof(c->err), "representation tree too deep"); return MR3_EMISC; }
       const int cur = level & 1, nxt = cur ^ 1;
@@ -2792,6 +2801,12 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
         LAUNCH(k_gaps_cl, gN, 256, NN, c->cl[cur], c->Wsh, c->Werr, c->Wgap, c->W, c->cl_of_slot,
                c->lvl_of_slot, level);
       }
+      // the classification below rewrites the singleton records and the
+      // cluster records that the previous level's rounds read
+      if (rounds_pending) {
+        CK(cudaStreamWaitEvent(st, c->rnd_done, 0), "rounds wait");
+        rounds_pending = false;
+      }
       CK(cudaMemsetAsync(&c->lc[nxt], 0, sizeof(LevelCounters), st), "lcn");
       CK(cudaMemsetAsync(&c->sc->n_sng, 0, sizeof(int), st), "scn");
       LAUNCH(k_classify<0>, gW, MR3_THREADS, ncl, c->cl[cur], c->blocks, c->Wsh, c->Wgap,
@@ -2809,7 +2824,12 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
       if ((rc = report_done()) != MR3_OK) return rc;
       if (c->h_sc->err) { snprintf(c->err, sizeof(c->err), "singleton rounds exhausted"); return MR3_EMISC; }
       if (c->h_sc->n_sng > 0) {
-        // the level's singletons in rounds (see k_sng_round)
+        // the level's singletons in rounds (see k_sng_round), on their own
+        // stream: the next level's cluster kernels (which read and write
+        // neither their records nor their eigenvalue slots) run beside the
+        // rounds' short tail
+        cudaStream_t st = c->rnd;
+        rounds_pending = true;
         const int nsng = c->h_sc->n_sng;
         const int ctas_all = (int)(nwarps / SNG_WARPS);
         const int ctas_first = std::min(ctas_all, (nsng + 32 * SNG_WARPS - 1) / (32 * SNG_WARPS));
@@ -2846,6 +2866,7 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
                    c->RP, c->RQ, c->arena[cur], c->Windex, c->sst, c->bsl, c->act[0], c->act[1],
                    c->sc, stats);
         }
+        CK(cudaEventRecord(c->rnd_done, st), "rounds record");
       }
       ncl = c->h_lc->n_cl;
       const size_t need = (size_t)c->h_lc->arena_need;
@@ -2856,6 +2877,7 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
         c->capArena[nxt] = nsz;
       }
     }
+    if (rounds_pending) CK(cudaStreamWaitEvent(st, c->rnd_done, 0), "rounds wait");
     if ((rc = sync_counters(nullptr, "rounds sync")) != MR3_OK) return rc;
     if (c->h_sc->err) { snprintf(c->err, sizeof(c->err), "singleton rounds exhausted"); return MR3_EMISC; }
     if ((rc = report_done()) != MR3_OK) return rc;

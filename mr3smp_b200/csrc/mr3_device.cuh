@@ -1035,6 +1035,9 @@ static __device__ __noinline__ double dv_r1c_progr(bool active, int n, double la
     // a block's rows (P; Q for the search's stationary recompute) are
     // loaded one block ahead of its arithmetic
     double2 cp[CK_K], cq[CK_K], np_[CK_K], nq[CK_K];
+    // the search's stationary checkpoints, also one block ahead
+    double ckSv = 0.0, ckIv = 0.0, nckS = 0.0, nckI = 0.0;
+    if (work && search) { ckSv = ckS[(size_t)jtop * 32]; ckIv = ckI[(size_t)jtop * 32]; }
     auto load = [&](int jb, double2 *bp, double2 *bq) {
       const int base = jb * CK_K + 1;
       const int hi = d_imin(base + CK_K - 1, top), lo = d_imax(base, r1);
@@ -1049,7 +1052,10 @@ static __device__ __noinline__ double dv_r1c_progr(bool active, int n, double la
     };
     load(jtop, cp, cq);
     for (int jb = jtop; jb >= jbot; jb--) {
-      if (jb - 1 >= jbot) load(jb - 1, np_, nq);
+      if (jb - 1 >= jbot) {
+        load(jb - 1, np_, nq);
+        if (work && search) { nckS = ckS[(size_t)(jb - 1) * 32]; nckI = ckI[(size_t)(jb - 1) * 32]; }
+      }
       const int base = jb * CK_K + 1;
       const int hi = d_imin(base + CK_K - 1, top), lo = d_imax(base, r1);
       const bool bw = work && lo <= hi;
@@ -1057,8 +1063,8 @@ static __device__ __noinline__ double dv_r1c_progr(bool active, int n, double la
       if (bw && search) {
         // SI of rows base-1 .. base+CK_K-2 (those of twist candidates only);
         // in search mode r1 = 1, so the block's rows were loaded unclamped
-        sia[0] = ckI[(size_t)jb * 32];
-        double s = ckS[(size_t)jb * 32];
+        sia[0] = ckIv;
+        double s = ckSv;
         const int rmax = d_imin(hi - 1, r2 - 1);
 #pragma unroll
         for (int u = 1; u < CK_K; u++) {
@@ -1096,6 +1102,8 @@ static __device__ __noinline__ double dv_r1c_progr(bool active, int n, double la
       }
 #pragma unroll
       for (int u = 0; u < CK_K; u++) { cp[u] = np_[u]; cq[u] = nq[u]; }
+      ckSv = nckS;
+      ckIv = nckI;
     }
   }
   *neg2o = neg2;
@@ -1172,11 +1180,14 @@ static __device__ __noinline__ void dv_r1c_solve(int n, double lambda, const dou
   {
     double zp = 1.0, zpp = 0.0;   // z(i+1), z(i+2)
     bool go = r - 1 >= 1;
+    // each block's checkpoint is loaded one block ahead
+    double s_next = go ? ckS[(size_t)((r - 2) / CK_K) * 32] : 0.0;
     for (int jb = (r - 2) / CK_K; go && jb >= 0; jb--) {
       const int base = jb * CK_K + 1;
       const int hi = d_imin(base + CK_K - 1, r - 1);
       double lpa[CK_K], lda[CK_K];
-      double s = ckS[(size_t)jb * 32];
+      double s = s_next;
+      if (jb > 0) s_next = ckS[(size_t)(jb - 1) * 32];
 #pragma unroll
       for (int u = 0; u < CK_K; u++) {
         const int i = base + u;
@@ -1224,11 +1235,14 @@ static __device__ __noinline__ void dv_r1c_solve(int n, double lambda, const dou
   {
     double zc = 1.0, zcp = 0.0;   // z(i), z(i-1)
     bool go = r <= n - 1;
-    for (int jb = (r - 1) / CK_K; go && jb <= (n - 2) / CK_K; jb++) {
+    const int jlast = (n - 2) / CK_K;
+    double p_next = go ? ckP[(size_t)((r - 1) / CK_K) * 32] : 0.0;
+    for (int jb = (r - 1) / CK_K; go && jb <= jlast; jb++) {
       const int base = jb * CK_K + 1;
       const int lo = d_imax(base, r), hi = d_imin(base + CK_K - 1, n - 1);
       double uma[CK_K], lda[CK_K];
-      double p = ckP[(size_t)jb * 32];
+      double p = p_next;
+      if (jb < jlast) p_next = ckP[(size_t)(jb + 1) * 32];
 #pragma unroll
       for (int u = CK_K - 1; u >= 0; u--) {
         const int i = base + u;

@@ -1663,6 +1663,47 @@ __global__ void k_round_reset(SngCounters *sc, int in, int first) {
 // with flag[j] = 0 (finished), 1 (next round) or 2 (bisection first).  The
 // survivors keep their order, so the warps of the next round again take
 // neighbouring singletons (mostly of one block and one representation).
+// The next round's list ordered within windows of LSORT_W entries by
+// (cluster, twist index), so that the 32 lanes of a warp take neighbouring
+// twist indices of one representation: the lock-step sweeps of a warp span
+// its lanes' twist indices (stationary rows up to the largest, progressive
+// rows down to the smallest), and neighbouring twists keep that span short.
+// Each singleton's result does not depend on the order.  Bitonic sort of
+// (cluster, twist, position) keys in shared memory, one window per block.
+#define LSORT_W 4096
+__global__ void __launch_bounds__(1024) k_list_sort(const SngCounters *sc, int out, int *act0,
+                                                    int *act1, const SngDev *sng,
+                                                    const SngState *sst) {
+  __shared__ unsigned long long key[LSORT_W];
+  __shared__ int val[LSORT_W];
+  const int cnt = sc->act_n[out], start = blockIdx.x * LSORT_W;
+  if (start >= cnt) return;
+  int *A = out ? act1 : act0;
+  const int m = min(LSORT_W, cnt - start);
+  const unsigned cap = (1u << 22) - 1;
+  for (int j = threadIdx.x; j < LSORT_W; j += blockDim.x) {
+    unsigned long long k = ~0ull;
+    if (j < m) {
+      const int idx = A[start + j];
+      val[j] = idx;
+      const unsigned c = min((unsigned)sng[idx].cl, cap), r = min((unsigned)sst[idx].r, cap);
+      k = ((unsigned long long)c << 34) | ((unsigned long long)r << 12) | (unsigned)j;
+    }
+    key[j] = k;
+  }
+  __syncthreads();
+  for (int size = 2; size <= LSORT_W; size <<= 1)
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int t = threadIdx.x; t < LSORT_W / 2; t += blockDim.x) {
+        const int lo = 2 * t - (t & (stride - 1)), hi = lo + stride;
+        const unsigned long long a = key[lo], b = key[hi];
+        if ((a > b) == ((lo & size) == 0)) { key[lo] = b; key[hi] = a; }
+      }
+      __syncthreads();
+    }
+  for (int j = threadIdx.x; j < m; j += blockDim.x) A[start + j] = val[key[j] & (LSORT_W - 1)];
+}
+
 #define LIST_T 1024   // entries per block: 256 threads x 4
 __global__ void __launch_bounds__(256) k_list_count(const SngCounters *sc,
                                                     const unsigned char *flag, int *bcnt) {
@@ -2861,10 +2902,13 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
           LAUNCH(k_list_scan, 1, 1024, nblk, c->sc, c->sbcnt, in ^ 1, last);
           LAUNCH(k_list_scatter, nblk, 256, rd == 0, c->sc, c->sflag, c->sbcnt, c->act[0],
                  c->act[1], in, c->bsl);
-          if (!last)
+          if (!last) {
             LAUNCH(k_sng_bisect, bis_ctas, 256, in ^ 1, c->sng, c->cl[cur], c->probs, c->blocks,
                    c->RP, c->RQ, c->arena[cur], c->Windex, c->sst, c->bsl, c->act[0], c->act[1],
                    c->sc, stats);
+            LAUNCH(k_list_sort, (nsng + LSORT_W - 1) / LSORT_W, 1024, c->sc, in ^ 1, c->act[0],
+                   c->act[1], c->sng, c->sst);
+          }
         }
         CK(cudaEventRecord(c->rnd_done, st), "rounds record");
       }

@@ -116,11 +116,13 @@ static __device__ __noinline__ void dv_ijob3(int n, const double2 *__restrict__ 
 
 // The interval of eigenvalue j under dlaebz IJOB=2 started from [a,b] with
 // counts (na,nb): midpoint bisection of that one interval (odebz.f 90-120).
+// it0 > 0 continues a bisection whose first it0 steps ended in [a,b].
 static __device__ __noinline__ int dv_bisect_one(int n, const double2 *__restrict__ tp, double pivmin,
                                           double abstol, double reltol, int itmax, int j,
-                                          double *a, double *b, int na, int nb, int *iters) {
+                                          double *a, double *b, int na, int nb, int *iters,
+                                          int it0 = 0) {
   double c = 0.5 * (*a + *b);
-  for (int it = 1; it <= itmax; it++) {
+  for (int it = it0 + 1; it <= itmax; it++) {
     int cnt = dv_count_bisect(n, tp, pivmin, c);
     cnt = d_imin(nb, d_imax(na, cnt));
     if (j <= cnt) { *b = c; nb = cnt; } else { *a = c; na = cnt; }

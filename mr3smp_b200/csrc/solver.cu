@@ -572,6 +572,204 @@ k_bisect(int N, int L, const ProbDev *probs, const BlockDev *blocks, const int *
 }
 
 // ------------------------------------------------------------------------
+// Stage A2 with shared intervals (the thread form's replacement for many
+// eigenvalues).  The bisection of eigenvalue j (dv_bisect_one from
+// [gl3, gu3]) visits the same intervals as every other eigenvalue of its
+// block until a Sturm count separates them: its state (a, b, na, nb) after
+// k steps is a node of a binary tree rooted at the block's start interval.
+// The tree's levels run breadth-first with one Sturm count per node, and a
+// node's eigenvalues continue in its children.  A child holding one
+// eigenvalue leaves the tree with its state (k_bisect_cont continues it, a
+// thread per eigenvalue); a converged child, or one at the iteration
+// limit, writes its eigenvalues' results.  Every eigenvalue sees the
+// operations of dv_bisect_one in the same order, so the results are those
+// of the thread form bit for bit, and the first levels, which all of a
+// block's eigenvalues share, are counted once per node.
+// ------------------------------------------------------------------------
+struct BisNode {
+  double a, b;
+  int na, nb, it, blk;   // counts at a and b, steps done, block
+};
+struct BisState {
+  int na, nb, it, pad;   // a single eigenvalue's state (a, b in Wt, Et); it < 0: none
+};
+#define BIS_DEPTH 16     // tree levels before the remaining nodes are split up
+
+__device__ __forceinline__ bool bis_block_ok(const BlockDev *B, const ProbDev *p) {
+  return !(p->trivial || p->jobz == MR3_JOB_C || p->status) &&
+         !(B->nbl < 2 || B->mbl <= 0 || B->none) && B->nab2 > B->nab1;
+}
+
+// Eigenvalues na+1..nb of an interval: results (done) or single states.
+__device__ __forceinline__ void bis_finish(const BlockDev *B, double a, double b, int na, int nb,
+                                           int it, bool done, double *Wt, double *Et, int *It,
+                                           BisState *st) {
+  for (int j = na + 1; j <= nb; j++) {
+    const int g = B->ibgn + (j - B->nab1 - 1);
+    if (done) {
+      Wt[g] = 0.5 * (a + b);
+      Et[g] = 0.5 * fabs(a - b);
+      It[g] = j;
+    } else {
+      Wt[g] = a;
+      Et[g] = b;
+      BisState q;
+      q.na = na; q.nb = nb; q.it = it; q.pad = 0;
+      st[g] = q;
+    }
+  }
+}
+
+// The children of a node after its count cnt (already clamped to [na, nb]):
+// kind 0 empty, 1 done, 2 one eigenvalue, 3 a node of the next level.
+__device__ __forceinline__ int bis_child(const BisNode &nd, int cnt, int side, double pivmin,
+                                         double abstol, double reltol, int itmax, BisNode *ch) {
+  const double c = 0.5 * (nd.a + nd.b);
+  ch->a = side ? c : nd.a;
+  ch->b = side ? nd.b : c;
+  ch->na = side ? cnt : nd.na;
+  ch->nb = side ? nd.nb : cnt;
+  ch->it = nd.it + 1;
+  ch->blk = nd.blk;
+  if (ch->nb <= ch->na) return 0;
+  const double w = fabs(ch->b - ch->a), t = fmax(fabs(ch->b), fabs(ch->a));
+  if (w < fmax(fmax(abstol, pivmin), reltol * t) || ch->it >= itmax) return 1;
+  return ch->nb - ch->na == 1 ? 2 : 3;
+}
+
+__global__ void __launch_bounds__(256)
+k_bis_roots(int N, const ProbDev *probs, const BlockDev *blocks, const int *blk_of_row,
+            BisNode *out, int *n_out, double *Wt, double *Et, int *It, BisState *st) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= N) return;
+  const int bk = blk_of_row[g];
+  const BlockDev *B = &blocks[bk];
+  if (g != B->ibgn) return;
+  const ProbDev *p = &probs[B->prob];
+  if (!bis_block_ok(B, p)) return;
+  if (B->itmax2 <= 0) {
+    bis_finish(B, B->gl3, B->gu3, B->nab1, B->nab2, 0, true, Wt, Et, It, st);
+  } else if (B->nab2 - B->nab1 == 1) {
+    bis_finish(B, B->gl3, B->gu3, B->nab1, B->nab2, 0, false, Wt, Et, It, st);
+  } else {
+    BisNode nd;
+    nd.a = B->gl3; nd.b = B->gu3; nd.na = B->nab1; nd.nb = B->nab2; nd.it = 0; nd.blk = bk;
+    out[atomicAdd(n_out, 1)] = nd;
+  }
+}
+
+// One level: a Sturm count per node; done and single children written out,
+// the number of next-level children per CTA in bcnt.
+__global__ void __launch_bounds__(256)
+k_bis_count(const BisNode *in, int n_in, const ProbDev *probs, const BlockDev *blocks,
+            const double2 *TP, Tol tol, int *ccnt, int *bcnt, double *Wt, double *Et, int *It,
+            BisState *st, unsigned long long *stats) {
+  __shared__ int sint[32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int nnext = 0;
+  unsigned long long work = 0;
+  if (i < n_in) {
+    const BisNode nd = in[i];
+    const BlockDev *B = &blocks[nd.blk];
+    const double pivmin = probs[B->prob].pivmin;
+    int cnt = dv_count_bisect(B->nbl, TP + B->ibgn, pivmin, 0.5 * (nd.a + nd.b));
+    cnt = d_imin(nd.nb, d_imax(nd.na, cnt));
+    ccnt[i] = cnt;
+    work = (unsigned long long)B->nbl;
+    for (int side = 0; side < 2; side++) {
+      BisNode ch;
+      const int kind = bis_child(nd, cnt, side, pivmin, B->atoli, tol.bsrtol, B->itmax2, &ch);
+      if (kind == 1 || kind == 2)
+        bis_finish(B, ch.a, ch.b, ch.na, ch.nb, ch.it, kind == 1, Wt, Et, It, st);
+      else if (kind == 3)
+        nnext++;
+    }
+  }
+  int total;
+  cta_exscan(nnext, sint, &total);
+  if (threadIdx.x == 0) bcnt[blockIdx.x] = total;
+  stat_add(stats, KID_BISECT * 4 + 0, work);
+}
+
+// Exclusive scan of the per-CTA counts (one CTA of 1024 threads); the total
+// is the next level's length.
+__global__ void __launch_bounds__(1024) k_bis_scan(int nblk, int *bcnt, int *n_out) {
+  __shared__ int sint[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int b0 = 0; b0 < nblk; b0 += 1024) {
+    const int b = b0 + threadIdx.x;
+    const int v = b < nblk ? bcnt[b] : 0;
+    int total;
+    const int ex = cta_exscan(v, sint, &total);
+    if (b < nblk) bcnt[b] = carry + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *n_out = carry;
+}
+
+// The next level's nodes, in the order of their parents (a block's nodes
+// stay together).  split: the depth limit is reached and the nodes' eigenvalues
+// leave the tree as single states instead.
+__global__ void __launch_bounds__(256)
+k_bis_scatter(const BisNode *in, int n_in, const ProbDev *probs, const BlockDev *blocks, Tol tol,
+              const int *ccnt, const int *bcnt, BisNode *out, int split, double *Wt, double *Et,
+              int *It, BisState *st) {
+  __shared__ int sint[32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  BisNode ch[2];
+  int kind[2] = {0, 0}, nnext = 0;
+  const BlockDev *B = nullptr;
+  if (i < n_in) {
+    const BisNode nd = in[i];
+    B = &blocks[nd.blk];
+    const double pivmin = probs[B->prob].pivmin;
+    for (int side = 0; side < 2; side++) {
+      kind[side] = bis_child(nd, ccnt[i], side, pivmin, B->atoli, tol.bsrtol, B->itmax2, &ch[side]);
+      nnext += kind[side] == 3;
+    }
+  }
+  int total;
+  int pos = bcnt[blockIdx.x] + cta_exscan(split ? 0 : nnext, sint, &total);
+  for (int side = 0; side < 2; side++)
+    if (kind[side] == 3) {
+      if (split) bis_finish(B, ch[side].a, ch[side].b, ch[side].na, ch[side].nb, ch[side].it, false,
+                            Wt, Et, It, st);
+      else out[pos++] = ch[side];
+    }
+}
+
+// The single eigenvalues that left the tree, a thread each, continued with
+// dv_bisect_one from their state.
+__global__ void __launch_bounds__(128)
+k_bisect_cont(int N, const ProbDev *probs, const BlockDev *blocks, const int *blk_of_row,
+              const double2 *TP, double *Wt, double *Et, int *It, const BisState *st, Tol tol,
+              unsigned long long *stats) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long work = 0;
+  if (g < N) {
+    const BisState q = st[g];
+    if (q.it >= 0) {
+      const BlockDev *B = &blocks[blk_of_row[g]];
+      const ProbDev *p = &probs[B->prob];
+      const int j = B->nab1 + 1 + (g - B->ibgn);
+      double a = Wt[g], b = Et[g];
+      int it = q.it;
+      dv_bisect_one(B->nbl, TP + B->ibgn, p->pivmin, B->atoli, tol.bsrtol, B->itmax2, j, &a, &b,
+                    q.na, q.nb, &it, q.it);
+      Wt[g] = 0.5 * (a + b);
+      Et[g] = 0.5 * fabs(a - b);
+      It[g] = j;
+      work = (unsigned long long)(it - q.it) * (unsigned long long)B->nbl;
+    }
+  }
+  stat_add(stats, KID_BISECT * 4 + 0, work);
+}
+
+// ------------------------------------------------------------------------
 // Stage A3: per problem, place each block's approximations in W after the
 // dlarrd discard of range I (SRC/LAPACK/odrrd.f:520-640).
 // ------------------------------------------------------------------------
@@ -2170,6 +2368,9 @@ struct mr3_cuda_ctx {
   int *act[2] = {nullptr, nullptr}, *bsl = nullptr, *sbcnt = nullptr;
   int *rl = nullptr, *rl_n = nullptr;       // a level's cluster eigenvalues to refine
   int *sbk = nullptr;                       // singleton size buckets (3 x 16)
+  BisNode *bis_nodes[2] = {nullptr, nullptr}; // shared-interval bisection: levels
+  int *bis_cnt = nullptr, *bis_bcnt = nullptr, *bis_n = nullptr;
+  BisState *bis_st = nullptr;
   int2 *done_list = nullptr;                // finished column tiles (problem, tile)
   int *tile_left = nullptr;                 // unwritten columns of each tile
   size_t capTiles = 0;
@@ -2192,6 +2393,7 @@ struct mr3_cuda_ctx {
   int *h_flag = nullptr;
   double *h_const = nullptr;   // {1.0}
   int *h_iconst = nullptr;     // {1, 1}
+  int *h_bisn = nullptr;       // a level's node count of the shared-interval bisection
   void *ws[MR3_CUDA_WS_SLOTS] = {nullptr};
   size_t ws_cap[MR3_CUDA_WS_SLOTS] = {0};
   // profiling: per-kernel CUDA-event timing and device work counters
@@ -2304,6 +2506,11 @@ static int ensure_rows(mr3_cuda_ctx *c, size_t N, size_t P) {
     CK(regrow(&c->rl, n), "rl");
     CK(regrow(&c->sflag, n), "sflag");
     CK(regrow(&c->sbcnt, 2 * (n / LIST_T + 1)), "sbcnt");
+    CK(regrow(&c->bis_nodes[0], n / 2 + 1), "bis nodes");
+    CK(regrow(&c->bis_nodes[1], n / 2 + 1), "bis nodes");
+    CK(regrow(&c->bis_cnt, n / 2 + 1), "bis cnt");
+    CK(regrow(&c->bis_bcnt, (n / 2 + 1) / 256 + 1), "bis bcnt");
+    CK(regrow(&c->bis_st, n), "bis st");
     c->capN = n;
   }
   if (P > c->capP) {
@@ -2346,12 +2553,14 @@ extern "C" int mr3_cuda_ctx_create(int device, mr3_cuda_ctx **out) {
       cudaMalloc((void **)&c->lc, 2 * sizeof(LevelCounters)) != cudaSuccess ||
       cudaMalloc((void **)&c->sc, sizeof(SngCounters)) != cudaSuccess ||
       cudaMalloc((void **)&c->rl_n, sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void **)&c->bis_n, 2 * sizeof(int)) != cudaSuccess ||
       cudaMalloc((void **)&c->sbk, 3 * SNG_BUCKETS * sizeof(int)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_lc, 2 * sizeof(LevelCounters)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_sc, sizeof(SngCounters)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_snap, SNG_ROUNDS * sizeof(int)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_const, sizeof(double)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_iconst, 2 * sizeof(int)) != cudaSuccess ||
+      cudaMallocHost((void **)&c->h_bisn, sizeof(int)) != cudaSuccess ||
       cudaMalloc((void **)&c->stats, KID_COUNT * 4 * sizeof(unsigned long long)) != cudaSuccess ||
       cudaHostGetDevicePointer((void **)&c->d_hlc, c->h_lc, 0) != cudaSuccess ||
       cudaHostGetDevicePointer((void **)&c->d_hsc, c->h_sc, 0) != cudaSuccess ||
@@ -2378,14 +2587,15 @@ extern "C" void mr3_cuda_ctx_destroy(mr3_cuda_ctx *c) {
                  c->prob_of_slot, c->cl_of_slot, c->lvl_of_slot, c->unit_list, c->flag, c->tmp2,
                  c->D, c->E, c->E2, c->Wt, c->Et, c->W, c->Werr, c->Wgap, c->Wcopy, c->Wsh,
                  c->Dt, c->Lt, c->Wout, c->gers, c->TP, c->TPc, c->RP, c->RQ, c->rec0, c->rec1,
-                 c->cl[0], c->cl[1], c->sng, c->sst, c->act[0], c->act[1], c->bsl, c->sflag, c->sbcnt, c->rl, c->rl_n, c->sbk, c->done_list, c->tile_left, c->lc, c->sc, c->scratch, c->arena[0],
+                 c->cl[0], c->cl[1], c->sng, c->sst, c->act[0], c->act[1], c->bsl, c->sflag, c->sbcnt, c->rl, c->rl_n, c->sbk, c->done_list, c->tile_left,
+                 c->bis_nodes[0], c->bis_nodes[1], c->bis_cnt, c->bis_bcnt, c->bis_n, c->bis_st, c->lc, c->sc, c->scratch, c->arena[0],
                  c->cls_ns, c->cls_soff, c->cls_cbase, c->cls_abase,
                  c->arena[1], (void *)c->Din, (void *)c->Ein, c->Wp, c->Dp, c->Ep};
   for (void *q : dev)
     if (q) cudaFree(q);
   for (int i = 0; i < MR3_CUDA_WS_SLOTS; i++)
     if (c->ws[i]) cudaFree(c->ws[i]);
-  void *host[] = {c->h_probs, c->h_ptrs, c->h_lc, c->h_sc, c->h_flag, c->h_const, c->h_iconst,
+  void *host[] = {c->h_probs, c->h_ptrs, c->h_lc, c->h_sc, c->h_flag, c->h_const, c->h_iconst, c->h_bisn,
                   c->h_done, c->h_snap};
   for (void *q : host)
     if (q) cudaFreeHost(q);
@@ -2755,10 +2965,32 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
   unsigned long long *stats = c->prof ? c->stats : nullptr;
   {
     const int Lb = tree_lanes(NN, (long long)c->nsm * 2048, tree_max);
-    if (Lb == 1)
-      LAUNCH(k_bisect<false>, gN128, 128, NN, 1, c->probs, c->blocks, c->blk_of_row, c->TP, c->Wt,
-             c->Et, c->It, tol, stats);
-    else
+    if (Lb == 1) {
+      // shared intervals breadth-first, then a thread per eigenvalue
+      CK(cudaMemsetAsync(c->bis_st, 0xff, N * sizeof(BisState), st), "bis st");
+      CK(cudaMemsetAsync(c->bis_n, 0, 2 * sizeof(int), st), "bis n");
+      LAUNCH(k_bis_roots, gN, 256, NN, c->probs, c->blocks, c->blk_of_row, c->bis_nodes[0],
+             c->bis_n, c->Wt, c->Et, c->It, c->bis_st);
+      CK(cudaMemcpyAsync(c->h_bisn, c->bis_n, sizeof(int), cudaMemcpyDeviceToHost, st), "bis n");
+      CK(cudaStreamSynchronize(st), "bis sync");
+      int nin = c->h_bisn[0], cur = 0;
+      for (int depth = 0; nin > 0; depth++) {
+        const int nb = (nin + 255) / 256, split = depth + 1 >= BIS_DEPTH;
+        LAUNCH(k_bis_count, nb, 256, c->bis_nodes[cur], nin, c->probs, c->blocks, c->TP, tol,
+               c->bis_cnt, c->bis_bcnt, c->Wt, c->Et, c->It, c->bis_st, stats);
+        if (!split) LAUNCH(k_bis_scan, 1, 1024, nb, c->bis_bcnt, c->bis_n + 1);
+        LAUNCH(k_bis_scatter, nb, 256, c->bis_nodes[cur], nin, c->probs, c->blocks, tol, c->bis_cnt,
+               c->bis_bcnt, c->bis_nodes[cur ^ 1], split, c->Wt, c->Et, c->It, c->bis_st);
+        if (split) break;
+        CK(cudaMemcpyAsync(c->h_bisn, c->bis_n + 1, sizeof(int), cudaMemcpyDeviceToHost, st),
+           "bis n");
+        CK(cudaStreamSynchronize(st), "bis sync");
+        nin = c->h_bisn[0];
+        cur ^= 1;
+      }
+      LAUNCH(k_bisect_cont, gN128, 128, NN, c->probs, c->blocks, c->blk_of_row, c->TP, c->Wt,
+             c->Et, c->It, c->bis_st, tol, stats);
+    } else
       LAUNCH(k_bisect<true>, (int)(((long long)NN * Lb + 127) / 128), 128, NN, Lb, c->probs,
              c->blocks, c->blk_of_row, c->TP, c->Wt, c->Et, c->It, tol, stats);
   }

@@ -412,8 +412,8 @@ def main():
             # DRAM bytes per dlar1v row of the round kernels, measured with ncu
             # (dram__bytes_read.sum + dram__bytes_write.sum) on a 256-problem
             # mixed batch (n <= 1024), scaled by this run's dlar1v rows
-            traffic = {"bytes_per_launch": 28.1 * ctr[4][2] / max(tcnt, 1),
-                       "source": "ncu on a 256-problem mixed batch: 28.1 B per dlar1v row, "
+            traffic = {"bytes_per_launch": 25.5 * ctr[4][2] / max(tcnt, 1),
+                       "source": "ncu on a 256-problem mixed batch: 25.5 B per dlar1v row, "
                                  "scaled by the live dlar1v-row counter"}
         roof = {"bound": "fp64-div", "kernel": tname, "achieved": achieved,
                 "peak": div_gops, "unit": "Gdiv/s",

@@ -294,6 +294,59 @@ def run_reference(args):
 # --------------------------------------------------------------------------
 # GPU arm
 # --------------------------------------------------------------------------
+_DENSE_REF = r"""
+import json, os, sys, time
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import oracle
+n, seed, threads = int(sys.argv[2]), int(sys.argv[3]), int(sys.argv[4])
+rng = np.random.default_rng(seed)
+B = rng.uniform(-1.0, 1.0, (n, n))
+A = (B + B.T) * 0.5
+t0 = time.perf_counter()
+r = oracle.ref_dsyeig("V", "A", "L", A, threads=threads)
+print(json.dumps({"seconds": time.perf_counter() - t0, "info": r["info"], "m": r["m"]}))
+"""
+
+
+def run_dense(M, n, seed, with_ref):
+    """The dense driver dsyeig (SRC/dense.c:151-232) on a seeded n x n
+    symmetric matrix, entries U(-1, 1): wall time through the C ABI from host
+    memory (reduction, tridiagonal solve, back-transformation and the copies
+    included), checked by residual and orthogonality; beside it the
+    reference's dsyeig on the host cores (a separate process, so that its
+    LAPACK runs with all cores)."""
+    rng = np.random.default_rng(seed)
+    B = rng.uniform(-1.0, 1.0, (n, n))
+    A = (B + B.T) * 0.5
+    M.dsyeig("V", "A", "L", A[:64, :64])   # loads the device LAPACK
+    t0 = time.perf_counter()
+    r = M.dsyeig("V", "A", "L", A)
+    sec = time.perf_counter() - t0
+    if r["info"] != 0:
+        return {"n": n, "info": r["info"]}
+    Z, W = r["Z"], r["W"]
+    eps = np.finfo(np.float64).eps
+    nrm = np.abs(W).max()
+    out = {"n": n, "seconds": sec, "eigenpairs_per_s": n / sec, "api": "dsyeig (C ABI), host arrays",
+           "resid": float(np.abs(A @ Z - Z * W).max() / (n * eps * nrm)),
+           "orth": float(np.abs(Z.T @ Z - np.eye(n)).max() / (n * eps)),
+           "steps": "dsytrd and dormtr: cuSOLVER; tridiagonal: this solver"}
+    if with_ref and os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libmrrr_ref.so")):
+        cores = os.cpu_count() or 1
+        env = dict(os.environ, OPENBLAS_NUM_THREADS=str(cores))
+        p = subprocess.run([sys.executable, "-c", _DENSE_REF, ROOT, str(n), str(seed), str(cores)],
+                           env=env, capture_output=True, text=True, timeout=1800)
+        try:
+            ref = json.loads(p.stdout.strip().splitlines()[-1])
+            out["reference"] = {"seconds": ref["seconds"], "eigenpairs_per_s": n / ref["seconds"],
+                                "cores": cores, "kind": "reference",
+                                "setup": "reference dsyeig, OpenBLAS and PMR_NUM_THREADS = cores"}
+        except Exception:
+            out["reference"] = {"error": (p.stderr or "")[-300:]}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -313,6 +366,9 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=40.0)
     ap.add_argument("--serve-count", type=int, default=400)
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--dense", type=int, default=0,
+                    help="also time the dense driver dsyeig on an n x n symmetric matrix "
+                         "(and the reference's on the host cores); 0 = off")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -520,6 +576,10 @@ def main():
     if rank == 0 and ws == 1 and not args.no_cpu:
         _, cpu = cpu_reference(problems, args.cpu_seconds)
 
+    dense = None
+    if rank == 0 and args.dense > 0:
+        dense = run_dense(M, args.dense, args.seed, not args.no_cpu)
+
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -538,7 +598,7 @@ def main():
                          f"{zbytes / 1e9:.1f} GB of Z"},
         "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "roofline": roof,
         "roofline_hbm": roof_hbm, "fp64_peaks": {"fma_tflops": fma_tflops, "div_gops": div_gops},
-        "percall": percall, "serving": serving, "cpu_baseline": cpu,
+        "percall": percall, "serving": serving, "cpu_baseline": cpu, "dense": dense,
         "kernels_ms_per_step": {k: v[0] / args.steps for k, v in
                                 sorted(kern.items(), key=lambda kv: -kv[1][0])},
         "work_counters": dict(zip(groups, ctr)),

@@ -82,6 +82,25 @@ int  mr3_server_poll(mr3_server *s, long long ticket, int wait, double *latency_
 int  mr3_server_stats(mr3_server *s, long long *submitted, long long *solved, long long *batches);
 void mr3_server_destroy(mr3_server *s);
 
+/* Replaces int dsyeig(...) of INCLUDE/mrrr.h:270-272 (implementation
+ * SRC/dense.c:151-232): all or some eigenpairs of the dense symmetric n x n
+ * matrix A (column-major, leading dimension lda; uplo "L" or "U" selects the
+ * stored triangle).  jobz, range, vl, vu, il, iu, m, W and Z (leading
+ * dimension ldz) mean what they mean for mrrr(); A is scaled, reduced to
+ * tridiagonal form, solved and back-transformed on the device (A on the host
+ * is left unchanged; the reference's contract allows it to be overwritten).
+ * Returns 0, 1 for a bad argument (also lda < n, or ldz < n with jobz "V"),
+ * 2 on an internal failure (also when the device's LAPACK library, cuSOLVER,
+ * cannot be loaded). */
+int dsyeig(char *jobz, char *range, char *uplo, int *n, double *A, int *lda,
+           double *vl, double *vu, int *il, int *iu, int *m, double *W,
+           double *Z, int *ldz);
+
+/* Replaces the Fortran binding dsyeig_ of SRC/dense.c:1037-1043. */
+void dsyeig_(char *jobz, char *range, char *uplo, int *n, double *A, int *lda,
+             double *vl, double *vu, int *il, int *iu, int *m, double *W,
+             double *Z, int *ldz, int *info);
+
 /* Kernels launched by the calling thread's last solve (diagnostics). */
 long long mr3_last_launches(void);
 

@@ -63,6 +63,9 @@ def lib() -> C.CDLL:
         L.mr3_batched.argtypes = [C.c_int, C.POINTER(HostProb)]
         L.mr3_batched_device.restype = C.c_int
         L.mr3_batched_device.argtypes = [C.c_int, C.POINTER(CudaProb), C.c_void_p]
+        L.dsyeig.restype = C.c_int
+        L.dsyeig.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pi, _pd, _pd, _pi,
+                             _pi, _pi, _pd, _pd, _pi]
         L.mr3_last_launches.restype = C.c_longlong
         L.mr3_last_error.restype = C.c_char_p
         _lib = L
@@ -117,6 +120,40 @@ def mrrr(jobz: str, rng: str, D, E, vl: float = 0.0, vu: float = 0.0, il: int = 
     if want_z:
         out["Z"] = Z[: ldz * m].reshape(m, ldz).T[:n].copy() if m > 0 else np.zeros((n, 0))
         out["Zsupp"] = Zs[: 2 * m].copy()
+    return out
+
+
+def dsyeig(jobz: str, rng: str, uplo: str, A, vl: float = 0.0, vu: float = 0.0, il: int = 1,
+           iu: int = 1, lda: int | None = None, ldz: int | None = None) -> dict:
+    """Eigenpairs of a dense symmetric matrix through the C ABI ``dsyeig()``.
+
+    ``A`` is an (n, n) array of which the ``uplo`` triangle is read.  Returns
+    a dict with ``info``, ``m``, ``W`` (m,), ``Z`` (n, m) for jobz "V", and the
+    refined ``vl, vu, il, iu``.
+    """
+    L = lib()
+    A = np.asarray(A, dtype=np.float64)
+    n = int(A.shape[0])
+    lda = n if lda is None else int(lda)
+    Ah = np.zeros(lda * max(n, 1))
+    if n > 0 and lda > 0:
+        r = min(n, lda)   # (lda < n is an argument error the library reports)
+        Ah.reshape(n, lda)[:, :r] = A.T[:, :r]   # column-major, leading dimension lda
+    ldz = n if ldz is None else int(ldz)
+    want_z = jobz[0] in "Vv"
+    W = np.zeros(max(n, 1))
+    Z = np.zeros(_ncols(jobz, rng, n, il, iu) * (ldz if want_z else 1))
+    n_, lda_, ldz_ = C.c_int(n), C.c_int(lda), C.c_int(ldz)
+    vl_, vu_, il_, iu_, m_ = C.c_double(vl), C.c_double(vu), C.c_int(il), C.c_int(iu), C.c_int(0)
+    info = L.dsyeig(jobz.encode(), rng.encode(), uplo.encode(), C.byref(n_),
+                    Ah.ctypes.data_as(_pd), C.byref(lda_), C.byref(vl_), C.byref(vu_),
+                    C.byref(il_), C.byref(iu_), C.byref(m_), W.ctypes.data_as(_pd),
+                    Z.ctypes.data_as(_pd), C.byref(ldz_))
+    m = m_.value if info == 0 else 0
+    out = dict(info=info, m=m, W=W[:m].copy(), vl=vl_.value, vu=vu_.value, il=il_.value,
+               iu=iu_.value)
+    if want_z:
+        out["Z"] = Z[: ldz * m].reshape(m, ldz).T[:n].copy() if m > 0 else np.zeros((n, 0))
     return out
 
 

@@ -73,7 +73,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         objs.append(obj)
     tmp = LIB + ".tmp"
     cmd = [nvcc, "-shared", "-cudart", "static", "-Wno-deprecated-gpu-targets", "-o", tmp, *objs,
-           "-lpthread"]
+           "-lpthread", "-ldl"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

@@ -86,6 +86,10 @@ def ref_lib() -> C.CDLL | None:
         os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
         L = C.CDLL(REF_SO)
         _mrrr_sig(L.mrrr)
+        if hasattr(L, "dsyeig"):
+            L.dsyeig.restype = C.c_int
+            L.dsyeig.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pi, _pd, _pd,
+                                 _pi, _pi, _pi, _pd, _pd, _pi]
         _libs["ref"] = L
     return _libs["ref"]
 
@@ -138,3 +142,33 @@ def ref_mrrr(jobz, rng, D, E, vl=0.0, vu=0.0, il=1, iu=1, tryrac=0, ldz=None,
         raise RuntimeError("reference library not built (oracle/_ref)")
     os.environ["PMR_NUM_THREADS"] = str(threads)
     return _call(L.mrrr, jobz, rng, D, E, vl, vu, il, iu, tryrac, ldz)
+
+
+def ref_dsyeig(jobz, rng, uplo, A, vl=0.0, vu=0.0, il=1, iu=1, threads: int = 2):
+    """The reference's own dense driver dsyeig() (SRC/dense.c:151-232; needs
+    the _ref build): scipy's LAPACK dsytrd/dormtr around the reference's
+    mrrr().  A is an (n, n) array; returns info, m, W, Z, vl, vu, il, iu."""
+    L = ref_lib()
+    if L is None:
+        raise RuntimeError("reference library not built (oracle/_ref)")
+    os.environ["PMR_NUM_THREADS"] = str(threads)
+    A = np.asarray(A, dtype=np.float64)
+    n = A.shape[0]
+    Af = np.array(A.T, dtype=np.float64, copy=True).reshape(-1)   # column-major
+    want_z = jobz[0] in "Vv"
+    W = np.zeros(max(n, 1))
+    # the reference back-transforms Z (dormtr) for every jobz, so Z must hold
+    # n x m doubles even when no eigenvectors are wanted
+    Z = np.zeros(max(n, 1) * max(n, 1))
+    n_, lda_, ldz_ = C.c_int(n), C.c_int(n), C.c_int(n)
+    vl_, vu_, il_, iu_, m_ = C.c_double(vl), C.c_double(vu), C.c_int(il), C.c_int(iu), C.c_int(0)
+    info = L.dsyeig(jobz.encode(), rng.encode(), uplo.encode(), C.byref(n_),
+                    Af.ctypes.data_as(_pd), C.byref(lda_), C.byref(vl_), C.byref(vu_),
+                    C.byref(il_), C.byref(iu_), C.byref(m_), W.ctypes.data_as(_pd),
+                    Z.ctypes.data_as(_pd), C.byref(ldz_))
+    m = m_.value
+    out = dict(info=info, m=m, W=W[:m].copy(), vl=vl_.value, vu=vu_.value, il=il_.value,
+               iu=iu_.value)
+    if want_z:
+        out["Z"] = Z[: n * m].reshape(m, n).T.copy() if m > 0 else np.zeros((n, 0))
+    return out

@@ -101,6 +101,44 @@ void dsyeig_(char *jobz, char *range, char *uplo, int *n, double *A, int *lda,
              double *vl, double *vu, int *il, int *iu, int *m, double *W,
              double *Z, int *ldz, int *info);
 
+/* Replaces int dspeig(...) of INCLUDE/mrrr.h:444-446 (implementation
+ * SRC/dense.c:319-398): dsyeig with A in LAPACK packed storage AP
+ * (n(n+1)/2 doubles, the uplo triangle column by column); AP on the host is
+ * left unchanged.  Same returns as dsyeig. */
+int dspeig(char *jobz, char *range, char *uplo, int *n, double *AP,
+           double *vl, double *vu, int *il, int *iu, int *m, double *W,
+           double *Z, int *ldz);
+void dspeig_(char *jobz, char *range, char *uplo, int *n, double *AP,
+             double *vl, double *vu, int *il, int *iu, int *m, double *W,
+             double *Z, int *ldz, int *info);   /* SRC/dense.c:1056-1062 */
+
+/* Replaces int dsygeig(...) of INCLUDE/mrrr.h:352-354 (implementation
+ * SRC/dense.c:236-313): the generalized symmetric-definite problem,
+ * itype 1 A x = lambda B x, 2 A B x = lambda x, 3 B A x = lambda x, B
+ * positive definite (leading dimension ldb).  On return B holds its
+ * Cholesky factor (uplo triangle) and, for jobz "V", the first m columns of
+ * A the eigenvectors, as in the reference.  n <= 1 is a bad argument there
+ * and here.  Returns 2 also when B is not positive definite. */
+int dsygeig(int *itype, char *jobz, char *range, char *uplo, int *n,
+            double *A, int *lda, double *B, int *ldb, double *vl,
+            double *vu, int *il, int *iu, int *m, double *W);
+void dsygeig_(int *itype, char *jobz, char *range, char *uplo, int *n,
+              double *A, int *lda, double *B, int *ldb, double *vl,
+              double *vu, int *il, int *iu, int *m, double *W,
+              int *info);   /* SRC/dense.c:1046-1053 */
+
+/* Replaces int dspgeig(...) of INCLUDE/mrrr.h:526-529 (implementation
+ * SRC/dense.c:403-470): dsygeig with A and B in packed storage; the
+ * eigenvectors go to Z (leading dimension ldz) and BP returns the packed
+ * Cholesky factor. */
+int dspgeig(int *itype, char *jobz, char *range, char *uplo, int *n,
+            double *AP, double *BP, double *vl, double *vu, int *il,
+            int *iu, int *m, double *W, double *Z, int *ldz);
+void dspgeig_(int *itype, char *jobz, char *range, char *uplo, int *n,
+              double *AP, double *BP, double *vl, double *vu, int *il,
+              int *iu, int *m, double *W, double *Z, int *ldz,
+              int *info);   /* SRC/dense.c:1065-1072 */
+
 /* Kernels launched by the calling thread's last solve (diagnostics). */
 long long mr3_last_launches(void);
 

@@ -66,6 +66,15 @@ def lib() -> C.CDLL:
         L.dsyeig.restype = C.c_int
         L.dsyeig.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pi, _pd, _pd, _pi,
                              _pi, _pi, _pd, _pd, _pi]
+        L.dspeig.restype = C.c_int
+        L.dspeig.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pd, _pd, _pi, _pi,
+                             _pi, _pd, _pd, _pi]
+        L.dsygeig.restype = C.c_int
+        L.dsygeig.argtypes = [_pi, C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pi, _pd, _pi,
+                              _pd, _pd, _pi, _pi, _pi, _pd]
+        L.dspgeig.restype = C.c_int
+        L.dspgeig.argtypes = [_pi, C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pd, _pd, _pd,
+                              _pi, _pi, _pi, _pd, _pd, _pi]
         L.mr3_last_launches.restype = C.c_longlong
         L.mr3_last_error.restype = C.c_char_p
         _lib = L
@@ -152,6 +161,88 @@ def dsyeig(jobz: str, rng: str, uplo: str, A, vl: float = 0.0, vu: float = 0.0, 
     m = m_.value if info == 0 else 0
     out = dict(info=info, m=m, W=W[:m].copy(), vl=vl_.value, vu=vu_.value, il=il_.value,
                iu=iu_.value)
+    if want_z:
+        out["Z"] = Z[: ldz * m].reshape(m, ldz).T[:n].copy() if m > 0 else np.zeros((n, 0))
+    return out
+
+
+def pack(A, uplo: str):
+    """The uplo triangle of a square array in LAPACK packed storage."""
+    A = np.asarray(A, dtype=np.float64)
+    n = A.shape[0]
+    if uplo[0] in "Ll":
+        return np.concatenate([A[j:, j] for j in range(n)]) if n else np.zeros(0)
+    return np.concatenate([A[: j + 1, j] for j in range(n)]) if n else np.zeros(0)
+
+
+def dspeig(jobz: str, rng: str, uplo: str, AP, n: int, vl: float = 0.0, vu: float = 0.0,
+           il: int = 1, iu: int = 1, ldz: int | None = None) -> dict:
+    """``dspeig()``: dsyeig with A in packed storage (``AP``, see :func:`pack`)."""
+    L = lib()
+    AP = np.array(AP, dtype=np.float64, copy=True)
+    ldz = n if ldz is None else int(ldz)
+    want_z = jobz[0] in "Vv"
+    W = np.zeros(max(n, 1))
+    Z = np.zeros(_ncols(jobz, rng, n, il, iu) * (ldz if want_z else 1))
+    n_, ldz_ = C.c_int(n), C.c_int(ldz)
+    vl_, vu_, il_, iu_, m_ = C.c_double(vl), C.c_double(vu), C.c_int(il), C.c_int(iu), C.c_int(0)
+    info = L.dspeig(jobz.encode(), rng.encode(), uplo.encode(), C.byref(n_),
+                    AP.ctypes.data_as(_pd), C.byref(vl_), C.byref(vu_), C.byref(il_),
+                    C.byref(iu_), C.byref(m_), W.ctypes.data_as(_pd), Z.ctypes.data_as(_pd),
+                    C.byref(ldz_))
+    m = m_.value if info == 0 else 0
+    out = dict(info=info, m=m, W=W[:m].copy(), vl=vl_.value, vu=vu_.value, il=il_.value,
+               iu=iu_.value)
+    if want_z:
+        out["Z"] = Z[: ldz * m].reshape(m, ldz).T[:n].copy() if m > 0 else np.zeros((n, 0))
+    return out
+
+
+def dsygeig(itype: int, jobz: str, rng: str, uplo: str, A, B, vl: float = 0.0, vu: float = 0.0,
+            il: int = 1, iu: int = 1) -> dict:
+    """``dsygeig()``: the generalized problem (itype 1 A x = l B x, 2 A B x = l x,
+    3 B A x = l x).  Returns ``info, m, W``, the eigenvectors ``Z`` (n, m) for
+    jobz "V" (the library returns them in A) and ``B`` (its Cholesky factor)."""
+    L = lib()
+    A = np.asarray(A, dtype=np.float64)
+    n = int(A.shape[0])
+    Af = np.array(A.T, dtype=np.float64, copy=True).reshape(-1)
+    Bf = np.array(np.asarray(B, dtype=np.float64).T, copy=True).reshape(-1)
+    W = np.zeros(max(n, 1))
+    it_, n_, lda_, ldb_ = C.c_int(itype), C.c_int(n), C.c_int(n), C.c_int(n)
+    vl_, vu_, il_, iu_, m_ = C.c_double(vl), C.c_double(vu), C.c_int(il), C.c_int(iu), C.c_int(0)
+    info = L.dsygeig(C.byref(it_), jobz.encode(), rng.encode(), uplo.encode(), C.byref(n_),
+                     Af.ctypes.data_as(_pd), C.byref(lda_), Bf.ctypes.data_as(_pd),
+                     C.byref(ldb_), C.byref(vl_), C.byref(vu_), C.byref(il_), C.byref(iu_),
+                     C.byref(m_), W.ctypes.data_as(_pd))
+    m = m_.value if info == 0 else 0
+    out = dict(info=info, m=m, W=W[:m].copy(), vl=vl_.value, vu=vu_.value, il=il_.value,
+               iu=iu_.value, B=Bf.reshape(max(n, 1), n).T.copy() if n else Bf)
+    if jobz[0] in "Vv":
+        out["Z"] = Af[: n * m].reshape(m, n).T.copy() if m > 0 else np.zeros((n, 0))
+    return out
+
+
+def dspgeig(itype: int, jobz: str, rng: str, uplo: str, AP, BP, n: int, vl: float = 0.0,
+            vu: float = 0.0, il: int = 1, iu: int = 1, ldz: int | None = None) -> dict:
+    """``dspgeig()``: dsygeig with A and B in packed storage; ``BP`` returns the
+    packed Cholesky factor."""
+    L = lib()
+    AP = np.array(AP, dtype=np.float64, copy=True)
+    BP = np.array(BP, dtype=np.float64, copy=True)
+    ldz = n if ldz is None else int(ldz)
+    want_z = jobz[0] in "Vv"
+    W = np.zeros(max(n, 1))
+    Z = np.zeros(_ncols(jobz, rng, n, il, iu) * (ldz if want_z else 1))
+    it_, n_, ldz_ = C.c_int(itype), C.c_int(n), C.c_int(ldz)
+    vl_, vu_, il_, iu_, m_ = C.c_double(vl), C.c_double(vu), C.c_int(il), C.c_int(iu), C.c_int(0)
+    info = L.dspgeig(C.byref(it_), jobz.encode(), rng.encode(), uplo.encode(), C.byref(n_),
+                     AP.ctypes.data_as(_pd), BP.ctypes.data_as(_pd), C.byref(vl_), C.byref(vu_),
+                     C.byref(il_), C.byref(iu_), C.byref(m_), W.ctypes.data_as(_pd),
+                     Z.ctypes.data_as(_pd), C.byref(ldz_))
+    m = m_.value if info == 0 else 0
+    out = dict(info=info, m=m, W=W[:m].copy(), vl=vl_.value, vu=vu_.value, il=il_.value,
+               iu=iu_.value, BP=BP)
     if want_z:
         out["Z"] = Z[: ldz * m].reshape(m, ldz).T[:n].copy() if m > 0 else np.zeros((n, 0))
     return out

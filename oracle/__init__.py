@@ -90,6 +90,15 @@ def ref_lib() -> C.CDLL | None:
             L.dsyeig.restype = C.c_int
             L.dsyeig.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pi, _pd, _pd,
                                  _pi, _pi, _pi, _pd, _pd, _pi]
+            L.dspeig.restype = C.c_int
+            L.dspeig.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pd, _pd, _pi,
+                                 _pi, _pi, _pd, _pd, _pi]
+            L.dsygeig.restype = C.c_int
+            L.dsygeig.argtypes = [_pi, C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pi, _pd,
+                                  _pi, _pd, _pd, _pi, _pi, _pi, _pd]
+            L.dspgeig.restype = C.c_int
+            L.dspgeig.argtypes = [_pi, C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pd, _pd,
+                                  _pd, _pi, _pi, _pi, _pd, _pd, _pi]
         _libs["ref"] = L
     return _libs["ref"]
 
@@ -170,5 +179,74 @@ def ref_dsyeig(jobz, rng, uplo, A, vl=0.0, vu=0.0, il=1, iu=1, threads: int = 2)
     out = dict(info=info, m=m, W=W[:m].copy(), vl=vl_.value, vu=vu_.value, il=il_.value,
                iu=iu_.value)
     if want_z:
+        out["Z"] = Z[: n * m].reshape(m, n).T.copy() if m > 0 else np.zeros((n, 0))
+    return out
+
+
+def _ref(threads):
+    L = ref_lib()
+    if L is None:
+        raise RuntimeError("reference library not built (oracle/_ref)")
+    os.environ["PMR_NUM_THREADS"] = str(threads)
+    return L
+
+
+def ref_dspeig(jobz, rng, uplo, AP, n, vl=0.0, vu=0.0, il=1, iu=1, threads: int = 2):
+    """The reference's dspeig() (SRC/dense.c:319-398), A packed in AP."""
+    L = _ref(threads)
+    AP = np.array(AP, dtype=np.float64, copy=True)
+    W = np.zeros(max(n, 1))
+    Z = np.zeros(max(n, 1) * max(n, 1))   # back-transformed for every jobz
+    n_, ldz_ = C.c_int(n), C.c_int(n)
+    vl_, vu_, il_, iu_, m_ = C.c_double(vl), C.c_double(vu), C.c_int(il), C.c_int(iu), C.c_int(0)
+    info = L.dspeig(jobz.encode(), rng.encode(), uplo.encode(), C.byref(n_),
+                    AP.ctypes.data_as(_pd), C.byref(vl_), C.byref(vu_), C.byref(il_),
+                    C.byref(iu_), C.byref(m_), W.ctypes.data_as(_pd), Z.ctypes.data_as(_pd),
+                    C.byref(ldz_))
+    m = m_.value
+    out = dict(info=info, m=m, W=W[:m].copy())
+    if jobz[0] in "Vv":
+        out["Z"] = Z[: n * m].reshape(m, n).T.copy() if m > 0 else np.zeros((n, 0))
+    return out
+
+
+def ref_dsygeig(itype, jobz, rng, uplo, A, B, vl=0.0, vu=0.0, il=1, iu=1, threads: int = 2):
+    """The reference's dsygeig() (SRC/dense.c:236-313): eigenvectors in A."""
+    L = _ref(threads)
+    A = np.asarray(A, dtype=np.float64)
+    n = A.shape[0]
+    Af = np.array(A.T, dtype=np.float64, copy=True).reshape(-1)
+    Bf = np.array(np.asarray(B, dtype=np.float64).T, copy=True).reshape(-1)
+    W = np.zeros(max(n, 1))
+    it_, n_, lda_, ldb_ = C.c_int(itype), C.c_int(n), C.c_int(n), C.c_int(n)
+    vl_, vu_, il_, iu_, m_ = C.c_double(vl), C.c_double(vu), C.c_int(il), C.c_int(iu), C.c_int(0)
+    info = L.dsygeig(C.byref(it_), jobz.encode(), rng.encode(), uplo.encode(), C.byref(n_),
+                     Af.ctypes.data_as(_pd), C.byref(lda_), Bf.ctypes.data_as(_pd),
+                     C.byref(ldb_), C.byref(vl_), C.byref(vu_), C.byref(il_), C.byref(iu_),
+                     C.byref(m_), W.ctypes.data_as(_pd))
+    m = m_.value
+    out = dict(info=info, m=m, W=W[:m].copy())
+    if jobz[0] in "Vv":
+        out["Z"] = Af[: n * m].reshape(m, n).T.copy() if m > 0 else np.zeros((n, 0))
+    return out
+
+
+def ref_dspgeig(itype, jobz, rng, uplo, AP, BP, n, vl=0.0, vu=0.0, il=1, iu=1,
+                threads: int = 2):
+    """The reference's dspgeig() (SRC/dense.c:403-470)."""
+    L = _ref(threads)
+    AP = np.array(AP, dtype=np.float64, copy=True)
+    BP = np.array(BP, dtype=np.float64, copy=True)
+    W = np.zeros(max(n, 1))
+    Z = np.zeros(max(n, 1) * max(n, 1))
+    it_, n_, ldz_ = C.c_int(itype), C.c_int(n), C.c_int(n)
+    vl_, vu_, il_, iu_, m_ = C.c_double(vl), C.c_double(vu), C.c_int(il), C.c_int(iu), C.c_int(0)
+    info = L.dspgeig(C.byref(it_), jobz.encode(), rng.encode(), uplo.encode(), C.byref(n_),
+                     AP.ctypes.data_as(_pd), BP.ctypes.data_as(_pd), C.byref(vl_), C.byref(vu_),
+                     C.byref(il_), C.byref(iu_), C.byref(m_), W.ctypes.data_as(_pd),
+                     Z.ctypes.data_as(_pd), C.byref(ldz_))
+    m = m_.value
+    out = dict(info=info, m=m, W=W[:m].copy())
+    if jobz[0] in "Vv":
         out["Z"] = Z[: n * m].reshape(m, n).T.copy() if m > 0 else np.zeros((n, 0))
     return out

@@ -95,3 +95,109 @@ def test_dsyeig_argument_checks():
     assert r["info"] == 0 and r["m"] == 4
     r = M.dsyeig("C", "A", "L", A)
     assert r["info"] == 0 and r["m"] == 6
+
+
+# ---- packed and generalized drivers (SRC/dense.c:236-470) -----------------
+
+def _spd(n, seed):
+    rng = np.random.default_rng(seed)
+    Y = rng.standard_normal((n, n))
+    return np.eye(n) + 0.1 * (Y @ Y.T) / n
+
+
+def check_generalized(itype, A, B, r, w_all, idx, tol=50.0):
+    """Eigenvalues of the pencil (scipy) within tol*n*eps*max|lambda|; the
+    residual of the generalized equation and the B-orthogonality of the
+    vectors (X^T B X = I for itypes 1 and 2, X^T inv(B) X = I for itype 3)
+    within tol, in units of n*eps times the norms involved."""
+    n = A.shape[0]
+    assert r["info"] == 0 and r["m"] == len(idx), (r["info"], r["m"], len(idx))
+    W = r["W"]
+    lam = max(np.abs(w_all).max(), 1.0)
+    assert np.abs(W - w_all[idx]).max() <= tol * n * EPS * lam
+    if "Z" not in r or r["m"] == 0:
+        return
+    X = r["Z"]
+    nA, nB = np.abs(A).max() * n, np.abs(B).max() * n
+    if itype == 1:
+        R = A @ X - (B @ X) * W
+        scale = (nA + lam * nB) * np.abs(X).max()
+        G = X.T @ B @ X
+    elif itype == 2:
+        R = A @ (B @ X) - X * W
+        scale = (nA * nB + lam) * np.abs(X).max()
+        G = X.T @ B @ X
+    else:
+        R = B @ (A @ X) - X * W
+        scale = (nA * nB + lam) * np.abs(X).max()
+        G = X.T @ np.linalg.solve(B, X)
+    assert np.abs(R).max() / (n * EPS * scale) <= tol
+    assert np.abs(G - np.eye(r["m"])).max() / (n * EPS * np.linalg.cond(B)) <= tol
+
+
+@needs_ref
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("itype", [1, 2, 3])
+def test_reference_dsygeig(itype, uplo):
+    import scipy.linalg as sl
+    n = 70
+    A, B = _sym(n, 40 + itype), _spd(n, 50 + itype)
+    w = sl.eigh(A, B, type=itype, eigvals_only=True)
+    check_generalized(itype, A, B, oracle.ref_dsygeig(itype, "V", "A", uplo, A, B), w,
+                      np.arange(n))
+    check_generalized(itype, A, B, oracle.ref_dsygeig(itype, "V", "I", uplo, A, B, il=4, iu=30),
+                      w, np.arange(3, 30))
+
+
+@needs_ref
+@pytest.mark.parametrize("uplo", ["L", "U"])
+def test_reference_packed(uplo):
+    import scipy.linalg as sl
+    import mr3smp_b200 as M
+    n = 64
+    A, B = _sym(n, 61), _spd(n, 62)
+    w = np.linalg.eigvalsh(A)
+    _check(A, oracle.ref_dspeig("V", "A", uplo, M.pack(A, uplo), n), w, np.arange(n))
+    for itype in (1, 2, 3):
+        wg = sl.eigh(A, B, type=itype, eigvals_only=True)
+        r = oracle.ref_dspgeig(itype, "V", "A", uplo, M.pack(A, uplo), M.pack(B, uplo), n)
+        check_generalized(itype, A, B, r, wg, np.arange(n))
+
+
+def test_pack_layout():
+    """pack() follows LAPACK's packed storage: column j of the lower triangle
+    starts at j*n - j*(j-1)/2, of the upper triangle at j*(j+1)/2."""
+    import mr3smp_b200 as M
+    n = 5
+    A = np.arange(n * n, dtype=float).reshape(n, n)
+    L, U = M.pack(A, "L"), M.pack(A, "U")
+    for j in range(n):
+        for i in range(n):
+            if i >= j:
+                assert L[i + j * (2 * n - j - 1) // 2] == A[i, j]
+            if i <= j:
+                assert U[i + j * (j + 1) // 2] == A[i, j]
+
+
+def test_packed_generalized_argument_checks():
+    """The checks of SRC/dense.c:257-262, 340-347, 420-425 (and ldz, uplo,
+    range bounds) return 1 without touching the device."""
+    import mr3smp_b200 as M
+    n = 6
+    A, B = _sym(n, 1), _spd(n, 2)
+    AP, BP = M.pack(A, "L"), M.pack(B, "L")
+    assert M.dsygeig(0, "V", "A", "L", A, B)["info"] == 1
+    assert M.dsygeig(4, "V", "A", "L", A, B)["info"] == 1
+    assert M.dsygeig(1, "V", "A", "X", A, B)["info"] == 1
+    assert M.dsygeig(1, "X", "A", "L", A, B)["info"] == 1
+    assert M.dsygeig(1, "V", "I", "L", A, B, il=3, iu=2)["info"] == 1
+    assert M.dsygeig(1, "V", "A", "L", A[:1, :1], B[:1, :1])["info"] == 1   # n <= 1
+    assert M.dspeig("V", "X", "L", AP, n)["info"] == 1
+    assert M.dspeig("V", "A", "X", AP, n)["info"] == 1
+    assert M.dspeig("V", "A", "L", AP, n, ldz=n - 1)["info"] == 1
+    assert M.dspeig("V", "V", "L", AP, n, vl=2.0, vu=1.0)["info"] == 1
+    r = M.dspeig("C", "I", "L", AP, n, il=2, iu=4)
+    assert r["info"] == 0 and r["m"] == 3
+    assert M.dspgeig(0, "V", "A", "L", AP, BP, n)["info"] == 1
+    assert M.dspgeig(1, "V", "A", "L", AP, BP, 0)["info"] == 1
+    assert M.dspgeig(1, "V", "A", "L", AP, BP, n, ldz=n - 1)["info"] == 1

@@ -98,3 +98,74 @@ def test_dsyeig_clustered():
     A = 0.5 * (A + A.T)
     w = np.linalg.eigvalsh(A)
     _check(A, M.dsyeig("V", "A", "L", A), w, np.arange(n))
+
+
+# ---- packed and generalized drivers (SRC/dense.c:236-470) -----------------
+
+@pytest.mark.parametrize("uplo", ["L", "U"])
+def test_dspeig(uplo):
+    import mr3smp_b200 as M
+    n = 150
+    A = _sym(n, 31)
+    w = np.linalg.eigvalsh(A)
+    AP = M.pack(A, uplo)
+    _check(A, M.dspeig("V", "A", uplo, AP, n), w, np.arange(n))
+    _check(A, M.dspeig("V", "I", uplo, AP, n, il=20, iu=70, ldz=n + 2), w, np.arange(19, 70))
+    _check(A, M.dspeig("N", "A", uplo, AP, n), w, np.arange(n))
+    if _have_ref():
+        ref = oracle.ref_dspeig("V", "A", uplo, AP, n)
+        assert np.abs(ref["W"] - w).max() <= 10 * n * EPS * np.abs(w).max()
+
+
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("itype", [1, 2, 3])
+def test_dsygeig(itype, uplo):
+    import scipy.linalg as sl
+    import mr3smp_b200 as M
+    from test_dense_cpu import _spd, check_generalized
+    n = 120
+    A, B = _sym(n, 70 + itype), _spd(n, 80 + itype)
+    w = sl.eigh(A, B, type=itype, eigvals_only=True)
+    r = M.dsygeig(itype, "V", "A", uplo, A, B)
+    check_generalized(itype, A, B, r, w, np.arange(n))
+    # B comes back as its Cholesky factor (uplo triangle)
+    Lc = np.linalg.cholesky(B)
+    F = np.tril(r["B"]) if uplo == "L" else np.triu(r["B"])
+    G = Lc if uplo == "L" else Lc.T
+    assert np.abs(F - G).max() <= 100 * n * EPS * np.abs(B).max()
+    check_generalized(itype, A, B, M.dsygeig(itype, "V", "I", uplo, A, B, il=5, iu=40), w,
+                      np.arange(4, 40))
+    vl, vu = float(0.5 * (w[10] + w[11])), float(0.5 * (w[60] + w[61]))
+    check_generalized(itype, A, B, M.dsygeig(itype, "N", "V", uplo, A, B, vl=vl, vu=vu), w,
+                      np.arange(11, 61))
+    if _have_ref():
+        ref = oracle.ref_dsygeig(itype, "V", "A", uplo, A, B)
+        assert np.abs(ref["W"] - r["W"]).max() <= 50 * n * EPS * max(np.abs(w).max(), 1.0)
+
+
+@pytest.mark.parametrize("itype", [1, 2, 3])
+def test_dspgeig(itype):
+    import scipy.linalg as sl
+    import mr3smp_b200 as M
+    from test_dense_cpu import _spd, check_generalized
+    n = 90
+    A, B = _sym(n, 90 + itype), _spd(n, 95 + itype)
+    w = sl.eigh(A, B, type=itype, eigvals_only=True)
+    for uplo in "LU":
+        r = M.dspgeig(itype, "V", "A", uplo, M.pack(A, uplo), M.pack(B, uplo), n)
+        check_generalized(itype, A, B, r, w, np.arange(n))
+        Lc = np.linalg.cholesky(B)
+        assert np.abs(r["BP"] - M.pack(Lc if uplo == "L" else Lc.T, uplo)).max() <= \
+            100 * n * EPS * np.abs(B).max()
+    # n = 1 is allowed for the packed generalized driver
+    r = M.dspgeig(itype, "V", "A", "L", np.array([3.0]), np.array([4.0]), 1)
+    expect = {1: 0.75, 2: 12.0, 3: 12.0}[itype]
+    assert r["info"] == 0 and r["m"] == 1 and abs(r["W"][0] - expect) <= 4 * EPS * expect
+
+
+def test_dsygeig_not_definite():
+    """B that is not positive definite: return 2 (the reference asserts)."""
+    import mr3smp_b200 as M
+    n = 20
+    A, B = _sym(n, 1), -np.eye(n)
+    assert M.dsygeig(1, "V", "A", "L", A, B)["info"] == 2

@@ -99,6 +99,20 @@ def ref_lib() -> C.CDLL | None:
             L.dspgeig.restype = C.c_int
             L.dspgeig.argtypes = [_pi, C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pd, _pd,
                                   _pd, _pi, _pi, _pi, _pd, _pd, _pi]
+        if hasattr(L, "zheeig"):
+            # complex arrays are passed as interleaved (re, im) doubles
+            L.zheeig.restype = C.c_int
+            L.zheeig.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pi, _pd, _pd,
+                                 _pi, _pi, _pi, _pd, _pd, _pi]
+            L.zhpeig.restype = C.c_int
+            L.zhpeig.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pd, _pd, _pi,
+                                 _pi, _pi, _pd, _pd, _pi]
+            L.zhegeig.restype = C.c_int
+            L.zhegeig.argtypes = [_pi, C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pi, _pd,
+                                  _pi, _pd, _pd, _pi, _pi, _pi, _pd]
+            L.zhpgeig.restype = C.c_int
+            L.zhpgeig.argtypes = [_pi, C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pd, _pd,
+                                  _pd, _pi, _pi, _pi, _pd, _pd, _pi]
         _libs["ref"] = L
     return _libs["ref"]
 
@@ -249,4 +263,89 @@ def ref_dspgeig(itype, jobz, rng, uplo, AP, BP, n, vl=0.0, vu=0.0, il=1, iu=1,
     out = dict(info=info, m=m, W=W[:m].copy())
     if jobz[0] in "Vv":
         out["Z"] = Z[: n * m].reshape(m, n).T.copy() if m > 0 else np.zeros((n, 0))
+    return out
+
+
+def _cpd(a):
+    """A complex128 array's data as a double pointer (interleaved re, im)."""
+    return a.ctypes.data_as(_pd)
+
+
+def ref_zheeig(jobz, rng, uplo, A, vl=0.0, vu=0.0, il=1, iu=1, threads: int = 2):
+    """The reference's zheeig() (SRC/dense.c:568-671; built with its
+    COMPLEX_SUPPORTED switch): A is an (n, n) Hermitian array."""
+    L = _ref(threads)
+    A = np.asarray(A, dtype=np.complex128)
+    n = A.shape[0]
+    Af = np.array(A.T, dtype=np.complex128, copy=True).reshape(-1)
+    W = np.zeros(max(n, 1))
+    Z = np.zeros(max(n, 1) * max(n, 1), dtype=np.complex128)
+    n_, lda_, ldz_ = C.c_int(n), C.c_int(n), C.c_int(n)
+    vl_, vu_, il_, iu_, m_ = C.c_double(vl), C.c_double(vu), C.c_int(il), C.c_int(iu), C.c_int(0)
+    info = L.zheeig(jobz.encode(), rng.encode(), uplo.encode(), C.byref(n_), _cpd(Af),
+                    C.byref(lda_), C.byref(vl_), C.byref(vu_), C.byref(il_), C.byref(iu_),
+                    C.byref(m_), W.ctypes.data_as(_pd), _cpd(Z), C.byref(ldz_))
+    m = m_.value
+    out = dict(info=info, m=m, W=W[:m].copy())
+    if jobz[0] in "Vv":
+        out["Z"] = Z[: n * m].reshape(m, n).T.copy() if m > 0 else np.zeros((n, 0), complex)
+    return out
+
+
+def ref_zhpeig(jobz, rng, uplo, AP, n, vl=0.0, vu=0.0, il=1, iu=1, threads: int = 2):
+    """The reference's zhpeig() (packed Hermitian, SRC/dense.c:760-862)."""
+    L = _ref(threads)
+    AP = np.array(AP, dtype=np.complex128, copy=True)
+    W = np.zeros(max(n, 1))
+    Z = np.zeros(max(n, 1) * max(n, 1), dtype=np.complex128)
+    n_, ldz_ = C.c_int(n), C.c_int(n)
+    vl_, vu_, il_, iu_, m_ = C.c_double(vl), C.c_double(vu), C.c_int(il), C.c_int(iu), C.c_int(0)
+    info = L.zhpeig(jobz.encode(), rng.encode(), uplo.encode(), C.byref(n_), _cpd(AP),
+                    C.byref(vl_), C.byref(vu_), C.byref(il_), C.byref(iu_), C.byref(m_),
+                    W.ctypes.data_as(_pd), _cpd(Z), C.byref(ldz_))
+    m = m_.value
+    out = dict(info=info, m=m, W=W[:m].copy())
+    if jobz[0] in "Vv":
+        out["Z"] = Z[: n * m].reshape(m, n).T.copy() if m > 0 else np.zeros((n, 0), complex)
+    return out
+
+
+def ref_zhegeig(itype, jobz, rng, uplo, A, B, vl=0.0, vu=0.0, il=1, iu=1, threads: int = 2):
+    """The reference's zhegeig() (SRC/dense.c:676-754): eigenvectors in A."""
+    L = _ref(threads)
+    A = np.asarray(A, dtype=np.complex128)
+    n = A.shape[0]
+    Af = np.array(A.T, dtype=np.complex128, copy=True).reshape(-1)
+    Bf = np.array(np.asarray(B, dtype=np.complex128).T, copy=True).reshape(-1)
+    W = np.zeros(max(n, 1))
+    it_, n_, lda_, ldb_ = C.c_int(itype), C.c_int(n), C.c_int(n), C.c_int(n)
+    vl_, vu_, il_, iu_, m_ = C.c_double(vl), C.c_double(vu), C.c_int(il), C.c_int(iu), C.c_int(0)
+    info = L.zhegeig(C.byref(it_), jobz.encode(), rng.encode(), uplo.encode(), C.byref(n_),
+                     _cpd(Af), C.byref(lda_), _cpd(Bf), C.byref(ldb_), C.byref(vl_),
+                     C.byref(vu_), C.byref(il_), C.byref(iu_), C.byref(m_),
+                     W.ctypes.data_as(_pd))
+    m = m_.value
+    out = dict(info=info, m=m, W=W[:m].copy())
+    if jobz[0] in "Vv":
+        out["Z"] = Af[: n * m].reshape(m, n).T.copy() if m > 0 else np.zeros((n, 0), complex)
+    return out
+
+
+def ref_zhpgeig(itype, jobz, rng, uplo, AP, BP, n, vl=0.0, vu=0.0, il=1, iu=1,
+                threads: int = 2):
+    """The reference's zhpgeig() (packed generalized Hermitian, SRC/dense.c:869-936)."""
+    L = _ref(threads)
+    AP = np.array(AP, dtype=np.complex128, copy=True)
+    BP = np.array(BP, dtype=np.complex128, copy=True)
+    W = np.zeros(max(n, 1))
+    Z = np.zeros(max(n, 1) * max(n, 1), dtype=np.complex128)
+    it_, n_, ldz_ = C.c_int(itype), C.c_int(n), C.c_int(n)
+    vl_, vu_, il_, iu_, m_ = C.c_double(vl), C.c_double(vu), C.c_int(il), C.c_int(iu), C.c_int(0)
+    info = L.zhpgeig(C.byref(it_), jobz.encode(), rng.encode(), uplo.encode(), C.byref(n_),
+                     _cpd(AP), _cpd(BP), C.byref(vl_), C.byref(vu_), C.byref(il_),
+                     C.byref(iu_), C.byref(m_), W.ctypes.data_as(_pd), _cpd(Z), C.byref(ldz_))
+    m = m_.value
+    out = dict(info=info, m=m, W=W[:m].copy())
+    if jobz[0] in "Vv":
+        out["Z"] = Z[: n * m].reshape(m, n).T.copy() if m > 0 else np.zeros((n, 0), complex)
     return out

@@ -31,7 +31,7 @@ def _check(A, r, w_all, idx):
     if "Z" in r and r["m"] > 0:
         Z = r["Z"]
         resid = np.abs(A @ Z - Z * W).max() / (n * EPS * nrm)
-        orth = np.abs(Z.T @ Z - np.eye(r["m"])).max() / (n * EPS)
+        orth = np.abs(Z.conj().T @ Z - np.eye(r["m"])).max() / (n * EPS)
         assert resid <= 10 and orth <= 10, (resid, orth)
 
 
@@ -122,15 +122,15 @@ def check_generalized(itype, A, B, r, w_all, idx, tol=50.0):
     if itype == 1:
         R = A @ X - (B @ X) * W
         scale = (nA + lam * nB) * np.abs(X).max()
-        G = X.T @ B @ X
+        G = X.conj().T @ B @ X
     elif itype == 2:
         R = A @ (B @ X) - X * W
         scale = (nA * nB + lam) * np.abs(X).max()
-        G = X.T @ B @ X
+        G = X.conj().T @ B @ X
     else:
         R = B @ (A @ X) - X * W
         scale = (nA * nB + lam) * np.abs(X).max()
-        G = X.T @ np.linalg.solve(B, X)
+        G = X.conj().T @ np.linalg.solve(B, X)
     assert np.abs(R).max() / (n * EPS * scale) <= tol
     assert np.abs(G - np.eye(r["m"])).max() / (n * EPS * np.linalg.cond(B)) <= tol
 
@@ -201,3 +201,53 @@ def test_packed_generalized_argument_checks():
     assert M.dspgeig(0, "V", "A", "L", AP, BP, n)["info"] == 1
     assert M.dspgeig(1, "V", "A", "L", AP, BP, 0)["info"] == 1
     assert M.dspgeig(1, "V", "A", "L", AP, BP, n, ldz=n - 1)["info"] == 1
+
+
+# ---- complex Hermitian drivers (SRC/dense.c:568-936, COMPLEX_SUPPORTED) ----
+
+def _herm(n, seed, scale=1.0):
+    rng = np.random.default_rng(seed)
+    X = rng.uniform(-1, 1, (n, n)) + 1j * rng.uniform(-1, 1, (n, n))
+    return (X + X.conj().T) * (0.5 * scale)
+
+
+def _hpd(n, seed):
+    rng = np.random.default_rng(seed)
+    Y = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    return np.eye(n) + 0.1 * (Y @ Y.conj().T) / n
+
+
+def _cpack(A, uplo):
+    n = A.shape[0]
+    cols = [A[j:, j] for j in range(n)] if uplo == "L" else [A[: j + 1, j] for j in range(n)]
+    return np.concatenate(cols)
+
+
+needs_cref = pytest.mark.skipif(oracle.ref_lib() is None or not hasattr(oracle.ref_lib(), "zheeig"),
+                                reason="reference library (oracle/_ref) without complex drivers")
+
+
+@needs_cref
+@pytest.mark.parametrize("uplo", ["L", "U"])
+def test_reference_zheeig(uplo):
+    n = 64
+    A = _herm(n, 71)
+    w = np.linalg.eigvalsh(A)
+    _check(A, oracle.ref_zheeig("V", "A", uplo, A), w, np.arange(n))
+    _check(A, oracle.ref_zheeig("V", "I", uplo, A, il=3, iu=30), w, np.arange(2, 30))
+    _check(A, oracle.ref_zhpeig("V", "A", uplo, _cpack(A, uplo), n), w, np.arange(n))
+    _check(A * 1e-160, oracle.ref_zheeig("V", "A", uplo, A * 1e-160), w * 1e-160, np.arange(n))
+
+
+@needs_cref
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("itype", [1, 2, 3])
+def test_reference_zhegeig(itype, uplo):
+    import scipy.linalg as sl
+    n = 56
+    A, B = _herm(n, 80 + itype), _hpd(n, 90 + itype)
+    w = sl.eigh(A, B, type=itype, eigvals_only=True)
+    check_generalized(itype, A, B, oracle.ref_zhegeig(itype, "V", "A", uplo, A, B), w,
+                      np.arange(n))
+    r = oracle.ref_zhpgeig(itype, "V", "A", uplo, _cpack(A, uplo), _cpack(B, uplo), n)
+    check_generalized(itype, A, B, r, w, np.arange(n))

@@ -139,6 +139,44 @@ void dspgeig_(int *itype, char *jobz, char *range, char *uplo, int *n,
               int *iu, int *m, double *W, double *Z, int *ldz,
               int *info);   /* SRC/dense.c:1065-1072 */
 
+/* The complex Hermitian drivers, which the reference compiles only with its
+ * COMPLEX_SUPPORTED switch.  Complex arrays (A, B, AP, BP, Z) are
+ * column-major with interleaved (re, im) doubles -- the layout of C99
+ * double complex -- and are passed as void * so that C and C++ callers
+ * can hand in double complex or std::complex<double> arrays alike; W, vl
+ * and vu are real.  Arguments, outputs and returns are those of the real
+ * drivers above, with conjugate transposes in place of transposes:
+ *   zheeig  replaces INCLUDE/mrrr.h:538-541 (SRC/dense.c:568-671);
+ *   zhegeig replaces INCLUDE/mrrr.h:624-627 (SRC/dense.c:676-754);
+ *   zhpeig  replaces INCLUDE/mrrr.h:718-721 (SRC/dense.c:760-862);
+ *   zhpgeig replaces INCLUDE/mrrr.h:802-805 (SRC/dense.c:869-936);
+ * and the _ bindings replace SRC/dense.c:1076-1113.  zhegeig and zhpgeig
+ * refuse n <= 1, as the reference does. */
+int zheeig(char *jobz, char *range, char *uplo, int *n, void *A, int *lda,
+           double *vl, double *vu, int *il, int *iu, int *m, double *W,
+           void *Z, int *ldz);
+int zhegeig(int *itype, char *jobz, char *range, char *uplo, int *n,
+            void *A, int *lda, void *B, int *ldb, double *vl, double *vu,
+            int *il, int *iu, int *m, double *W);
+int zhpeig(char *jobz, char *range, char *uplo, int *n, void *AP,
+           double *vl, double *vu, int *il, int *iu, int *m, double *W,
+           void *Z, int *ldz);
+int zhpgeig(int *itype, char *jobz, char *range, char *uplo, int *n,
+            void *AP, void *BP, double *vl, double *vu, int *il, int *iu,
+            int *m, double *W, void *Z, int *ldz);
+void zheeig_(char *jobz, char *range, char *uplo, int *n, void *A, int *lda,
+             double *vl, double *vu, int *il, int *iu, int *m, double *W,
+             void *Z, int *ldz, int *info);
+void zhegeig_(int *itype, char *jobz, char *range, char *uplo, int *n,
+              void *A, int *lda, void *B, int *ldb, double *vl, double *vu,
+              int *il, int *iu, int *m, double *W, int *info);
+void zhpeig_(char *jobz, char *range, char *uplo, int *n, void *AP,
+             double *vl, double *vu, int *il, int *iu, int *m, double *W,
+             void *Z, int *ldz, int *info);
+void zhpgeig_(int *itype, char *jobz, char *range, char *uplo, int *n,
+              void *AP, void *BP, double *vl, double *vu, int *il, int *iu,
+              int *m, double *W, void *Z, int *ldz, int *info);
+
 /* Kernels launched by the calling thread's last solve (diagnostics). */
 long long mr3_last_launches(void);
 

@@ -75,6 +75,19 @@ def lib() -> C.CDLL:
         L.dspgeig.restype = C.c_int
         L.dspgeig.argtypes = [_pi, C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pd, _pd, _pd,
                               _pi, _pi, _pi, _pd, _pd, _pi]
+        # complex drivers: complex arrays as interleaved (re, im) doubles
+        L.zheeig.restype = C.c_int
+        L.zheeig.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pi, _pd, _pd, _pi,
+                             _pi, _pi, _pd, _pd, _pi]
+        L.zhpeig.restype = C.c_int
+        L.zhpeig.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pd, _pd, _pi, _pi,
+                             _pi, _pd, _pd, _pi]
+        L.zhegeig.restype = C.c_int
+        L.zhegeig.argtypes = [_pi, C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pi, _pd, _pi,
+                              _pd, _pd, _pi, _pi, _pi, _pd]
+        L.zhpgeig.restype = C.c_int
+        L.zhpgeig.argtypes = [_pi, C.c_char_p, C.c_char_p, C.c_char_p, _pi, _pd, _pd, _pd, _pd,
+                              _pi, _pi, _pi, _pd, _pd, _pi]
         L.mr3_last_launches.restype = C.c_longlong
         L.mr3_last_error.restype = C.c_char_p
         _lib = L
@@ -245,6 +258,107 @@ def dspgeig(itype: int, jobz: str, rng: str, uplo: str, AP, BP, n: int, vl: floa
                iu=iu_.value, BP=BP)
     if want_z:
         out["Z"] = Z[: ldz * m].reshape(m, ldz).T[:n].copy() if m > 0 else np.zeros((n, 0))
+    return out
+
+
+def _zcols(jobz, rng, n, il, iu, ldz):
+    return np.zeros(_ncols(jobz, rng, n, il, iu) * (ldz if jobz[0] in "Vv" else 1),
+                    dtype=np.complex128)
+
+
+def _zout(info, m_, W, vl_, vu_, il_, iu_):
+    m = m_.value if info == 0 else 0
+    return m, dict(info=info, m=m, W=W[:m].copy(), vl=vl_.value, vu=vu_.value, il=il_.value,
+                   iu=iu_.value)
+
+
+def zheeig(jobz: str, rng: str, uplo: str, A, vl: float = 0.0, vu: float = 0.0, il: int = 1,
+           iu: int = 1, lda: int | None = None, ldz: int | None = None) -> dict:
+    """``zheeig()``: eigenpairs of a dense Hermitian matrix (``A`` complex
+    (n, n), the ``uplo`` triangle read); ``Z`` (n, m) complex for jobz "V"."""
+    L = lib()
+    A = np.asarray(A, dtype=np.complex128)
+    n = int(A.shape[0])
+    lda = n if lda is None else int(lda)
+    Ah = np.zeros(lda * max(n, 1), dtype=np.complex128)
+    if n > 0 and lda > 0:
+        r = min(n, lda)
+        Ah.reshape(n, lda)[:, :r] = A.T[:, :r]
+    ldz = n if ldz is None else int(ldz)
+    W, Z = np.zeros(max(n, 1)), _zcols(jobz, rng, n, il, iu, ldz)
+    n_, lda_, ldz_ = C.c_int(n), C.c_int(lda), C.c_int(ldz)
+    vl_, vu_, il_, iu_, m_ = C.c_double(vl), C.c_double(vu), C.c_int(il), C.c_int(iu), C.c_int(0)
+    info = L.zheeig(jobz.encode(), rng.encode(), uplo.encode(), C.byref(n_),
+                    Ah.ctypes.data_as(_pd), C.byref(lda_), C.byref(vl_), C.byref(vu_),
+                    C.byref(il_), C.byref(iu_), C.byref(m_), W.ctypes.data_as(_pd),
+                    Z.ctypes.data_as(_pd), C.byref(ldz_))
+    m, out = _zout(info, m_, W, vl_, vu_, il_, iu_)
+    if jobz[0] in "Vv":
+        out["Z"] = Z[: ldz * m].reshape(m, ldz).T[:n].copy() if m > 0 else np.zeros((n, 0), complex)
+    return out
+
+
+def zhpeig(jobz: str, rng: str, uplo: str, AP, n: int, vl: float = 0.0, vu: float = 0.0,
+           il: int = 1, iu: int = 1, ldz: int | None = None) -> dict:
+    """``zhpeig()``: zheeig with A in packed storage (see :func:`pack`)."""
+    L = lib()
+    AP = np.array(AP, dtype=np.complex128, copy=True)
+    ldz = n if ldz is None else int(ldz)
+    W, Z = np.zeros(max(n, 1)), _zcols(jobz, rng, n, il, iu, ldz)
+    n_, ldz_ = C.c_int(n), C.c_int(ldz)
+    vl_, vu_, il_, iu_, m_ = C.c_double(vl), C.c_double(vu), C.c_int(il), C.c_int(iu), C.c_int(0)
+    info = L.zhpeig(jobz.encode(), rng.encode(), uplo.encode(), C.byref(n_),
+                    AP.ctypes.data_as(_pd), C.byref(vl_), C.byref(vu_), C.byref(il_),
+                    C.byref(iu_), C.byref(m_), W.ctypes.data_as(_pd), Z.ctypes.data_as(_pd),
+                    C.byref(ldz_))
+    m, out = _zout(info, m_, W, vl_, vu_, il_, iu_)
+    if jobz[0] in "Vv":
+        out["Z"] = Z[: ldz * m].reshape(m, ldz).T[:n].copy() if m > 0 else np.zeros((n, 0), complex)
+    return out
+
+
+def zhegeig(itype: int, jobz: str, rng: str, uplo: str, A, B, vl: float = 0.0, vu: float = 0.0,
+            il: int = 1, iu: int = 1) -> dict:
+    """``zhegeig()``: the generalized Hermitian-definite problem; eigenvectors
+    ``Z`` (returned in A by the library) and ``B`` (its Cholesky factor)."""
+    L = lib()
+    A = np.asarray(A, dtype=np.complex128)
+    n = int(A.shape[0])
+    Af = np.array(A.T, dtype=np.complex128, copy=True).reshape(-1)
+    Bf = np.array(np.asarray(B, dtype=np.complex128).T, copy=True).reshape(-1)
+    W = np.zeros(max(n, 1))
+    it_, n_, lda_, ldb_ = C.c_int(itype), C.c_int(n), C.c_int(n), C.c_int(n)
+    vl_, vu_, il_, iu_, m_ = C.c_double(vl), C.c_double(vu), C.c_int(il), C.c_int(iu), C.c_int(0)
+    info = L.zhegeig(C.byref(it_), jobz.encode(), rng.encode(), uplo.encode(), C.byref(n_),
+                     Af.ctypes.data_as(_pd), C.byref(lda_), Bf.ctypes.data_as(_pd),
+                     C.byref(ldb_), C.byref(vl_), C.byref(vu_), C.byref(il_), C.byref(iu_),
+                     C.byref(m_), W.ctypes.data_as(_pd))
+    m, out = _zout(info, m_, W, vl_, vu_, il_, iu_)
+    out["B"] = Bf.reshape(max(n, 1), n).T.copy() if n else Bf
+    if jobz[0] in "Vv":
+        out["Z"] = Af[: n * m].reshape(m, n).T.copy() if m > 0 else np.zeros((n, 0), complex)
+    return out
+
+
+def zhpgeig(itype: int, jobz: str, rng: str, uplo: str, AP, BP, n: int, vl: float = 0.0,
+            vu: float = 0.0, il: int = 1, iu: int = 1, ldz: int | None = None) -> dict:
+    """``zhpgeig()``: zhegeig with A and B packed; ``BP`` returns the packed
+    Cholesky factor."""
+    L = lib()
+    AP = np.array(AP, dtype=np.complex128, copy=True)
+    BP = np.array(BP, dtype=np.complex128, copy=True)
+    ldz = n if ldz is None else int(ldz)
+    W, Z = np.zeros(max(n, 1)), _zcols(jobz, rng, n, il, iu, ldz)
+    it_, n_, ldz_ = C.c_int(itype), C.c_int(n), C.c_int(ldz)
+    vl_, vu_, il_, iu_, m_ = C.c_double(vl), C.c_double(vu), C.c_int(il), C.c_int(iu), C.c_int(0)
+    info = L.zhpgeig(C.byref(it_), jobz.encode(), rng.encode(), uplo.encode(), C.byref(n_),
+                     AP.ctypes.data_as(_pd), BP.ctypes.data_as(_pd), C.byref(vl_), C.byref(vu_),
+                     C.byref(il_), C.byref(iu_), C.byref(m_), W.ctypes.data_as(_pd),
+                     Z.ctypes.data_as(_pd), C.byref(ldz_))
+    m, out = _zout(info, m_, W, vl_, vu_, il_, iu_)
+    out["BP"] = BP
+    if jobz[0] in "Vv":
+        out["Z"] = Z[: ldz * m].reshape(m, ldz).T[:n].copy() if m > 0 else np.zeros((n, 0), complex)
     return out
 
 

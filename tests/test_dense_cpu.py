@@ -251,3 +251,30 @@ def test_reference_zhegeig(itype, uplo):
                       np.arange(n))
     r = oracle.ref_zhpgeig(itype, "V", "A", uplo, _cpack(A, uplo), _cpack(B, uplo), n)
     check_generalized(itype, A, B, r, w, np.arange(n))
+
+
+def test_complex_argument_checks():
+    """The complex drivers' argument checks (SRC/dense.c:596-602, 697-701,
+    788-796, 888-892, plus lda, ldb, ldz, uplo) return 1 without touching the
+    device."""
+    import mr3smp_b200 as M
+    n = 5
+    A, B = _herm(n, 1), _hpd(n, 2)
+    AP, BP = _cpack(A, "L"), _cpack(B, "L")
+    assert M.zheeig("X", "A", "L", A)["info"] == 1
+    assert M.zheeig("V", "A", "X", A)["info"] == 1
+    assert M.zheeig("V", "I", "L", A, il=2, iu=9)["info"] == 1
+    assert M.zheeig("V", "A", "L", A, lda=4)["info"] == 1
+    assert M.zheeig("V", "A", "L", A, ldz=4)["info"] == 1
+    r = M.zheeig("C", "I", "U", A, il=2, iu=4)
+    assert r["info"] == 0 and r["m"] == 3
+    assert M.zhpeig("V", "V", "L", AP, n, vl=1.0, vu=0.0)["info"] == 1
+    assert M.zhpeig("V", "A", "L", AP, n, ldz=4)["info"] == 1
+    r = M.zhpeig("C", "A", "L", AP, n)
+    assert r["info"] == 0 and r["m"] == n
+    assert M.zhegeig(0, "V", "A", "L", A, B)["info"] == 1
+    assert M.zhegeig(1, "V", "A", "L", A[:1, :1], B[:1, :1])["info"] == 1
+    assert M.zhegeig(1, "V", "X", "L", A, B)["info"] == 1
+    assert M.zhpgeig(4, "V", "A", "L", AP, BP, n)["info"] == 1
+    assert M.zhpgeig(1, "V", "A", "L", AP[:1], BP[:1], 1)["info"] == 1
+    assert M.zhpgeig(1, "V", "A", "L", AP, BP, n, ldz=4)["info"] == 1

@@ -1,7 +1,8 @@
 /*
  * mr3_b200.h -- public C ABI of the B200 MRRR tridiagonal eigensolver.
  *
- * Drop-in replacement for the tridiagonal entry points of MR3-SMP.  All
+ * Drop-in replacement for the entry points of MR3-SMP: the tridiagonal
+ * solver mrrr() and the dense drivers of SRC/dense.c built on it.  All
  * arguments keep the reference's meaning; host pointers throughout.
  */
 #ifndef MR3_B200_H

@@ -121,14 +121,51 @@ def _clocks_stop(proc, path):
 # --------------------------------------------------------------------------
 # CPU baseline: the reference's own mrrr() on a bounded sample
 # --------------------------------------------------------------------------
-def cpu_reference(problems, budget_s: float, check: bool = True):
+def host_cores():
+    """(physical cores, logical CPUs) of this host."""
+    logical = os.cpu_count() or 1
+    try:
+        import psutil
+        phys = psutil.cpu_count(logical=False) or logical
+    except Exception:
+        phys = logical
+    return int(phys), int(logical)
+
+
+def check_host_result(D, E, r, rng):
+    """Scaled residual and orthogonality of one host result (numpy): the
+    residual over every column; the orthogonality of every column pair for
+    n <= 1024, else of 64 random columns against all columns."""
+    n = len(D)
+    eps = np.finfo(np.float64).eps
+    W, Z = r["W"], r["Z"]
+    m = Z.shape[1]
+    if m == 0:
+        return 0.0, 0.0
+    e = np.asarray(E[: n - 1], dtype=np.float64)
+    tn = max(np.abs(D).max(), np.abs(e).max() if n > 1 else 0.0) or 1.0
+    TZ = D[:, None] * Z
+    TZ[:-1] += e[:, None] * Z[1:]
+    TZ[1:] += e[:, None] * Z[:-1]
+    res = np.abs(TZ - Z * W[None, :]).max() / (n * eps * tn)
+    cols = np.arange(m) if n <= 1024 else np.sort(rng.choice(m, size=min(64, m), replace=False))
+    G = Z.T @ Z[:, cols]
+    G[cols, np.arange(len(cols))] -= 1.0
+    return float(res), float(np.abs(G).max() / (n * eps))
+
+
+def cpu_reference(problems, budget_s: float):
     """Time the reference mrrr() (oracle/_ref) problem by problem on a
-    stratified sample whose predicted cost is about budget_s seconds.
+    stratified sample whose predicted cost is about budget_s seconds, with
+    PMR_NUM_THREADS = the physical cores.  Every result is checked outside
+    the timed calls (the reference's asserts are compiled out): a problem
+    with info != 0, a wrong count, or residual or orthogonality above 10
+    (units n eps ||T||, n eps) is a failure and its eigenpairs do not count.
     Returns (eigenpairs/s, dict)."""
     import oracle
     if oracle.ref_lib() is None:
         return None, {"unavailable": "reference library oracle/_ref not built"}
-    cores = os.cpu_count() or 1
+    cores, logical = host_cores()
     os.environ["PMR_NUM_THREADS"] = str(cores)
     os.environ["OPENBLAS_NUM_THREADS"] = "1"
     ns = [len(D) for D, E in problems]
@@ -142,118 +179,250 @@ def cpu_reference(problems, budget_s: float, check: bool = True):
     total = float(sum(n * n for n in ns))
     count = int(max(8, min(len(ns), round(len(ns) * want / total))))
     sample = _stratified(ns, count)
-    t0 = time.perf_counter()
-    pairs, bad = 0, 0
+    rng = np.random.default_rng(0)
+    el, pairs, bad, worst = 0.0, 0, 0, 0.0
     for i in sample:
         D, E = problems[i]
+        t0 = time.perf_counter()
         r = oracle.ref_mrrr("V", "A", D, E, threads=cores)
-        pairs += r["m"]
-        if r["info"] != 0 or r["m"] != len(D):
-            bad += 1
-    el = time.perf_counter() - t0
-    # the reference is checked, not trusted (its asserts are compiled out):
-    # residuals of the sampled results, outside the timed region
-    from mr3smp_b200.workloads import residual_orth
-    worst = 0.0
-    for i in (sample[: min(len(sample), 64)] if check else []):
-        D, E = problems[i]
-        r = oracle.ref_mrrr("V", "A", D, E, threads=cores)
-        if len(D) <= 1500:
-            res, orth = residual_orth(D, E, r["W"], r["Z"])
+        el += time.perf_counter() - t0
+        ok = r["info"] == 0 and r["m"] == len(D)
+        if ok:
+            res, orth = check_host_result(D, E, r, rng)
             worst = max(worst, res, orth)
-            bad += int(res > 10 or orth > 10)
-    info = {"value": pairs / el, "unit": "eigenpairs/s", "cores": cores, "kind": "reference",
+            ok = res <= 10.0 and orth <= 10.0
+        if ok:
+            pairs += r["m"]
+        else:
+            bad += 1
+    info = {"value": pairs / el, "unit": "eigenpairs/s", "cores": cores, "logical_cpus": logical,
+            "kind": "reference",
             "sample": f"{len(sample)} of {len(ns)} problems stratified by n "
-                      f"({pairs} eigenpairs, {el:.1f} s), PMR_NUM_THREADS={cores}",
-            "checked_bad": bad, "checked_worst_resid_orth": worst}
+                      f"({pairs} checked eigenpairs, {el:.1f} s in mrrr()), "
+                      f"PMR_NUM_THREADS={cores} (physical cores), OPENBLAS_NUM_THREADS=1",
+            "mrrr_seconds": el, "checked": True, "checked_problems": len(sample), "checked_bad": bad,
+            "checked_worst_resid_orth": worst,
+            "check": "every sampled result: info, count, residual; orthogonality of all "
+                     "columns (n <= 1024) or 64 random columns (larger n); failures excluded"}
     return pairs / el, info
+
+
+def check_batch(recs, T, ns):
+    """Checks every problem of a device batch in place on the device: info,
+    count, ascending W, scaled residual max|T z - lambda z|/(n eps ||T||) and
+    orthogonality max|Z^T Z - I|/(n eps), both <= 10.  Returns a summary with
+    the eigenpairs of the problems that passed (pairs_ok)."""
+    import torch
+    eps = float(np.finfo(np.float64).eps)
+    offs, zoffs = T["offs"], T["zoffs"]
+    bad, worst, pairs_ok = 0, 0.0, 0
+    for k, n in enumerate(ns):
+        q = recs[k]
+        ok = q.info == 0 and q.m == n
+        if ok:
+            d = T["D0"][offs[k]:offs[k] + n]
+            e = T["E0"][offs[k]:offs[k] + n - 1]
+            w = T["W"][offs[k]:offs[k] + n]
+            Z = T["Z"][zoffs[k]:zoffs[k] + n * n].view(n, n).T
+            tn = max(float(d.abs().max()), float(e.abs().max()) if n > 1 else 0.0) or 1.0
+            TZ = d[:, None] * Z
+            if n > 1:
+                TZ[:-1] += e[:, None] * Z[1:]
+                TZ[1:] += e[:, None] * Z[:-1]
+            res = float((TZ - Z * w[None, :]).abs().max()) / (n * eps * tn)
+            G = Z.T @ Z
+            G.diagonal().sub_(1.0)
+            orth = float(G.abs().max()) / (n * eps)
+            asc = bool((w[1:] >= w[:-1]).all()) if n > 1 else True
+            worst = max(worst, res, orth)
+            ok = asc and res <= 10.0 and orth <= 10.0
+        if ok:
+            pairs_ok += n
+        else:
+            bad += 1
+    return {"checked": True, "checked_problems": len(ns), "checked_bad": bad,
+            "checked_worst_resid_orth": worst, "pairs_ok": pairs_ok,
+            "how": "every problem on the device: info, m = n, ascending W, residual and "
+                   "orthogonality <= 10 (units n eps ||T||, n eps); failures count no eigenpairs"}
 
 
 SERVE_SIZES = (64, 256, 1024, 4096, 16384)
 SERVE_PROBS = (0.4, 0.3, 0.2, 0.08, 0.02)
 
 
-def run_serving(M, wl, rate: float, count: int, seed: int):
-    """Poisson stream of independent requests through the serving API.
+class _ZPool:
+    """Device buffers for the eigenvectors of in-flight serving requests,
+    recycled by size, with the bytes held (in flight or idle) kept within
+    the device budget: a request whose Z does not fit waits until finished
+    requests give theirs back (admission by device memory)."""
+
+    def __init__(self, budget):
+        import threading
+        self.budget, self.held = budget, 0
+        self.free = {}
+        self.cv = threading.Condition()
+
+    def get(self, size):
+        import torch
+        with self.cv:
+            while True:
+                lst = self.free.get(size)
+                if lst:
+                    return lst.pop()
+                if self.held + 8 * size <= self.budget:
+                    self.held += 8 * size
+                    break
+                # drop idle buffers of other sizes before waiting
+                dropped = False
+                for k, v in self.free.items():
+                    while v and self.held + 8 * size > self.budget:
+                        v.pop()
+                        self.held -= 8 * k
+                        dropped = True
+                if dropped and self.held + 8 * size <= self.budget:
+                    self.held += 8 * size
+                    break
+                self.cv.wait()
+        return torch.empty(max(size, 1), dtype=torch.float64, device="cuda")
+
+    def put(self, size, buf):
+        with self.cv:
+            self.free.setdefault(size, []).append(buf)
+            self.cv.notify_all()
+
+
+def run_serving(M, wl, rates, count: int, seed: int, budget: int):
+    """The serving configuration: Poisson streams of independent requests
+    through the serving API with continuous batching, one stream per rate.
 
     Sizes n in SERVE_SIZES with SERVE_PROBS, D, E ~ U(-1,1), range
-    alternating A and I (il = 1, iu = ceil(n/10)), results to host memory.
-    Latency = arrival to result ready (queueing in the client included)."""
+    alternating A and I (il = 1, iu = ceil(n/10)), jobz V.  Requests are
+    device requests: D, E staged in device memory beforehand (as they would
+    arrive from an earlier device step), W, Z, Zsupp written in device
+    memory and kept there -- the eigenvectors held by requests in flight stay
+    within the device budget, a request waiting for admission until they
+    fit.  Latency = scheduled arrival to result ready (client queueing and
+    admission waits included).  Returns one record per rate."""
     import threading
+    import torch
     rng = np.random.default_rng(seed)
-    ns = rng.choice(SERVE_SIZES, size=count, p=SERVE_PROBS)
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=count))
-    reqs = []
+    ns = rng.choice(SERVE_SIZES, size=count, p=SERVE_PROBS).astype(int)
+    rng_i = np.arange(count) % 2 == 1
+    cols = np.where(rng_i, -(-ns // 10), ns)
+    offs = np.concatenate([[0], np.cumsum(ns)]).astype(np.int64)
+    D0 = np.empty(int(offs[-1]))
+    E0 = np.empty(int(offs[-1]))
     for k, n in enumerate(ns):
-        D, E = wl.uniform(int(n), seed=seed * 100003 + k)
-        if k % 2 == 0:
-            reqs.append(dict(jobz="V", range="A", D=D, E=E))
-        else:
-            reqs.append(dict(jobz="V", range="I", D=D, E=E, il=1, iu=-(-int(n) // 10)))
-    S = M.Server(pinned=True)
-    # page-locked result buffers, recycled per request shape
-    pool = {}
-    plock = threading.Lock()
+        d, e = wl.uniform(int(n), seed=seed * 100003 + k)
+        D0[offs[k]:offs[k + 1]] = d
+        E0[offs[k]:offs[k + 1]] = e
+    D0t = torch.from_numpy(D0).cuda()
+    E0t = torch.from_numpy(E0).cuda()
+    Dt, Et = torch.empty_like(D0t), torch.empty_like(E0t)
+    Wt = torch.empty_like(D0t)
+    St = torch.empty(2 * int(offs[-1]), dtype=torch.int32, device="cuda")
+    pool = _ZPool(budget)
+    pairs = (cols).astype(np.int64)
+    out = []
+    S = M.Server(budget_bytes=budget)
+    try:
+        # warm-up: every lane's workspaces at the largest sizes
+        for n in SERVE_SIZES:
+            D, E = wl.uniform(int(n), seed=1)
+            for rg in ("A", "I"):
+                c = n if rg == "A" else -(-n // 10)
+                z = pool.get(n * c)
+                d = dict(jobz="V", range=rg, il=1, iu=c,
+                         D=torch.tensor(D, device="cuda"), E=torch.tensor(E, device="cuda"),
+                         W=torch.empty(n, dtype=torch.float64, device="cuda"), Z=z,
+                         Zsupp=torch.empty(2 * n, dtype=torch.int32, device="cuda"))
+                ts = [S.submit_device(d) for _ in range(4)]
+                for t in ts:
+                    S.poll(t, wait=True)
+                pool.put(n * c, z)
+        for rate in rates:
+            Dt.copy_(D0t)
+            Et.copy_(E0t)
+            torch.cuda.synchronize()
+            arrivals = np.cumsum(np.random.default_rng(seed + int(rate)).exponential(1.0 / rate,
+                                                                                   size=count))
+            reqs = []
+            for k in range(count):
+                n, o = int(ns[k]), int(offs[k])
+                q = M.CudaProb()
+                q.n, q.jobz, q.range = n, 1, (3 if rng_i[k] else 1)
+                q.il, q.iu, q.tryrac, q.ldz = 1, int(cols[k]), 0, n
+                q.D = Dt.data_ptr() + 8 * o
+                q.E = Et.data_ptr() + 8 * o
+                q.W = Wt.data_ptr() + 8 * o
+                q.Zsupp = St.data_ptr() + 8 * o
+                reqs.append(q)
+            b0 = S.stats()
+            sub = [None] * count
+            zbuf = [None] * count
+            lat = np.zeros(count)
+            qwait = np.zeros(count)
+            done_t = np.zeros(count)
+            bad = [0]
+            ready = threading.Semaphore(0)
 
-    def shape(p):
-        return (len(p["D"]), p["range"], p.get("iu", 0))
+            def poller():
+                for k in range(count):
+                    ready.acquire()
+                    t, t_arr, t_sub = sub[k]
+                    (info, m, _), l = S.poll(t, wait=True, raw=True)
+                    done_t[k] = time.perf_counter()
+                    lat[k] = (t_sub - t_arr) * 1e3 + l
+                    tq = S.timing(t)
+                    qwait[k] = (t_sub - t_arr) * 1e3 + (tq[0] if tq else 0.0)
+                    if info != 0 or m != cols[k]:
+                        bad[0] += 1
+                    pool.put(int(ns[k] * cols[k]), zbuf[k])
+                    zbuf[k] = None
 
-    for n in SERVE_SIZES:   # warm-up: workspaces of both workers, one buffer set each
-        D, E = wl.uniform(n, seed=1)
-        for p in (dict(jobz="V", range="A", D=D, E=E),
-                  dict(jobz="V", range="I", D=D, E=E, il=1, iu=-(-n // 10))):
-            (info, m, arr), _ = S.poll(S.submit(p), wait=True, raw=True)
-            pool.setdefault(shape(p), []).append(arr)
-    lat = [None] * count
-    pairs = [0] * count
-    sub = [None] * count
-    done_t = [0.0] * count
-    ready = threading.Semaphore(0)
-
-    def poller():
-        for k in range(count):
-            ready.acquire()
-            t, t_arr, t_sub = sub[k]
-            (info, m, arr), l = S.poll(t, wait=True, raw=True)
-            done_t[k] = time.perf_counter()
-            lat[k] = (t_sub - t_arr) * 1e3 + l
-            pairs[k] = m if info == 0 else 0
-            with plock:
-                pool.setdefault(shape(reqs[k]), []).append(arr)
-
-    th = threading.Thread(target=poller)
-    th.start()
-    t0 = time.perf_counter()
-    for k in range(count):
-        ta = t0 + arrivals[k]
-        d = ta - time.perf_counter()
-        if d > 0:
-            time.sleep(d)
-        with plock:
-            free = pool.get(shape(reqs[k]))
-            arr = free.pop() if free else None
-        ts = time.perf_counter()
-        sub[k] = (S.submit(reqs[k], arr), ta, ts)
-        ready.release()
-    th.join()
-    st = S.stats()
-    S.close()
-    el = max(done_t) - t0
-    lat_a = np.array(lat)
-    by_n = {}
-    for n in SERVE_SIZES:
-        sel = lat_a[ns == n]
-        if len(sel):
-            by_n[str(n)] = {"count": int(len(sel)), "p50_ms": float(np.percentile(sel, 50)),
-                            "p99_ms": float(np.percentile(sel, 99))}
-    return {"rate_per_s": rate, "requests": count, "p50_ms": float(np.percentile(lat_a, 50)),
-            "p99_ms": float(np.percentile(lat_a, 99)), "mean_ms": float(lat_a.mean()),
-            "by_n": by_n,
-            "eigenpairs_per_s": float(sum(pairs) / el), "requests_per_s": count / el,
-            "batches": st["batches"],
+            th = threading.Thread(target=poller)
+            th.start()
+            t0 = time.perf_counter()
+            for k in range(count):
+                ta = t0 + arrivals[k]
+                d = ta - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                z = pool.get(int(ns[k] * cols[k]))   # waits while the budget is full
+                zbuf[k] = z
+                reqs[k].Z = z.data_ptr()
+                ts = time.perf_counter()
+                sub[k] = (S.submit_device(None, req=reqs[k]), ta, ts)
+                ready.release()
+            th.join()
+            el = float(done_t.max() - t0)
+            b1 = S.stats()
+            by_n = {}
+            for n in SERVE_SIZES:
+                sel = lat[ns == n]
+                if len(sel):
+                    by_n[str(n)] = {"count": int(len(sel)),
+                                    "p50_ms": round(float(np.percentile(sel, 50)), 3),
+                                    "p99_ms": round(float(np.percentile(sel, 99)), 3)}
+            nb = b1["batches"] - b0["batches"]
+            out.append({"rate_per_s": rate, "requests": count,
+                        "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                        "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                        "queue_p50_ms": round(float(np.percentile(qwait, 50)), 3),
+                        "eigenpairs_per_s": float(pairs.sum() / el),
+                        "requests_per_s": count / el, "failed": bad[0],
+                        "batches": nb, "requests_per_batch": round(count / max(nb, 1), 2),
+                        "batches_overlapping_others": b1["batches_overlapping_others"]
+                        - b0["batches_overlapping_others"],
+                        "by_n": by_n})
+        lanes = S.stats()["lanes"]
+    finally:
+        S.close()
+    return {"streams": out, "lanes": lanes, "budget_gb": budget / 2**30,
             "mix": "n in {64,256,1024,4096,16384} w.p. {.4,.3,.2,.08,.02}; range A/I alternating "
-                   "(I: il=1, iu=ceil(n/10)); D,E U(-1,1); results to host memory",
-            "api": "mr3_server_submit/poll (C ABI)"}
+                   "(I: il=1, iu=ceil(n/10)); D,E U(-1,1); jobz V",
+            "api": "mr3_server_submit_device/poll (C ABI): D, E staged in HBM, W, Z, Zsupp "
+                   "resident in HBM (Z within the budget)"}
 
 
 def _workload(args):
@@ -269,22 +438,31 @@ def run_reference(args):
     probs = [(D, E) for D, E, _ in wl.mixed_batch(args.count, seed=args.seed, nmax=args.nmax)]
     budget = args.ref_step_seconds
     for _ in range(args.warmup):
-        cpu_reference(probs, budget / 4, check=False)
-    vals = []
-    info = None
-    for _ in range(args.steps):
-        v, info = cpu_reference(probs, budget, check=False)
+        v, info = cpu_reference(probs, budget / 4)
         if v is None:
             print(json.dumps({"impl": "reference", "unavailable": info["unavailable"]}))
             return 0
+    vals, secs, bad, checked, worst = [], [], 0, 0, 0.0
+    info = None
+    for _ in range(args.steps):
+        v, info = cpu_reference(probs, budget)
         vals.append(v)
+        secs.append(info["mrrr_seconds"])
+        bad += info["checked_bad"]
+        checked += info["checked_problems"]
+        worst = max(worst, info["checked_worst_resid_orth"])
     value = float(np.mean(vals))
+    info = {**info, "value": value, "checked_problems": checked, "checked_bad": bad,
+            "checked_worst_resid_orth": worst}
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "eigenpairs/s",
            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": 1e3 * float(np.mean(secs)),
            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
            "config": {"workload": _workload(args), "problems_per_gpu": args.count,
-                      "seed": args.seed},
-           "cpu_baseline": {**info, "value": value},
+                      "seed": args.seed,
+                      "step": f"a stratified sample of about {budget:.0f} s of reference "
+                              "mrrr() calls (results checked outside the calls)"},
+           "cpu_baseline": info,
            "e2e": {"value": value, "unit": "eigenpairs/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
@@ -358,13 +536,19 @@ def main():
     ap.add_argument("--nmax", type=int, default=4096,
                     help="largest n of the batch (smaller values make small profiling cases)")
     ap.add_argument("--percall-sample", type=int, default=128)
+    ap.add_argument("--detail-out", default="",
+                    help="file for the per-kernel times and work counters (default: a file "
+                         "in the temporary directory)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
-    ap.add_argument("--ref-step-seconds", type=float, default=20.0)
-    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--ref-step-seconds", type=float, default=4.0)
+    ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--serve-rate", type=float, default=40.0)
-    ap.add_argument("--serve-count", type=int, default=400)
+    ap.add_argument("--serve-rates", default="1000,5000,20000",
+                    help="request rates (per second) of the serving streams, comma-separated")
+    ap.add_argument("--serve-count", type=int, default=10000,
+                    help="requests per serving stream")
+    ap.add_argument("--serve-budget-gb", type=float, default=120.0)
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--dense", type=int, default=0,
                     help="also time the dense driver dsyeig on an n x n symmetric matrix "
@@ -408,9 +592,10 @@ def main():
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    for q in recs:
-        if q.info != 0 or q.m != q.n:
-            raise SystemExit(f"solve failed: info {q.info} m {q.m} n {q.n}")
+    # every problem of the batch is checked (outside the timed region) on the
+    # result of the last warm-up step; a failure does not count as eigenpairs
+    check = check_batch(recs, T, ns)
+    pairs_per_step = check.pop("pairs_ok")
 
     # timed region
     S.profile(True)
@@ -523,10 +708,19 @@ def main():
         del PT, precs, single
 
     # end to end through the C ABI with pinned host buffers
+    # the batch's device arrays (56 GB of Z) are no longer needed
+    del T, recs
+    torch.cuda.empty_cache()
+
+    serving = None
+    if rank == 0 and not args.no_serve:
+        rates = [float(x) for x in args.serve_rates.split(",") if x]
+        serving = run_serving(M, wl, rates, args.serve_count, args.seed,
+                              int(args.serve_budget_gb * 2**30))
+        torch.cuda.empty_cache()
+
     e2e = None
     if rank == 0 and not args.no_e2e:
-        del T, recs
-        torch.cuda.empty_cache()
         hp = (M.HostProb * len(problems))()
         keep = []
         h2d = d2h = 0
@@ -568,10 +762,6 @@ def main():
                "steps": args.e2e_steps}
         del keep, hp
 
-    serving = None
-    if rank == 0 and not args.no_serve:
-        serving = run_serving(M, wl, args.serve_rate, args.serve_count, args.seed)
-
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         _, cpu = cpu_reference(problems, args.cpu_seconds)
@@ -585,6 +775,14 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return 0
+    detail = {"kernels_ms_per_step": {k: v[0] / args.steps for k, v in
+                                      sorted(kern.items(), key=lambda kv: -kv[1][0])},
+              "kernel_launches_per_step": {k: v[1] / args.steps for k, v in kern.items()},
+              "work_counters": dict(zip(groups, ctr))}
+    detail_path = args.detail_out or os.path.join(tempfile.gettempdir(), "mr3_bench_detail.json")
+    with open(detail_path, "w") as f:
+        json.dump(detail, f, indent=1)
+    top = sorted(detail["kernels_ms_per_step"].items(), key=lambda kv: -kv[1])[:6]
     out = {
         "metric": METRIC, "value": value, "unit": "eigenpairs/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -597,11 +795,11 @@ def main():
                    "l2": "flushed between steps by a 256 MB write; each step also writes "
                          f"{zbytes / 1e9:.1f} GB of Z"},
         "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "roofline": roof,
-        "roofline_hbm": roof_hbm, "fp64_peaks": {"fma_tflops": fma_tflops, "div_gops": div_gops},
-        "percall": percall, "serving": serving, "cpu_baseline": cpu, "dense": dense,
-        "kernels_ms_per_step": {k: v[0] / args.steps for k, v in
-                                sorted(kern.items(), key=lambda kv: -kv[1][0])},
-        "work_counters": dict(zip(groups, ctr)),
+        "check": check, "cpu_baseline": cpu, "dense": dense,
+        "fp64_peaks": {"fma_tflops": fma_tflops, "div_gops": div_gops},
+        "top_kernels_ms_per_step": {k: round(v, 2) for k, v in top},
+        "detail_file": detail_path,
+        "roofline_hbm": roof_hbm, "percall": percall, "serving": serving,
     }
     print(json.dumps(out))
     return 0

@@ -62,25 +62,43 @@ int mr3_batched_device(int nprob, mr3_cuda_prob *probs, void *stream);
 
 /* Serving (no counterpart in the reference, which answers one call at a
  * time; SRC/mrrr.c:87-296 is the per-request computation).  A server takes
- * a stream of independent requests and solves them in batches as they
- * arrive: one worker thread per size class (n <= 2048, and larger) takes
- * the oldest queued requests of its class that fit its share of the device
- * memory budget (budget_bytes; 0 = 120 GB) and solves them in one pass.
- * Results are those of a call alone.
+ * a stream of independent requests and solves them with continuous
+ * batching: several lanes (worker threads, each with its own solver
+ * context and streams) admit queued requests in arrival order whenever
+ * they free up, as long as the device bytes of all requests in flight
+ * (eigenvectors plus per-row work arrays) stay within the budget
+ * (budget_bytes; 0 = 120 GB) and the batch stays under a work cap; batches
+ * of different lanes run on the device at the same time, and lanes
+ * reserved for small requests (n <= 2048) run at high stream priority.
+ * Results are those of a call alone.  Environment (read at create):
+ * MR3_SERVE_LANES (default 4), MR3_SERVE_SMALL_LANES (default 2),
+ * MR3_SERVE_BATCH_WORK (work cap in eigenvector entries, default 2^27).
  *
- * mr3_server_submit: the request (an mr3_host_prob as for mr3_batched) and
- * its arrays must stay valid and untouched until poll reports it done.
- * Returns a ticket >= 1, or -1 bad arguments, -2 request larger than its
- * class's budget, -3 server stopping, -4 out of host memory.
- * mr3_server_poll: 1 done (req->info, req->m, ... are set), 0 pending,
+ * mr3_server_submit: a host request (an mr3_host_prob as for mr3_batched);
+ * eigenvectors are copied back to its host arrays.
+ * mr3_server_submit_device: a device request (an mr3_cuda_prob as for
+ * mr3_batched_device): D, E, W, Z, Zsupp stay resident in device memory and
+ * nothing crosses PCIe.
+ * The request struct and its arrays must stay valid and untouched until
+ * poll reports it done.  Both return a ticket >= 1, or -1 bad arguments,
+ * -2 request larger than the budget, -3 server stopping, -4 out of host
+ * memory.
+ * mr3_server_poll: 1 done (the request's info, m, ... are set), 0 pending,
  * -1 unknown ticket; wait = 1 blocks until done; latency_ms (or NULL)
  * receives the submit-to-done time.
+ * mr3_server_timing: of a done request, the time it waited for admission
+ * and the time from admission to done (1 done, 0 pending, -1 unknown).
+ * mr3_server_stats2: batches admitted while another lane's batch was on
+ * the device, the number of lanes and the budget.
  * mr3_server_destroy finishes every queued request, then stops. */
 typedef struct mr3_server mr3_server;
 int  mr3_server_create(int device, size_t budget_bytes, mr3_server **out);
 long long mr3_server_submit(mr3_server *s, mr3_host_prob *req);
+long long mr3_server_submit_device(mr3_server *s, mr3_cuda_prob *req);
 int  mr3_server_poll(mr3_server *s, long long ticket, int wait, double *latency_ms);
+int  mr3_server_timing(mr3_server *s, long long ticket, double *queued_ms, double *solve_ms);
 int  mr3_server_stats(mr3_server *s, long long *submitted, long long *solved, long long *batches);
+int  mr3_server_stats2(mr3_server *s, long long *overlapped, int *lanes, size_t *budget_bytes);
 void mr3_server_destroy(mr3_server *s);
 
 /* Replaces int dsyeig(...) of INCLUDE/mrrr.h:270-272 (implementation

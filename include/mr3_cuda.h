@@ -55,6 +55,12 @@ typedef struct mr3_cuda_ctx mr3_cuda_ctx;
 /* Per-device solver context with a grow-only workspace.  One context serves
  * one host thread at a time. */
 int  mr3_cuda_ctx_create(int device, mr3_cuda_ctx **out);
+
+/* mr3_cuda_ctx_create whose streams run at the device's highest stream
+ * priority when high != 0: the block scheduler starts their kernels'
+ * blocks ahead of those of normal-priority streams (no preemption of
+ * blocks already running).  The serving lanes for small requests use it. */
+int  mr3_cuda_ctx_create_prio(int device, int high, mr3_cuda_ctx **out);
 void mr3_cuda_ctx_destroy(mr3_cuda_ctx *ctx);
 
 /* Solve nprob problems in one batched pass on `stream` (a cudaStream_t, or

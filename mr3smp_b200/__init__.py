@@ -422,16 +422,7 @@ def mrrr_batched_device(problems: list[dict], stream: int | None = None) -> tupl
     P = len(problems)
     arr = (CudaProb * P)()
     for k, pb in enumerate(problems):
-        q = arr[k]
-        q.n = int(pb["D"].numel())
-        q.jobz = _JOB[pb["jobz"][0].upper()]
-        q.range = _RANGE[pb["range"][0].upper()]
-        q.il, q.iu, q.tryrac = int(pb.get("il", 1)), int(pb.get("iu", 1)), int(pb.get("tryrac", 0))
-        q.vl, q.vu = float(pb.get("vl", 0.0)), float(pb.get("vu", 0.0))
-        q.ldz = q.n
-        q.D, q.E, q.W = pb["D"].data_ptr(), pb["E"].data_ptr(), pb["W"].data_ptr()
-        q.Z = pb["Z"].data_ptr() if pb.get("Z") is not None else None
-        q.Zsupp = pb["Zsupp"].data_ptr() if pb.get("Zsupp") is not None else None
+        arr[k] = device_request(pb)
     rc = L.mr3_batched_device(P, arr, C.c_void_p(stream) if stream else None)
     return rc, [arr[k] for k in range(P)]
 
@@ -557,13 +548,32 @@ def _host_result(h, keep) -> dict:
     return out
 
 
-class Server:
-    """Serving handle (mr3_server_*): requests solved in batches as they arrive.
+def device_request(pb: dict):
+    """A ``CudaProb`` for one problem dict whose ``D, E, W`` (and for jobz V
+    ``Z``, ``Zsupp``) are CUDA tensors (float64 / int32, Z column-major with
+    ldz = n); the tensors must outlive the request."""
+    q = CudaProb()
+    q.n = int(pb["D"].numel())
+    q.jobz = _JOB[pb["jobz"][0].upper()]
+    q.range = _RANGE[pb["range"][0].upper()]
+    q.il, q.iu, q.tryrac = int(pb.get("il", 1)), int(pb.get("iu", 1)), int(pb.get("tryrac", 0))
+    q.vl, q.vu = float(pb.get("vl", 0.0)), float(pb.get("vu", 0.0))
+    q.ldz = q.n
+    q.D, q.E, q.W = pb["D"].data_ptr(), pb["E"].data_ptr(), pb["W"].data_ptr()
+    q.Z = pb["Z"].data_ptr() if pb.get("Z") is not None else None
+    q.Zsupp = pb["Zsupp"].data_ptr() if pb.get("Zsupp") is not None else None
+    return q
 
-    ``submit(problem)`` takes a problem dict as :func:`mrrr_batched` does and
-    returns a ticket; ``poll(ticket, wait)`` returns ``(result, latency_ms)``
-    once the request is done (``(None, None)`` while pending).  Results are
-    those of a call alone.
+
+class Server:
+    """Serving handle (mr3_server_*): requests solved with continuous batching.
+
+    ``submit(problem)`` takes a problem dict as :func:`mrrr_batched` does
+    (host arrays) and returns a ticket; ``submit_device(problem)`` takes one
+    whose arrays are CUDA tensors (results stay resident on the device);
+    ``poll(ticket, wait)`` returns ``(result, latency_ms)`` once the request
+    is done (``(None, None)`` while pending).  Results are those of a call
+    alone.
     """
 
     def __init__(self, device: int = 0, budget_bytes: int = 0, pinned: bool = False):
@@ -572,11 +582,19 @@ class Server:
         L.mr3_server_create.argtypes = [C.c_int, C.c_size_t, C.POINTER(C.c_void_p)]
         L.mr3_server_submit.restype = C.c_longlong
         L.mr3_server_submit.argtypes = [C.c_void_p, C.POINTER(HostProb)]
+        L.mr3_server_submit_device.restype = C.c_longlong
+        L.mr3_server_submit_device.argtypes = [C.c_void_p, C.POINTER(CudaProb)]
         L.mr3_server_poll.restype = C.c_int
         L.mr3_server_poll.argtypes = [C.c_void_p, C.c_longlong, C.c_int, C.POINTER(C.c_double)]
+        L.mr3_server_timing.restype = C.c_int
+        L.mr3_server_timing.argtypes = [C.c_void_p, C.c_longlong, C.POINTER(C.c_double),
+                                        C.POINTER(C.c_double)]
         L.mr3_server_stats.restype = C.c_int
         L.mr3_server_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong),
                                        C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+        L.mr3_server_stats2.restype = C.c_int
+        L.mr3_server_stats2.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_int),
+                                        C.POINTER(C.c_size_t)]
         L.mr3_server_destroy.argtypes = [C.c_void_p]
         self._L = L
         self._pinned = pinned
@@ -594,9 +612,21 @@ class Server:
         self._live[t] = (h, keep)
         return t
 
+    def submit_device(self, problem: dict, req: CudaProb | None = None) -> int:
+        """A device request: ``problem`` as for :func:`device_request` (or a
+        prepared ``req``); the tensors must stay alive until polled."""
+        q = req if req is not None else device_request(problem)
+        t = self._L.mr3_server_submit_device(self._h, C.byref(q))
+        if t < 1:
+            raise MR3Error(f"mr3_server_submit_device refused the request ({t})")
+        self._live[t] = (q, None)
+        return t
+
     def poll(self, ticket: int, wait: bool = True, raw: bool = False):
         """(result dict, latency ms), or with raw=True ((info, m, arrays),
-        latency ms) where arrays can be passed to submit() again."""
+        latency ms) where arrays can be passed to submit() again.  For a
+        device request the result is ``{"info", "m", ...}`` (the arrays are
+        the caller's tensors)."""
         lat = C.c_double(0.0)
         rc = self._L.mr3_server_poll(self._h, ticket, 1 if wait else 0, C.byref(lat))
         if rc < 0:
@@ -604,14 +634,29 @@ class Server:
         if rc == 0:
             return None, None
         h, keep = self._live.pop(ticket)
+        if keep is None:   # device request
+            r = dict(info=h.info, m=h.m, vl=h.vl_out, vu=h.vu_out, il=h.il_out, iu=h.iu_out,
+                     tryrac=h.tryrac_out)
+            return ((h.info, h.m, None) if raw else r), lat.value
         if raw:
             return (h.info, h.m, keep[:5]), lat.value
         return _host_result(h, keep), lat.value
 
+    def timing(self, ticket: int):
+        """(queued ms, solve ms) of a done request."""
+        a, b = C.c_double(0.0), C.c_double(0.0)
+        if self._L.mr3_server_timing(self._h, ticket, C.byref(a), C.byref(b)) != 1:
+            return None
+        return a.value, b.value
+
     def stats(self):
         a, b, c = C.c_longlong(), C.c_longlong(), C.c_longlong()
         self._L.mr3_server_stats(self._h, C.byref(a), C.byref(b), C.byref(c))
-        return {"submitted": a.value, "solved": b.value, "batches": c.value}
+        o, ln, bud = C.c_longlong(), C.c_int(), C.c_size_t()
+        self._L.mr3_server_stats2(self._h, C.byref(o), C.byref(ln), C.byref(bud))
+        return {"submitted": a.value, "solved": b.value, "batches": c.value,
+                "batches_overlapping_others": o.value, "lanes": ln.value,
+                "budget_bytes": bud.value}
 
     def close(self):
         if self._h:

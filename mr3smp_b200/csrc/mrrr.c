@@ -6,6 +6,7 @@
  * through the C ABI of mr3_cuda.h; there is no CPU path.  Calls are reentrant:
  * each calling thread borrows a solver context from a small pool.
  */
+#include <math.h>
 #include <pthread.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -91,6 +92,19 @@ static int ncols_of(const mr3_host_prob *h, int jz, int rg)
 
 static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+/* Whether the matrix entries the solver reads (D[0..n-1], E[0..n-2]) are
+ * all finite.  The reference does not check; a NaN or infinity there makes
+ * its bisection loop on meaningless counts.  Here such a problem is refused
+ * before any launch with info = 2 and the other problems of its batch are
+ * solved as if it were absent. */
+int mr3__finite_input(const double *D, const double *E, int n)
+{
+  int i, ok = 1;
+  for (i = 0; i < n; i++) ok &= isfinite(D[i]) != 0;
+  for (i = 0; i + 1 < n; i++) ok &= isfinite(E[i]) != 0;
+  return ok;
+}
+
 /* Batches whose eigenvectors exceed PIPE_MIN_BYTES are solved in chunks of
  * consecutive problems holding about PIPE_CHUNK_BYTES of Z each, so that the
  * device Z buffers stay within memory; the device-to-host copy of one
@@ -174,6 +188,10 @@ __attribute__((visibility("hidden"))) int mr3__batched_on(mr3_cuda_ctx *ctx, int
     dp[i].jobz = ok ? jz : -1;
     dp[i].range = ok ? rg : -1;
     if (!ok) continue;
+    if (!(jz == MR3_JOB_C && rg != MR3_RANGE_V) && !mr3__finite_input(h->D, h->E, h->n)) {
+      dp[i].jobz = -2;   /* non-finite input: info 2, not solved */
+      continue;
+    }
     orow[i] = nrow;
     ozs[i] = nzs;
     nrow += align_up((size_t)h->n, 32);
@@ -282,7 +300,7 @@ __attribute__((visibility("hidden"))) int mr3__batched_on(mr3_cuda_ctx *ctx, int
     mr3_host_prob *h = &hp[i];
     mr3_cuda_prob *q = &dp[i];
     h->m = 0;
-    if (q->jobz < 0) { h->info = MR3_EARG; continue; }
+    if (q->jobz < 0) { h->info = q->jobz == -2 ? MR3_EMISC : MR3_EARG; continue; }
     h->info = q->info;
     h->m = q->m;
     h->vl_out = q->vl_out; h->vu_out = q->vu_out;
@@ -300,7 +318,7 @@ __attribute__((visibility("hidden"))) int mr3__batched_on(mr3_cuda_ctx *ctx, int
 done:
   if (rc != MR3_OK) mr3_cuda_sync_all(ctx);
   for (i = 0; i < nprob; i++) {
-    if (rc != MR3_OK) hp[i].info = dp[i].jobz < 0 ? MR3_EARG : MR3_EMISC;
+    if (rc != MR3_OK) hp[i].info = dp[i].jobz == -1 ? MR3_EARG : MR3_EMISC;
     if (hp[i].info > worst) worst = hp[i].info;
   }
   free(dp);
@@ -352,6 +370,7 @@ int mrrr(char *jobz, char *range, int *np, double *D, double *E, double *vl,
     if (rg == MR3_RANGE_I) { *m = *iu - *il + 1; return 0; }
   }
   if (jz == MR3_JOB_V && *ldz < n) return 1;
+  if (!mr3__finite_input(D, E, n)) return 2;
   memset(&h, 0, sizeof(h));
   h.jobz = jobz[0]; h.range = range[0]; h.n = n;
   h.il = *il; h.iu = *iu; h.tryrac = *tryrac; h.ldz = (jz == MR3_JOB_V) ? *ldz : n;

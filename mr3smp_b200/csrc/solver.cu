@@ -195,6 +195,25 @@ __global__ void k_gather(ProbDev *probs, const double *const *Din, const double 
   }
 }
 
+// Non-finite entries among the values a problem's solve reads (D[0..n-1],
+// E[0..n-2]): flag[k] = 1.  Such a problem is refused before the solve.
+__global__ void k_finite(const ProbDev *probs, const double *const *Din, const double *const *Ein,
+                         int *flag) {
+  __shared__ int bad;
+  const int n = probs[blockIdx.x].n;
+  const double *d = Din[blockIdx.x], *e = Ein[blockIdx.x];
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  int b = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    b |= !isfinite(d[i]);
+    if (i < n - 1) b |= !isfinite(e[i]);
+  }
+  if (b) bad = 1;
+  __syncthreads();
+  if (threadIdx.x == 0) flag[blockIdx.x] = bad;
+}
+
 __global__ void __launch_bounds__(MR3_THREADS)
 k_prologue(ProbDev *probs, BlockDev *blocks, int *blk_of_row, double *D, double *E, double *E2,
            double2 *gers, double2 *TP, double2 *TPc, Tol tol) {
@@ -2535,8 +2554,16 @@ static int ensure_rows(mr3_cuda_ctx *c, size_t N, size_t P) {
 }
 
 extern "C" int mr3_cuda_ctx_create(int device, mr3_cuda_ctx **out) {
+  return mr3_cuda_ctx_create_prio(device, 0, out);
+}
+
+extern "C" int mr3_cuda_ctx_create_prio(int device, int high, mr3_cuda_ctx **out) {
+  if (!out) return MR3_EARG;
   *out = nullptr;
   if (cudaSetDevice(device) != cudaSuccess) return MR3_EMISC;
+  int prio_lo = 0, prio_hi = 0;
+  if (high && cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi) != cudaSuccess) prio_hi = 0;
+  const int prio = high ? prio_hi : 0;
   mr3_cuda_ctx *c = new mr3_cuda_ctx();
   c->device = device;
   cudaDeviceProp prop;
@@ -2546,9 +2573,9 @@ extern "C" int mr3_cuda_ctx_create(int device, mr3_cuda_ctx **out) {
     evok = evok && cudaEventCreateWithFlags(&c->xev[i], cudaEventDisableTiming) == cudaSuccess;
   for (int i = 0; i < SNG_ROUNDS; i++)
     evok = evok && cudaEventCreateWithFlags(&c->rev[i], cudaEventDisableTiming) == cudaSuccess;
-  if (!evok || cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&c->rnd, cudaStreamNonBlocking) != cudaSuccess ||
+  if (!evok || cudaStreamCreateWithPriority(&c->own, cudaStreamNonBlocking, prio) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&c->aux, cudaStreamNonBlocking, prio) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&c->rnd, cudaStreamNonBlocking, prio) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->rnd_done, cudaEventDisableTiming) != cudaSuccess ||
       cudaMalloc((void **)&c->lc, 2 * sizeof(LevelCounters)) != cudaSuccess ||
       cudaMalloc((void **)&c->sc, sizeof(SngCounters)) != cudaSuccess ||
@@ -2853,8 +2880,51 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
   idx.reserve(nlive);
   for (int i = 0; i < P; i++)
     if (live[i]) idx.push_back(i);
+  int rc = ensure_rows(c, 0, (size_t)nlive);
+  if (rc != MR3_OK) return rc;
+  {
+    // a problem with a non-finite entry is refused (info 2) before the
+    // solve, so that it cannot disturb the others of the batch
+    const int Lc = nlive;
+    for (int k = 0; k < Lc; k++) {
+      c->h_probs[k].n = pr[idx[k]].n;
+      c->h_ptrs[k] = (void *)pr[idx[k]].D;
+      c->h_ptrs[Lc + k] = (void *)pr[idx[k]].E;
+    }
+    CK(cudaMemcpyAsync(c->probs, c->h_probs, Lc * sizeof(ProbDev), cudaMemcpyHostToDevice, st),
+       "screen probs");
+    CK(cudaMemcpyAsync(c->Din, c->h_ptrs, Lc * sizeof(void *), cudaMemcpyHostToDevice, st),
+       "screen D");
+    CK(cudaMemcpyAsync(c->Ein, c->h_ptrs + Lc, Lc * sizeof(void *), cudaMemcpyHostToDevice, st),
+       "screen E");
+    LAUNCH(k_finite, Lc, 256, c->probs, c->Din, c->Ein, c->flag);
+    CK(cudaMemcpyAsync(c->h_flag, c->flag, Lc * sizeof(int), cudaMemcpyDeviceToHost, st),
+       "screen flags");
+    CK(cudaStreamSynchronize(st), "screen sync");
+    int kept = 0;
+    for (int k = 0; k < Lc; k++) {
+      mr3_cuda_prob &q = pr[idx[k]];
+      if (c->h_flag[k]) {
+        q.info = MR3_EMISC;
+        N -= (size_t)q.n;
+        nlive--;
+      } else {
+        idx[kept++] = idx[k];
+      }
+    }
+    idx.resize(kept);
+    if (nlive == 0) return MR3_OK;
+    mmax = 0; nmaxV = 0; anyV = anyN = anyTry = false;
+    for (int i : idx) {
+      const mr3_cuda_prob &q = pr[i];
+      mmax = std::max(mmax, q.n);
+      if (q.jobz == MR3_JOB_V) { anyV = true; nmaxV = std::max(nmaxV, q.n); }
+      if (q.jobz == MR3_JOB_N) anyN = true;
+      if (q.tryrac) anyTry = true;
+    }
+  }
   const int L = nlive;
-  int rc = ensure_rows(c, N, (size_t)L);
+  rc = ensure_rows(c, N, (size_t)L);
   if (rc != MR3_OK) return rc;
   // column tiles of the problems whose column count is known up front
   // (jobz V, range A or I); finished tiles are reported to done_fn at the

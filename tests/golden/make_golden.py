@@ -33,7 +33,9 @@ sys.path.insert(0, ROOT)
 import oracle  # noqa: E402
 from mr3smp_b200 import workloads as wl  # noqa: E402
 
-REF = "/root/reference"
+# the reference's source tree (for its example input file): the environment
+# variable MR3_REFERENCE_DIR, or the first command-line argument
+REF = os.environ.get("MR3_REFERENCE_DIR") or (sys.argv[1] if len(sys.argv) > 1 else "")
 
 
 def read_tridiag(path):
@@ -51,7 +53,9 @@ def main():
     oracle.build()
     subprocess_ok = oracle.ref_lib() is not None
     if not subprocess_ok:
-        raise SystemExit("reference library not built: make -C oracle ref")
+        raise SystemExit("reference library not built: make -C oracle ref REF=<reference tree>")
+    if not REF or not os.path.isdir(REF):
+        raise SystemExit("give the reference's source tree: MR3_REFERENCE_DIR=<dir> or argument 1")
     cases = []
     D21, E21 = read_tridiag(os.path.join(REF, "EXAMPLES/Tridiag/C/Wilkinson21.data"))
     assert np.array_equal(D21, wl.wilkinson_plus(21)) and np.all(E21[:-1] == 1.0)

@@ -1,6 +1,8 @@
 """The serving front end (mr3_server_*): requests of mixed sizes and ranges
-submitted as a stream, from several host threads, are solved in batches,
-and each result is identical to the one the same request gets alone."""
+submitted as a stream, from several host threads, with host or
+device-resident arrays, are solved with continuous batching on several
+lanes, and each result is identical to the one the same request gets
+alone."""
 import threading
 
 import numpy as np
@@ -76,11 +78,11 @@ def test_server_alone_and_mixed_identical_from_threads():
 
 
 def test_server_rejects_bad_and_oversized_requests():
-    S = M.Server(budget_bytes=64 << 20)   # 8 MB for the small class, 56 MB large
+    S = M.Server(budget_bytes=64 << 20)
     try:
         D, E = wl.uniform(3000, seed=1)
         with pytest.raises(M.MR3Error):
-            S.submit(dict(jobz="V", range="A", D=D, E=E))   # 72 MB of Z > 56 MB
+            S.submit(dict(jobz="V", range="A", D=D, E=E))   # 72 MB of Z > 64 MB
         D, E = wl.uniform(50, seed=2)
         with pytest.raises(M.MR3Error):
             S.submit(dict(jobz="V", range="I", D=D, E=E, il=5, iu=4))
@@ -89,3 +91,78 @@ def test_server_rejects_bad_and_oversized_requests():
         assert r["info"] == 0 and r["m"] == 50
     finally:
         S.close()
+
+
+def _c4_requests(count, seed):
+    """The serving mix at sizes up to 4096: n in {64, 256, 1024, 4096},
+    range A and I (il = 1, iu = ceil(n/10)) alternating, D, E ~ U(-1, 1)."""
+    rng = np.random.default_rng(seed)
+    ns = rng.choice([64, 256, 1024, 4096], size=count, p=[0.4, 0.3, 0.2, 0.1])
+    out = []
+    for k, n in enumerate(ns):
+        n = int(n)
+        D, E = wl.uniform(n, seed=seed * 1000 + k)
+        if k % 2 == 0:
+            out.append(dict(jobz="V", range="A", D=D, E=E))
+        else:
+            out.append(dict(jobz="V", range="I", D=D, E=E, il=1, iu=-(-n // 10)))
+    return out
+
+
+def _device_arrays(p):
+    import torch
+    n = len(p["D"])
+    cols = n if p["range"] == "A" else p["iu"] - p["il"] + 1
+    return dict(p, D=torch.tensor(p["D"], device="cuda"), E=torch.tensor(p["E"], device="cuda"),
+                W=torch.zeros(n, dtype=torch.float64, device="cuda"),
+                Z=torch.zeros(n * cols, dtype=torch.float64, device="cuda"),
+                Zsupp=torch.zeros(2 * n, dtype=torch.int32, device="cuda"))
+
+
+def test_server_device_requests_c4_sizes_alone_and_mixed():
+    """Device-resident requests of the serving mix (n up to 4096), submitted
+    all at once so that lanes admit them while others are in flight: every
+    result (W, Z, Zsupp, the overwritten D, E) equals the request's result
+    alone, bit for bit."""
+    import torch
+    reqs = _c4_requests(48, seed=17)
+    dev = [_device_arrays(p) for p in reqs]
+    S = M.Server()
+    try:
+        tickets = [S.submit_device(d) for d in dev]
+        res = [S.poll(t, wait=True)[0] for t in tickets]
+        st = S.stats()
+    finally:
+        S.close()
+    torch.cuda.synchronize()
+    assert st["solved"] == len(reqs) and st["lanes"] >= 2
+    print("batches", st["batches"], "overlapping others", st["batches_overlapping_others"])
+    for k, (p, d, r) in enumerate(zip(reqs, dev, res)):
+        n = len(p["D"])
+        alone = M.mrrr(p["jobz"], p["range"], p["D"], p["E"], **_kw(p))
+        assert r["info"] == 0 and r["m"] == alone["m"], k
+        m = r["m"]
+        assert np.array_equal(d["W"].cpu().numpy()[:m], alone["W"]), k
+        Z = d["Z"].cpu().numpy()[: n * m].reshape(m, n).T
+        assert np.array_equal(Z, alone["Z"]), k
+        assert np.array_equal(d["Zsupp"].cpu().numpy()[: 2 * m], alone["Zsupp"]), k
+        assert np.array_equal(d["D"].cpu().numpy(), alone["D"]), k
+        assert np.array_equal(d["E"].cpu().numpy(), alone["E"]), k
+
+
+def test_server_budget_admits_in_turn():
+    """A budget that holds one large request at a time: requests wait for
+    admission until the bytes in flight allow them, and all finish with
+    their results alone."""
+    reqs = _c4_requests(12, seed=23)
+    big = max(8 * len(p["D"]) * (len(p["D"]) if p["range"] == "A" else p["iu"])
+              + 560 * len(p["D"]) for p in reqs)
+    S = M.Server(budget_bytes=big + (1 << 20))
+    try:
+        tickets = [S.submit(p) for p in reqs]
+        res = [S.poll(t, wait=True)[0] for t in tickets]
+    finally:
+        S.close()
+    for k, (p, r) in enumerate(zip(reqs, res)):
+        alone = M.mrrr(p["jobz"], p["range"], p["D"], p["E"], **_kw(p))
+        assert_same(r, alone, f"request {k}")

@@ -6,9 +6,6 @@ cuSOLVER's/cuBLAS's, so the results match the reference's within
 tolerances: eigenvalues against numpy/scipy and the reference's own complex
 drivers (oracle/_ref) within 10*n*eps*||A|| (50 for the generalized
 problems), vectors by residual and (B-)orthogonality.
-
-These tests have not run on a GPU yet; they are skipped until their first
-run on a device has been checked.
 """
 import numpy as np
 import pytest
@@ -18,7 +15,6 @@ from conftest import EPS, gpu_available
 import oracle
 
 pytestmark = [pytest.mark.gpu,
-              pytest.mark.skip(reason="complex drivers: awaiting their first GPU run"),
               pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")]
 
 

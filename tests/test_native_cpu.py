@@ -73,3 +73,24 @@ def test_server_create_fails_cleanly_without_gpu():
         pytest.skip("a GPU is present")
     with pytest.raises(M.MR3Error):
         M.Server()
+
+
+@pytest.mark.parametrize("where", ["D0", "Dlast", "E0", "Einf"])
+def test_non_finite_input_refused_without_gpu(where):
+    """A NaN or infinity among the entries the solve reads (D[0..n-1],
+    E[0..n-2]) is refused with info 2 before any device work; E[n-1] is not
+    read (the reference overwrites it), so a NaN there is accepted."""
+    D = np.linspace(-1, 1, 10)
+    E = np.full(10, 0.5)
+    if where == "D0":
+        D[0] = np.nan
+    elif where == "Dlast":
+        D[-1] = np.inf
+    elif where == "E0":
+        E[0] = np.nan
+    else:
+        E[8] = -np.inf
+    assert M.mrrr("V", "A", D, E)["info"] == 2
+    assert M.mrrr("N", "V", D, E, vl=-1.0, vu=1.0)["info"] == 2
+    # counting with range A or I never reads the matrix (SRC/mrrr.c:130-138)
+    assert M.mrrr("C", "A", D, E)["info"] == 0

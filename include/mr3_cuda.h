@@ -146,7 +146,9 @@ int  mr3_cuda_fp64_peaks(int device, double *fma_tflops, double *div_gops);
  * eigenvector, zero outside its support, Zsupp[2j..2j+1] the 1-based support.
  * D (n), L (n-1), lambda (m), Z (ldz*m), Zsupp (2m) are device pointers;
  * gaptol is dlar1v's support-truncation tolerance (0 keeps every entry).
- * Scratch is one static device array of the library (16.8 MB per GPU), so
+ * The pivot threshold is derived from the representation as the solver
+ * derives it from T: DBL_MIN * max(1, max_i (D(i) L(i))^2).  n = 1 gives
+ * unit vectors.  Scratch is one static device array of the library (16.8 MB per GPU), so
  * n <= MR3_NOALLOC_NMAX; larger n, m < 0 or ldz < n return 1.  The first call
  * on a device looks the array up (cudaGetSymbolAddress); make that first call
  * before any stream capture.  All calls share the array: calls that overlap

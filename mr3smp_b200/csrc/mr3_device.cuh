@@ -694,7 +694,7 @@ static __device__ __noinline__ double dv_r1v_passB(bool active, int n, double la
           if (slow && tmp == 0.0) pn = cpx[u] - lambda;
           Y[(size_t)i * R1V_LD] = um;
           p = pn;
-          if (i > r1 && i <= r2) {        // candidate r = i: S(i-1) + P(i-1)
+          if (SEARCH && i > r1 && i <= r2) {   // candidate r = i: S(i-1) + P(i-1)
             const double sprev = csp[u];
             double c = sprev + p;
             if (c == 0.0) c = eps * sprev;
@@ -1007,7 +1007,7 @@ static __device__ __noinline__ bool dv_r1c_statio(double lambda, const double2 *
 // checkpoint rows stay aligned.  The twist search needs the stationary SI of
 // row i-1 at row i: in search mode a block's SI values are recomputed from
 // its stationary checkpoint first.  Returns P(R1-1).
-template <bool SLOW>
+template <bool SLOW, bool SEARCH>
 static __device__ __noinline__ double dv_r1c_progr(bool active, int n, double lambda,
                                             const double2 *__restrict__ P,
                                             const double2 *__restrict__ Q, int ps, double pivmin,
@@ -1029,7 +1029,9 @@ static __device__ __noinline__ double dv_r1c_progr(bool active, int n, double la
     }
   }
   const bool work = active && top >= r1;
-  const bool search = r2 > r1;
+  // SEARCH = false: no lane of the warp searches the twist index (the rows'
+  // Q halves and the stationary recompute are not needed)
+  const bool search = SEARCH && r2 > r1;
   const int topw = __reduce_max_sync(0xffffffffu, work ? top : 0);
   const int r1w = __reduce_min_sync(0xffffffffu, work ? r1 : 0x7fffffff);
   if (topw >= 1) {
@@ -1048,7 +1050,7 @@ static __device__ __noinline__ double dv_r1c_progr(bool active, int n, double la
         for (int u = 0; u < CK_K; u++) {
           const int i = d_imax(d_imin(base + u, hi), lo);
           bp[u] = P[(size_t)(i - 1) * ps];
-          if (search) bq[u] = Q[(size_t)(i - 1) * ps];
+          if (SEARCH && search) bq[u] = Q[(size_t)(i - 1) * ps];
         }
       }
     };
@@ -1062,7 +1064,7 @@ static __device__ __noinline__ double dv_r1c_progr(bool active, int n, double la
       const int hi = d_imin(base + CK_K - 1, top), lo = d_imax(base, r1);
       const bool bw = work && lo <= hi;
       double sia[CK_K];
-      if (bw && search) {
+      if (SEARCH && bw && search) {
         // SI of rows base-1 .. base+CK_K-2 (those of twist candidates only);
         // in search mode r1 = 1, so the block's rows were loaded unclamped
         sia[0] = ckIv;
@@ -1103,7 +1105,10 @@ static __device__ __noinline__ double dv_r1c_progr(bool active, int n, double la
         }
       }
 #pragma unroll
-      for (int u = 0; u < CK_K; u++) { cp[u] = np_[u]; cq[u] = nq[u]; }
+      for (int u = 0; u < CK_K; u++) {
+        cp[u] = np_[u];
+        if (SEARCH) cq[u] = nq[u];
+      }
       ckSv = nckS;
       ckIv = nckI;
     }
@@ -1134,8 +1139,13 @@ static __device__ __noinline__ void dv_r1c_factor(bool active, int n, double lam
   }
   double best = 0.0;
   bool have = false;
-  double pr1 = dv_r1c_progr<false>(active, n, lambda, P, Q, ps, pivmin, r1, r2, sawnan1, ck.S, ck.I,
-                                   ck.P, silast, &neg2, &rbest, &best, &have);
+  // the search form only when a lane of the warp searches its twist index
+  const bool anysearch = __any_sync(0xffffffffu, active && r2 > r1);
+  double pr1 = anysearch
+      ? dv_r1c_progr<false, true>(active, n, lambda, P, Q, ps, pivmin, r1, r2, sawnan1, ck.S,
+                                  ck.I, ck.P, silast, &neg2, &rbest, &best, &have)
+      : dv_r1c_progr<false, false>(active, n, lambda, P, Q, ps, pivmin, r1, r2, sawnan1, ck.S,
+                                   ck.I, ck.P, silast, &neg2, &rbest, &best, &have);
   bool sawnan2 = active && isnan(pr1);
   if (__any_sync(0xffffffffu, sawnan2)) {
     // odr1v.f:234-250: the progressive sweep again with the NaN-safe
@@ -1143,8 +1153,8 @@ static __device__ __noinline__ void dv_r1c_factor(bool active, int n, double lam
     int n2b = 0, rbb = 0;
     double bb = 0.0;
     bool hb = false;
-    double pb = dv_r1c_progr<true>(sawnan2, n, lambda, P, Q, ps, pivmin, r1, r2, sawnan1, ck.S, ck.I,
-                                   ck.P, silast, &n2b, &rbb, &bb, &hb);
+    double pb = dv_r1c_progr<true, true>(sawnan2, n, lambda, P, Q, ps, pivmin, r1, r2, sawnan1,
+                                         ck.S, ck.I, ck.P, silast, &n2b, &rbb, &bb, &hb);
     if (sawnan2) { pr1 = pb; neg2 = n2b; rbest = rbb; best = bb; have = hb; }
   }
   if (!active) return;
@@ -1287,6 +1297,191 @@ static __device__ __noinline__ void dv_r1c_solve(int n, double lambda, const dou
         }
       }
     }
+  }
+  o->r = r;
+  o->mingma = mingma;
+  o->isupp1 = is1;
+  o->isupp2 = is2;
+  o->ztz = ztz;
+  const double tmp = 1.0 / ztz;
+  o->nrminv = sqrt(tmp);
+  o->resid = fabs(mingma) * o->nrminv;
+  o->rqcorr = mingma * tmp;
+  o->sawnan = slow;
+}
+
+// Back-substitution of dlar1v (as dv_r1c_solve) for the whole warp in
+// lock-step: the lanes visit the same absolute rows at the same time (the
+// upward solve from the largest twist index down, the downward one from the
+// smallest up), each lane working only inside its own range, so that a
+// checkpoint access is one 256-byte row across the lanes and lanes that
+// share a representation read its rows once.  With `write`, the lanes' z
+// values go to a shared-memory tile of 32 rows x 32 lanes (tile[row * 33 +
+// lane], 8448 bytes per warp); a tile is written out when the sweep leaves
+// it, one column at a time by the whole warp (lane k writes row k of the
+// tile's segment of that column): coalesced 256-byte segments instead of
+// one 8-byte store per lane and row.  A block of CK_K rows never straddles
+// two tiles (upward tiles cover rows 32t+1 .. 32t+32, downward ones, whose
+// block j writes z of rows 4j+2 .. 4j+5, rows 32t+2 .. 32t+33).  zout is the
+// lane's column of Z at the block's first row; z is written unscaled.  Every
+// value and every test is the one of dv_r1c_solve, in the same order per
+// lane.
+#define R1W_T 32
+static __device__ __noinline__ void dv_r1w_solve(bool active, int n, double lambda,
+                                          const double2 *__restrict__ P,
+                                          const double2 *__restrict__ Q, int ps, double pivmin,
+                                          double gaptol, int r, bool slow, bool slowA, bool slowB,
+                                          const double *__restrict__ ckS,
+                                          const double *__restrict__ ckP, double mingma,
+                                          double *zout, bool write, double *tile,
+                                          dlar1v_out *o) {
+  static_assert(R1W_T == 32 && R1W_T % CK_K == 0, "tiles hold whole blocks");
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  int is1 = 1, is2 = n;
+  double ztz = 1.0;
+  const bool wr = active && write;
+  if (wr) zout[r - 1] = 1.0;
+  const bool anyw = __any_sync(full, wr);
+  // rows [tlo, thi] (1-based) of the current tile hold this lane's values
+  int tbase = 0, tlo = 1, thi = 0;
+  auto flush = [&]() {   // warp-uniform call sites only
+    __syncwarp();
+    unsigned m = __ballot_sync(full, wr && tlo <= thi);
+    while (m) {
+      const int c = __ffs(m) - 1;
+      m &= m - 1;
+      const int lo = __shfl_sync(full, tlo, c), hi = __shfl_sync(full, thi, c);
+      double *zc = (double *)__shfl_sync(full, (unsigned long long)zout, c);
+      const int row = tbase + lane;
+      if (row >= lo && row <= hi) zc[row - 1] = tile[lane * 33 + c];
+    }
+    __syncwarp();
+    tlo = 1;
+    thi = 0;
+  };
+  auto put = [&](int row, double z) {
+    tile[(row - tbase) * 33 + lane] = z;
+    if (tlo > thi) { tlo = row; thi = row; }
+    else { tlo = d_imin(tlo, row); thi = d_imax(thi, row); }
+  };
+  // upward solve: i = r-1 .. 1, blocks from the warp's largest r down
+  {
+    double zp = 1.0, zpp = 0.0;   // z(i+1), z(i+2)
+    bool go = active && r - 1 >= 1;
+    const int jtop = __reduce_max_sync(full, go ? (r - 2) / CK_K : -1);
+    int cur_tile = -1;
+    for (int jb = jtop; jb >= 0; jb--) {
+      if (!__any_sync(full, go)) break;
+      const int base = jb * CK_K + 1;
+      if (anyw && jb * CK_K / R1W_T != cur_tile) {
+        if (cur_tile >= 0) flush();
+        cur_tile = jb * CK_K / R1W_T;
+        tbase = cur_tile * R1W_T + 1;
+      }
+      const int hi = d_imin(base + CK_K - 1, r - 1);
+      if (go && jb <= (r - 2) / CK_K) {
+        double lpa[CK_K], lda[CK_K];
+        double s = ckS[(size_t)jb * 32];
+#pragma unroll
+        for (int u = 0; u < CK_K; u++) {
+          const int i = base + u;
+          if (i <= hi) {
+            const double2 pp = P[(size_t)(i - 1) * ps];
+            const double2 q = Q[(size_t)(i - 1) * ps];
+            double dplus = pp.x + s;
+            if (slowA && fabs(dplus) < pivmin) dplus = -pivmin;
+            const double lp = q.y / dplus;
+            double si = s * lp * q.x;
+            if (slowA && lp == 0.0) si = pp.y;
+            s = si - lambda;
+            lpa[u] = lp;
+            lda[u] = q.y;
+          }
+        }
+#pragma unroll
+        for (int u = CK_K - 1; u >= 0; u--) {
+          const int i = base + u;
+          if (go && i <= hi) {
+            const double ldi = lda[u];
+            double zi;
+            if (!slow) zi = -(lpa[u] * zp);
+            else if (zp == 0.0) zi = -(Q[(size_t)i * ps].y / ldi) * zpp;
+            else zi = -(lpa[u] * zp);
+            if ((fabs(zi) + fabs(zp)) * fabs(ldi) < gaptol) {
+              is1 = i + 1;
+              go = false;
+            } else {
+              ztz = ztz + zi * zi;
+              if (wr) put(i, zi);
+              zpp = zp;
+              zp = zi;
+            }
+          }
+        }
+      }
+    }
+    if (anyw && cur_tile >= 0) flush();
+  }
+  // downward solve: i = r .. n-1 (z of row i+1 from z of row i), blocks from
+  // the warp's smallest r up
+  {
+    double zc = 1.0, zcp = 0.0;   // z(i), z(i-1)
+    bool go = active && r <= n - 1;
+    const int jbot = __reduce_min_sync(full, go ? (r - 1) / CK_K : 0x7fffffff);
+    const int jend = __reduce_max_sync(full, go ? (n - 2) / CK_K : -1);
+    int cur_tile = -1;
+    for (int jb = jbot; jb <= jend; jb++) {
+      if (!__any_sync(full, go)) break;
+      const int base = jb * CK_K + 1;
+      if (anyw && jb * CK_K / R1W_T != cur_tile) {
+        if (cur_tile >= 0) flush();
+        cur_tile = jb * CK_K / R1W_T;
+        tbase = cur_tile * R1W_T + 2;
+      }
+      const int lo = d_imax(base, r), hi = d_imin(base + CK_K - 1, n - 1);
+      if (go && jb >= (r - 1) / CK_K && lo <= hi) {
+        double uma[CK_K], lda[CK_K];
+        double p = ckP[(size_t)jb * 32];
+#pragma unroll
+        for (int u = CK_K - 1; u >= 0; u--) {
+          const int i = base + u;
+          if (i >= lo && i <= hi) {
+            const double2 pp = P[(size_t)(i - 1) * ps];
+            const double2 q = Q[(size_t)(i - 1) * ps];
+            double dminus = pp.y + p;
+            if (slowB && fabs(dminus) < pivmin) dminus = -pivmin;
+            const double tmp = pp.x / dminus;
+            uma[u] = q.x * tmp;
+            lda[u] = q.y;
+            double pn = p * tmp - lambda;
+            if (slowB && tmp == 0.0) pn = pp.x - lambda;
+            p = pn;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < CK_K; u++) {
+          const int i = base + u;
+          if (go && i >= lo && i <= hi) {
+            const double ldi = lda[u];
+            double zn;
+            if (!slow) zn = -(uma[u] * zc);
+            else if (zc == 0.0) zn = -(Q[(size_t)(i - 2) * ps].y / ldi) * zcp;
+            else zn = -(uma[u] * zc);
+            if ((fabs(zc) + fabs(zn)) * fabs(ldi) < gaptol) {
+              is2 = i;
+              go = false;
+            } else {
+              ztz = ztz + zn * zn;
+              if (wr) put(i + 1, zn);
+              zcp = zc;
+              zc = zn;
+            }
+          }
+        }
+      }
+    }
+    if (anyw && cur_tile >= 0) flush();
   }
   o->r = r;
   o->mingma = mingma;

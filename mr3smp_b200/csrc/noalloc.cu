@@ -10,13 +10,19 @@
 // workspace.  The caller passes the representation, the eigenvalues and the
 // output arrays; the call allocates nothing.
 //
-// Scratch: packed representation rows (4 * NMAX doubles) and, for each of
-// NA_WARPS warps, two per-lane arrays of NMAX rows x 32 lanes: 16.8 MB that
-// every GPU which loads the library holds until the process exits.  All
-// calls share it and it keeps the last call's contents; every call rewrites
-// the rows it reads before reading them, so nothing has to start at zero.
-// Calls that overlap on the GPU (different streams or host threads at the
-// same time) race on it.
+// Scratch: packed representation rows (4 * NMAX doubles), the pivot
+// threshold, and, for each of NA_WARPS warps, two per-lane arrays of NMAX
+// rows x 32 lanes: 16.8 MB that every GPU which loads the library holds
+// until the process exits.  All calls share it and it keeps the last call's
+// contents; every call rewrites what it reads before reading it, so nothing
+// has to start at zero.  Calls that overlap on the GPU (different streams
+// or host threads at the same time) race on it.
+//
+// The pivot threshold is the solver's, pivmin = DBL_MIN * max(1, max e_i^2)
+// (SRC/mrrr_val.c:226-233), with the off-diagonal e_i of the represented
+// matrix taken as D(i) L(i); for a root representation L D L^T = T - sigma I
+// that is T's off-diagonal up to rounding.  Each warp runs on an SM of its
+// own (one-warp blocks).
 #include <cuda_runtime.h>
 #include <float.h>
 
@@ -28,8 +34,9 @@
 #define NA_NMAX 2048   // largest n accepted (MR3_NOALLOC_NMAX in mr3_cuda.h)
 #define NA_WARPS 16    // warps that share the scratch
 #define NA_ROWS_OFF 0
-#define NA_LANES_OFF (4 * NA_NMAX)
-#define NA_TOTAL (4 * NA_NMAX + NA_WARPS * 2 * NA_NMAX * 32)
+#define NA_PIV_OFF (4 * NA_NMAX)
+#define NA_LANES_OFF (4 * NA_NMAX + 32)
+#define NA_TOTAL (4 * NA_NMAX + 32 + NA_WARPS * 2 * NA_NMAX * 32)
 
 static_assert(NA_NMAX == MR3_NOALLOC_NMAX, "limit must match the header");
 
@@ -41,33 +48,56 @@ static std::mutex g_na_mu;
 
 namespace {
 
-// Rows of the representation: P[i] = (D(i), D(i)L(i)^2), Q[i] = (L(i), D(i)L(i)).
-__global__ void k_na_pack(int n, const double *D, const double *L, double *scratch) {
+// Rows of the representation: P[i] = (D(i), D(i)L(i)^2), Q[i] = (L(i), D(i)L(i)),
+// and the pivot threshold (one block).
+__global__ void __launch_bounds__(1024) k_na_pack(int n, const double *D, const double *L,
+                                                  double *scratch) {
+  __shared__ double red[32];
   double2 *P = reinterpret_cast<double2 *>(scratch + NA_ROWS_OFF);
   double2 *Q = P + NA_NMAX;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  double emax = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
     double dv = D[i];
     if (i < n - 1) {
       double lv = L[i];
       double ld = dv * lv;
       P[i] = make_double2(dv, ld * lv);
       Q[i] = make_double2(lv, ld);
+      emax = fmax(emax, fabs(ld));
     } else {
       P[i] = make_double2(dv, 0.0);
       Q[i] = make_double2(0.0, 0.0);
     }
   }
+  for (int o = 16; o > 0; o >>= 1) emax = fmax(emax, __shfl_xor_sync(0xffffffffu, emax, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = emax;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double e = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) e = fmax(e, red[w]);
+    scratch[NA_PIV_OFF] = MR3_SAFMIN * fmax(1.0, e * e);
+  }
+}
+
+// n = 1: every eigenvector is (1), support {1}.
+__global__ void k_na_unit(int m, double *Z, int ldz, int *Zsupp) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < m; v += gridDim.x * blockDim.x) {
+    Z[(size_t)v * ldz] = 1.0;
+    Zsupp[2 * v] = 1;
+    Zsupp[2 * v + 1] = 1;
+  }
 }
 
 // One lane per eigenvalue: dlar1v with the twist index searched over 1..n,
 // then the normalised vector (zero outside its support) into Z.
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(32)
 k_na_vec(int n, int m, const double *lambda, double gaptol, double *Z, int ldz, int *Zsupp,
          double *scratch) {
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const double2 *P = reinterpret_cast<const double2 *>(scratch + NA_ROWS_OFF);
   const double2 *Q = P + NA_NMAX;
+  const double pivmin = scratch[NA_PIV_OFF];
   double *X = scratch + NA_LANES_OFF + (size_t)gw * 2 * NA_NMAX * 32 + lane;
   double *Y = X + (size_t)NA_NMAX * 32;
   for (int v0 = gw * 32; v0 < m; v0 += NA_WARPS * 32) {
@@ -76,7 +106,7 @@ k_na_vec(int n, int m, const double *lambda, double gaptol, double *Z, int ldz, 
     r1v_state st;
     st.r = 0; st.mingma = 0.0; st.sawnan = false;
     int negc = 0;
-    dv_r1v_factor(active, n, active ? lambda[v] : 0.0, P, Q, 1, MR3_SAFMIN, false, 0, X, Y, &negc,
+    dv_r1v_factor(active, n, active ? lambda[v] : 0.0, P, Q, 1, pivmin, false, 0, X, Y, &negc,
                   &st);
     dlar1v_out o;
     o.isupp1 = 1; o.isupp2 = n; o.nrminv = 0.0; o.r = 0;
@@ -116,7 +146,11 @@ extern "C" int mr3_cuda_eigvec_noalloc(int n, const double *D, const double *L, 
     scratch = g_na_ptr[dev];
   }
   cudaStream_t st = (cudaStream_t)stream;
-  k_na_pack<<<(n + 255) / 256, 256, 0, st>>>(n, D, L, scratch);
-  k_na_vec<<<NA_WARPS * 32 / 256, 256, 0, st>>>(n, m, lambda, gaptol, Z, ldz, Zsupp, scratch);
+  if (n == 1) {
+    k_na_unit<<<(m + 255) / 256, 256, 0, st>>>(m, Z, ldz, Zsupp);
+    return cudaGetLastError() == cudaSuccess ? MR3_OK : MR3_EMISC;
+  }
+  k_na_pack<<<1, 1024, 0, st>>>(n, D, L, scratch);
+  k_na_vec<<<NA_WARPS, 32, 0, st>>>(n, m, lambda, gaptol, Z, ldz, Zsupp, scratch);
   return cudaGetLastError() == cudaSuccess ? MR3_OK : MR3_EMISC;
 }

@@ -91,6 +91,8 @@ struct SngCounters {
   int bs_n, bs_next, err, nin; // bisection list; err: a list outlived the
                                // rounds; nin: entries of this round's list
   int done_n, done_exp;        // finished column tiles: listed, exported to the host
+  int mode, fin_ctas;          // 0 rounds; 1 the next list is finished by k_sng_finish;
+                               // 2 finished (later rounds are empty)
 };
 
 // Output column zind of a problem is written.  Columns are counted in tiles
@@ -1860,7 +1862,8 @@ __global__ void k_bucket_scan(int *bk) {
 // ------------------------------------------------------------------------
 #define SNG_WARPS 8
 #define SNG_ROUNDS (MR3_MAXITER + 1)   // MAXITER loop calls and the step-2 call
-enum { SF_USEDBS = 1, SF_USEDRQ = 2, SF_NEEDBS = 4, SF_STEP2 = 8 };
+#define SNG_TILE_BYTES (SNG_WARPS * 32 * 33 * (int)sizeof(double))   // k_sng_round's z tiles
+enum { SF_USEDBS = 1, SF_USEDRQ = 2, SF_NEEDBS = 4, SF_STEP2 = 8, SF_REWRITE = 16 };
 
 // Loop variables of one singleton between rounds
 // (SRC/process_singleton.c:159-292: lambda, Wshifted[i], Werr[i], left,
@@ -1874,6 +1877,7 @@ __global__ void k_round_reset(SngCounters *sc, int in, int first) {
   sc->nin = first ? sc->n_sng : sc->act_n[in];
   sc->act_next[in] = 0;
   sc->bs_next = 0;
+  if (first) { sc->mode = 0; sc->fin_ctas = 0; }
 }
 
 // Stable compaction of a round's list: entry j of the list leaves the round
@@ -1948,7 +1952,7 @@ __global__ void __launch_bounds__(256) k_list_count(const SngCounters *sc,
 // Exclusive scan of the block counts (one block of 1024 threads); the totals
 // become the next list's length and the bisection list's length.
 __global__ void __launch_bounds__(1024) k_list_scan(int nblk, SngCounters *sc, int *bcnt, int out,
-                                                    int last_round) {
+                                                    int last_round, int finish_max) {
   __shared__ int wa[32], wb[32];
   __shared__ int carry[2];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -1984,6 +1988,9 @@ __global__ void __launch_bounds__(1024) k_list_scan(int nblk, SngCounters *sc, i
     sc->act_n[out] = carry[0];
     sc->bs_n = carry[1];
     if (last_round && (carry[0] | carry[1])) sc->err = 1;
+    // a short list is finished in one launch, a warp per singleton
+    const int left = carry[0] + carry[1];
+    if (!last_round && sc->mode == 0 && left > 0 && left <= finish_max) sc->mode = 1;
   }
 }
 
@@ -2041,6 +2048,7 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
   const int nin = sc->nin;
   const double rqtol = 2.0 * MR3_EPS;
   __shared__ SngState sm_st[SNG_WARPS * 32];
+  extern __shared__ double ztile[];   // SNG_WARPS tiles of 32 x 33 doubles
   unsigned long long w_r1v = 0, w_sweep = 0, w_chunks = 0;
   for (;;) {
     int base = 0;
@@ -2058,7 +2066,7 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
     const double2 *P, *Q;
     double *zcol;   // the eigenvector's column of Z at the block's first row
     int ps, r_in;
-    bool usedBS;
+    bool usedBS, write;
     {
       // the loop state waits in shared memory while the sweeps run, so that
       // they have the registers to themselves
@@ -2089,8 +2097,15 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
       sm_st[threadIdx.x] = st;
       usedBS = (st.flags & SF_USEDBS) != 0;
       lam_call = (st.flags & SF_STEP2) ? st.bstw : st.lambda;
-      r_in = st.r;
+      // a rewrite repeats the accepted first call (twist searched, r = 0)
+      r_in = (st.flags & SF_REWRITE) ? 0 : st.r;
       gaptol = st.gaptol;
+      // the first call of a Rayleigh-quotient iteration (no bisection
+      // before it) is practically never accepted: its eigenvalue carries
+      // the refinement's error, far above the acceptance test's tolerance.
+      // Its vector is not written; in the rare case that it is accepted,
+      // the next round repeats the identical call and writes the vector.
+      write = (st.flags & (SF_REWRITE | SF_STEP2 | SF_USEDBS)) || st.k > 1;
     }
     r1c_state rs;
     rs.r = 0; rs.mingma = 0.0; rs.sawnan = false; rs.slowA = false; rs.slowB = false;
@@ -2098,20 +2113,24 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
     dv_r1c_factor(active, nb, lam_call, P, Q, ps, pivmin, !usedBS, r_in, ck, &negc, &rs);
     dlar1v_out o;
     o.isupp1 = 1; o.isupp2 = nb; o.nrminv = 0.0; o.r = 0; o.resid = 0.0; o.rqcorr = 0.0;
-    // z of the support goes to the column unscaled; an accepted vector is
-    // scaled below (z * nrminv, the reference's dscal after dlar1v)
-    if (active)
-      dv_r1c_solve(nb, lam_call, P, Q, ps, pivmin, gaptol, rs.r, rs.sawnan, rs.slowA, rs.slowB,
-                   ck.S, ck.P, rs.mingma, zcol, 1.0, &o);
+    // z of the support goes to the column unscaled (through the warp's
+    // tile, in coalesced column segments); an accepted vector is scaled
+    // below (z * nrminv, the reference's dscal after dlar1v)
+    dv_r1w_solve(active, nb, lam_call, P, Q, ps, pivmin, gaptol, rs.r, rs.sawnan, rs.slowA,
+                 rs.slowB, ck.S, ck.P, rs.mingma, zcol, write, ztile + (threadIdx.x >> 5) * 32 * 33,
+                 &o);
     SngState st = sm_st[threadIdx.x];
     const bool step2 = (st.flags & SF_STEP2) != 0;
+    const bool rewrite = (st.flags & SF_REWRITE) != 0;
     const int nb_sweep = __reduce_max_sync(full, active ? nb : 0);
     if (lane == 0) { w_chunks++; w_sweep += nb_sweep; }
     bool done = false, tobs = false;
     if (active) {
       w_r1v += nb;
       st.r = o.r;
-      if (step2) {
+      if (rewrite) {
+        done = true;   // the decision was taken in the round before
+      } else if (step2) {
         st.lambda = st.bstw;
         done = true;
       } else {
@@ -2138,8 +2157,10 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
         if (!more) {
           if ((st.flags & SF_USEDRQ) && (st.flags & SF_USEDBS) && st.bstres <= st.resid)
             st.flags |= SF_STEP2;
-          else
+          else if (write)
             done = true;
+          else
+            st.flags |= SF_REWRITE;   // accepted, vector not written yet
         } else if (st.flags & SF_NEEDBS) {
           tobs = true;
         }
@@ -2250,6 +2271,164 @@ k_sng_bisect(int out, const SngDev *sng, const ClusterDev *cl, const ProbDev *pr
     __syncwarp();
   }
   stat_add(stats, KID_SNG * 4 + 1, w_neg);
+}
+
+// The rest of a level's singletons when few are left (SngCounters.mode 1):
+// one warp per singleton runs its remaining Rayleigh-quotient loop
+// (SRC/process_singleton.c:159-292) to the end in one launch -- dlar1v on
+// lane 0 (the warp's lane-0 checkpoints), a bisection by all 32 lanes with
+// the tree bisection -- instead of one call per round with a launch
+// sequence (round, compaction, bisection, sort) between calls.  Every call
+// and every state update is the one the rounds make, so the results are the
+// same bits.  The last block to finish empties the list (mode 2).
+__global__ void __launch_bounds__(SNG_WARPS * 32, 2)
+k_sng_finish(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
+             const BlockDev *blocks, const double2 *RP, const double2 *RQ, const double *arena,
+             double *W, double *Wsh, double *Werr, double *Wgap, const int *Windex,
+             const int *Zindex, SngState *sst, const int *act0, const int *act1, SngCounters *sc,
+             double *scratch, long long nmax, int2 *done_list, int *tile_left,
+             unsigned long long *stats) {
+  if (sc->mode != 1) return;
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nck = nmax / CK_K + 1;
+  r1c_ck ck;
+  ck.S = scratch + gw * 3 * nck * 32 + lane;
+  ck.I = ck.S + nck * 32;
+  ck.P = ck.I + nck * 32;
+  const int *Ain = in ? act1 : act0;
+  const int nin = sc->nin;
+  const double rqtol = 2.0 * MR3_EPS;
+  unsigned long long w_r1v = 0, w_neg = 0;
+  for (;;) {
+    int j = 0;
+    if (lane == 0) j = atomicAdd(&sc->act_next[in], 1);
+    j = __shfl_sync(full, j, 0);
+    if (j >= nin) break;
+    const int idx = Ain[j];
+    const SngDev S = sng[idx];
+    const int s = S.slot;
+    const ClusterDev C = cl[S.cl];
+    const BlockDev &B = blocks[C.blk];
+    ProbDev *p = &probs[B.prob];
+    const int nb = B.nbl;
+    const double pivmin = p->pivmin;
+    const double2 *P, *Q;
+    int ps;
+    own_rrr(C, B, RP, RQ, arena, &P, &Q, &ps);
+    double *zcol = p->Z + (size_t)Zindex[s] * p->ldz + (B.ibgn - p->off);
+    const int wi = Windex[s];
+    SngState st = sst[idx];   // identical in every lane
+    dlar1v_out o;
+    for (;;) {
+      // the bisection a round would have sent this singleton to (a second
+      // step or a rewrite follows the loop's end: no bisection then)
+      if ((st.flags & SF_NEEDBS) && !(st.flags & (SF_STEP2 | SF_REWRITE))) {
+        const int maxitr = dv_itmax(C.bl_spdiam + pivmin, pivmin);
+        const int tw = (st.r < 1 || st.r > nb) ? nb : st.r;
+        int nc = 0;
+        dv_dlarrb_tree(32, nb, P, ps, wi, 1, 0, 0.0, 0.0, 0.0, 2.0 * MR3_EPS, pivmin, maxitr, tw,
+                       &st.wsh, &st.werr, &nc);
+        st.flags = (st.flags | SF_USEDBS) & ~SF_NEEDBS;
+        st.lambda = st.wsh;
+        st.r = 0;
+        if (lane == 0) w_neg += (unsigned long long)nc * nb;
+      }
+      const bool usedBS = (st.flags & SF_USEDBS) != 0;
+      const double lam_call = (st.flags & SF_STEP2) ? st.bstw : st.lambda;
+      const int r_in = (st.flags & SF_REWRITE) ? 0 : st.r;
+      const bool write = (st.flags & (SF_REWRITE | SF_STEP2 | SF_USEDBS)) || st.k > 1;
+      r1c_state rs;
+      rs.r = 0; rs.mingma = 0.0; rs.sawnan = false; rs.slowA = false; rs.slowB = false;
+      int negc = 0;
+      dv_r1c_factor(lane == 0, nb, lam_call, P, Q, ps, pivmin, !usedBS, r_in, ck, &negc, &rs);
+      o.isupp1 = 1; o.isupp2 = nb; o.nrminv = 0.0; o.r = 0; o.resid = 0.0; o.rqcorr = 0.0;
+      if (lane == 0)
+        dv_r1c_solve(nb, lam_call, P, Q, ps, pivmin, st.gaptol, rs.r, rs.sawnan, rs.slowA,
+                     rs.slowB, ck.S, ck.P, rs.mingma, write ? zcol : nullptr, 1.0, &o);
+      o.r = __shfl_sync(full, o.r, 0);
+      o.isupp1 = __shfl_sync(full, o.isupp1, 0);
+      o.isupp2 = __shfl_sync(full, o.isupp2, 0);
+      o.nrminv = __shfl_sync(full, o.nrminv, 0);
+      o.resid = __shfl_sync(full, o.resid, 0);
+      o.rqcorr = __shfl_sync(full, o.rqcorr, 0);
+      negc = __shfl_sync(full, negc, 0);
+      if (lane == 0) w_r1v += nb;
+      // the state update of k_sng_round, in every lane
+      bool done = false;
+      const bool step2 = (st.flags & SF_STEP2) != 0;
+      st.r = o.r;
+      if (st.flags & SF_REWRITE) {
+        done = true;
+      } else if (step2) {
+        st.lambda = st.bstw;
+        done = true;
+      } else {
+        const double tolr = 4.0 * dv_log((double)nb) * MR3_EPS;
+        st.resid = o.resid;
+        if (st.k == 1 || o.resid < st.bstres) { st.bstres = o.resid; st.bstw = st.lambda; }
+        bool more = false;
+        if (!usedBS && o.resid > tolr * st.gap && fabs(o.rqcorr) > rqtol * fabs(st.lambda)) {
+          const int sgndef = (wi <= negc) ? -1 : 1;
+          if (o.rqcorr * sgndef >= 0.0 && st.lambda + o.rqcorr <= st.right &&
+              st.lambda + o.rqcorr >= st.left) {
+            st.flags |= SF_USEDRQ;
+            if (sgndef == 1) st.left = st.lambda; else st.right = st.lambda;
+            st.wsh = 0.5 * (st.left + st.right);
+            st.lambda += o.rqcorr;
+          } else {
+            st.flags |= SF_NEEDBS;
+          }
+          if (st.right - st.left < rqtol * fabs(st.lambda)) st.flags |= SF_USEDBS;
+          else if (st.k == MR3_MAXITER - 1) st.flags |= SF_NEEDBS;
+          st.k++;
+          more = (st.k <= MR3_MAXITER);
+        }
+        if (!more) {
+          if ((st.flags & SF_USEDRQ) && (st.flags & SF_USEDBS) && st.bstres <= st.resid)
+            st.flags |= SF_STEP2;
+          else if (write)
+            done = true;
+          else
+            st.flags |= SF_REWRITE;
+        }
+      }
+      if (done) break;
+    }
+    // outputs and the finished column (support scaled, the rest zero)
+    const int bl0 = B.ibgn - p->off;
+    const int zind = Zindex[s];
+    if (lane == 0) {
+      Wsh[s] = st.lambda;
+      Werr[s] = st.werr;
+      Wgap[s] = st.gap;
+      W[s] = st.lambda + C.sigma;
+      p->Zsupp[2 * (size_t)zind] = o.isupp1 + bl0;
+      p->Zsupp[2 * (size_t)zind + 1] = o.isupp2 + bl0;
+    }
+    const int a = bl0 + o.isupp1 - 1, b = bl0 + o.isupp2;
+    double *Zc = p->Z + (size_t)zind * p->ldz;
+    __syncwarp();
+    for (int row = lane; row < a; row += 32) Zc[row] = 0.0;
+    for (int row = a + lane; row < b; row += 32) Zc[row] = Zc[row] * o.nrminv;
+    for (int row = b + lane; row < p->n; row += 32) Zc[row] = 0.0;
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence();
+      column_done(p, B.prob, zind, sc, done_list, tile_left);
+    }
+  }
+  stat_add(stats, KID_SNG * 4 + 2, w_r1v);
+  stat_add(stats, KID_SNG * 4 + 1, w_neg);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&sc->fin_ctas, 1) == (int)gridDim.x - 1) {
+      sc->nin = 0;
+      sc->mode = 2;
+    }
+  }
 }
 
 // Unit vectors of 1x1 blocks (SRC/process_singleton.c:125-133).
@@ -2596,8 +2775,15 @@ extern "C" int mr3_cuda_ctx_create_prio(int device, int high, mr3_cuda_ctx **out
     return MR3_EMISC;
   }
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_sng_round<false>, SNG_WARPS * 32, 0) ==
-          cudaSuccess &&
+  if (cudaFuncSetAttribute(k_sng_round<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           SNG_TILE_BYTES) != cudaSuccess ||
+      cudaFuncSetAttribute(k_sng_round<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           SNG_TILE_BYTES) != cudaSuccess) {
+    mr3_cuda_ctx_destroy(c);
+    return MR3_EMISC;
+  }
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_sng_round<false>, SNG_WARPS * 32,
+                                                    SNG_TILE_BYTES) == cudaSuccess &&
       nb > 0)
     c->sng_ctas_per_sm = nb;
   c->h_const[0] = 1.0;
@@ -3176,12 +3362,21 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
         const int nsng = c->h_sc->n_sng;
         const int ctas_all = (int)(nwarps / SNG_WARPS);
         const int ctas_first = std::min(ctas_all, (nsng + 32 * SNG_WARPS - 1) / (32 * SNG_WARPS));
-        const size_t smem = 0;
+        const size_t smem = SNG_TILE_BYTES;
         const int bis_ctas = c->nsm * 4;
         const int nblk = (nsng + LIST_T - 1) / LIST_T;
+        // a list of at most this many singletons is finished in one launch
+        // (k_sng_finish), a warp each; MR3_FINISH_MAX overrides it (0: never)
+        int finish_max = (int)nwarps;
+        if (const char *ev = getenv("MR3_FINISH_MAX")) finish_max = atoi(ev);
         for (int rd = 0; rd < SNG_ROUNDS; rd++) {
           const int in = rd & 1, last = rd == SNG_ROUNDS - 1;
           LAUNCH(k_round_reset, 1, 1, c->sc, in, rd == 0);
+          if (rd > 0)
+            LAUNCH(k_sng_finish, ctas_all, SNG_WARPS * 32, in, c->sng, c->cl[cur], c->probs,
+                   c->blocks, c->RP, c->RQ, c->arena[cur], c->W, c->Wsh, c->Werr, c->Wgap,
+                   c->Windex, c->Zindex, c->sst, c->act[0], c->act[1], c->sc, c->scratch,
+                   (long long)nmaxV, c->done_list, c->tile_left, stats);
           if (rd == 0)
             LAUNCH_SMEM(k_sng_round<true>, ctas_first, SNG_WARPS * 32, smem, in, c->sng,
                         c->cl[cur], c->probs, c->blocks, c->RP, c->RQ, c->arena[cur], c->W, c->Wsh,
@@ -3201,7 +3396,7 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
             npend++;
           }
           LAUNCH(k_list_count, nblk, 256, c->sc, c->sflag, c->sbcnt);
-          LAUNCH(k_list_scan, 1, 1024, nblk, c->sc, c->sbcnt, in ^ 1, last);
+          LAUNCH(k_list_scan, 1, 1024, nblk, c->sc, c->sbcnt, in ^ 1, last, finish_max);
           LAUNCH(k_list_scatter, nblk, 256, rd == 0, c->sc, c->sflag, c->sbcnt, c->act[0],
                  c->act[1], in, c->bsl);
           if (!last) {

@@ -7,8 +7,11 @@ entry point, whose scratch is a static device array of the library.  This
 test feeds it the root representation and the eigenvalues that mrrr() (the
 existing entry point) returns for matrices whose eigenvalues are all
 singletons of the root, and checks, on two calls in a row, that its vectors
-agree with mrrr()'s within the tolerance the parity tests use.  It lives in
-its own file, collected last, and passes alone or after the other tests.
+agree with mrrr()'s within the tolerance the parity tests use; it also checks
+n = 1 and, against the oracle's dlar1v bit for bit, a shift that makes a
+pivot exactly zero (the NaN-safe sweeps) with the pivot threshold the entry
+point derives from the representation.  It lives in its own file, collected
+last, and passes alone or after the other tests.
 """
 import ctypes as C
 
@@ -16,6 +19,7 @@ import numpy as np
 import pytest
 
 import mr3smp_b200 as M
+import oracle
 from conftest import EPS, tnorm
 from mr3smp_b200 import workloads as wl
 
@@ -88,3 +92,71 @@ def test_noalloc_rejects_sizes_beyond_the_limit():
                                    C.c_void_p(t.data_ptr()), C.c_double(0.0),
                                    C.c_void_p(t.data_ptr()), n, C.c_void_p(t.data_ptr()), None)
     assert rc == 1
+
+
+def _setup(L):
+    L.mr3_cuda_eigvec_noalloc.restype = C.c_int
+    L.mr3_cuda_eigvec_noalloc.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                          C.c_double, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+
+
+def test_noalloc_n1_unit_vectors():
+    import torch
+    L = M.lib()
+    _setup(L)
+    dev = torch.device("cuda")
+    D = torch.tensor([0.7], dtype=torch.float64, device=dev)
+    lam = torch.tensor([0.7, 0.7], dtype=torch.float64, device=dev)
+    Z = torch.full((6,), np.nan, dtype=torch.float64, device=dev)
+    Zs = torch.zeros(4, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream().cuda_stream
+    rc = _call(L, 1, D, D, 2, lam, 0.0, Z, 3, Zs, stream)
+    torch.cuda.synchronize()
+    assert rc == 0
+    assert Z.cpu().numpy()[0] == 1.0 and Z.cpu().numpy()[3] == 1.0
+    assert Zs.cpu().numpy().tolist() == [1, 1, 1, 1]
+
+
+def test_noalloc_zero_pivot_matches_oracle_dlar1v():
+    """lambda = D(1) makes the first stationary pivot exactly zero, so the
+    sweeps rerun with the NaN-safe formulas; the vector, its support and the
+    twist must be the oracle's dlar1v with the same pivot threshold."""
+    import torch
+    L = M.lib()
+    _setup(L)
+    OL = oracle.lib()
+    n = 60
+    rng = np.random.default_rng(4)
+    d = rng.uniform(0.5, 2.0, n)
+    l = rng.uniform(-0.9, 0.9, n)
+    l[-1] = 0.0
+    ld = d * l
+    lld = ld * l
+    pivmin = 2.2250738585072014e-308 * max(1.0, float(np.max(np.abs(ld[: n - 1])) ** 2))
+    lams = np.array([d[0], 0.5 * (d[3] + d[4])])
+    dev = torch.device("cuda")
+    Dd = torch.from_numpy(d).to(dev)
+    Ld = torch.from_numpy(l).to(dev)
+    lam = torch.from_numpy(lams).to(dev)
+    stream = torch.cuda.current_stream().cuda_stream
+    for call in range(2):
+        Z = torch.full((n * 2,), np.nan, dtype=torch.float64, device=dev)
+        Zs = torch.zeros(4, dtype=torch.int32, device=dev)
+        assert _call(L, n, Dd, Ld, 2, lam, 0.0, Z, n, Zs, stream) == 0
+        torch.cuda.synchronize()
+        Zn = Z.cpu().numpy().reshape(2, n)
+        Zsn = Zs.cpu().numpy()
+        for j, lm in enumerate(lams):
+            z = np.zeros(n)
+            isz = np.zeros(2, dtype=np.int32)
+            work = np.zeros(4 * n)
+            neg, r = C.c_int(), C.c_int(0)
+            ztz, mg, nr, rs, rq = (C.c_double() for _ in range(5))
+            OL.or_dlar1v(n, 1, n, float(lm), d, l, ld, lld, pivmin, 0.0, z, 0, C.byref(neg),
+                         C.byref(ztz), C.byref(mg), C.byref(r), isz, C.byref(nr), C.byref(rs),
+                         C.byref(rq), work)
+            want = np.zeros(n)
+            a, b = isz[0] - 1, isz[1]
+            want[a:b] = z[a:b] * nr.value
+            assert Zsn[2 * j] == isz[0] and Zsn[2 * j + 1] == isz[1], (call, j)
+            assert np.array_equal(Zn[j], want), (call, j, np.abs(Zn[j] - want).max())

@@ -487,6 +487,69 @@ print(json.dumps({"seconds": time.perf_counter() - t0, "info": r["info"], "m": r
 """
 
 
+def run_single(M, wl, which: str, hbm_gbs):
+    """One large solve on the device (arrays resident in HBM, CUDA events on
+    the solve's stream, after one warm-up solve): the 20010-row glued
+    Wilkinson matrix (30 blocks of W+ of size 667, glue 1e-12; jobz V,
+    range I, il = 1, iu = 10005) or the 40000-row matrix, half uniform
+    (-1, 1), half glued W+ blocks of size 401 with glue 1e-10 (jobz V, range
+    A; 12.8 GB of Z).  Reports seconds, eigenpairs/s, the residual and
+    orthogonality of the result, and the Z write against the HBM copy
+    bandwidth."""
+    import torch
+    if which == "c2":
+        D, E = wl.glued_wilkinson(30, 667, 1e-12)
+        n = len(D)
+        rng, il, iu = 3, 1, n // 2
+    else:
+        D, E = wl.large_mixed(40000)
+        n = len(D)
+        rng, il, iu = 1, 1, n
+    m = iu - il + 1
+    dev = "cuda"
+    D0 = torch.tensor(D, device=dev)
+    E0 = torch.tensor(E, device=dev)
+    Dd, Ed = D0.clone(), E0.clone()
+    W = torch.zeros(n, dtype=torch.float64, device=dev)
+    Z = torch.empty(n * m, dtype=torch.float64, device=dev)
+    Zs = torch.zeros(2 * n, dtype=torch.int32, device=dev)
+    rec = (M.CudaProb * 1)()
+    q = rec[0]
+    q.n, q.jobz, q.range, q.il, q.iu, q.tryrac, q.ldz = n, 1, rng, il, iu, 0, n
+    q.D, q.E, q.W, q.Z, q.Zsupp = (Dd.data_ptr(), Ed.data_ptr(), W.data_ptr(), Z.data_ptr(),
+                                   Zs.data_ptr())
+    S = M.Solver(torch.cuda.current_device())
+    st = torch.cuda.current_stream()
+    times = []
+    for _ in range(2):   # warm-up, then the timed solve
+        Dd.copy_(D0)
+        Ed.copy_(E0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        S.solve(rec, st.cuda_stream)
+        e1.record(st)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) * 1e-3)
+    sec = times[-1]
+    from mr3smp_b200.workloads import residual_orth_torch
+    ok = rec[0].info == 0 and rec[0].m == m
+    res, orth = residual_orth_torch(D, E, W[:m].cpu().numpy(), Z.view(m, n).T)
+    zb = 8.0 * n * m
+    out = {"workload": ("glued W+ 30x667 (glue 1e-12), n=20010, jobz=V range=I 1..10005"
+                        if which == "c2" else
+                        "n=40000: half U(-1,1), half glued W+ 401 (glue 1e-10), jobz=V range=A"),
+           "seconds": sec, "eigenpairs_per_s": m / sec, "ok": bool(ok),
+           "resid": res, "orth": orth, "z_bytes": zb,
+           "z_write_gbs": zb / sec * 1e-9,
+           "z_write_frac_of_hbm": (zb / sec * 1e-9 / hbm_gbs) if hbm_gbs else None,
+           "api": "mr3_cuda_solve, arrays resident in HBM, CUDA events"}
+    S.close()
+    del Z, W
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_dense(M, n, seed, with_ref):
     """The dense driver dsyeig (SRC/dense.c:151-232) on a seeded n x n
     symmetric matrix, entries U(-1, 1): wall time through the C ABI from host
@@ -550,6 +613,8 @@ def main():
                     help="requests per serving stream")
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-large", action="store_true",
+                    help="skip the single 20010-row and 40000-row solves")
     ap.add_argument("--dense", type=int, default=0,
                     help="also time the dense driver dsyeig on an n x n symmetric matrix "
                          "(and the reference's on the host cores); 0 = off")
@@ -712,6 +777,11 @@ def main():
     del T, recs
     torch.cuda.empty_cache()
 
+    large = None
+    if rank == 0 and not args.no_large:
+        hbm = peaks.get("hbm_gbs")
+        large = {"c2": run_single(M, wl, "c2", hbm), "c5": run_single(M, wl, "c5", hbm)}
+
     serving = None
     if rank == 0 and not args.no_serve:
         rates = [float(x) for x in args.serve_rates.split(",") if x]
@@ -799,7 +869,7 @@ def main():
         "fp64_peaks": {"fma_tflops": fma_tflops, "div_gops": div_gops},
         "top_kernels_ms_per_step": {k: round(v, 2) for k, v in top},
         "detail_file": detail_path,
-        "roofline_hbm": roof_hbm, "percall": percall, "serving": serving,
+        "roofline_hbm": roof_hbm, "large": large, "percall": percall, "serving": serving,
     }
     print(json.dumps(out))
     return 0

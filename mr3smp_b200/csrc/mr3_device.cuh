@@ -694,7 +694,7 @@ static __device__ __noinline__ double dv_r1v_passB(bool active, int n, double la
           if (slow && tmp == 0.0) pn = cpx[u] - lambda;
           Y[(size_t)i * R1V_LD] = um;
           p = pn;
-          if (SEARCH && i > r1 && i <= r2) {   // candidate r = i: S(i-1) + P(i-1)
+          if (i > r1 && i <= r2) {        // candidate r = i: S(i-1) + P(i-1)
             const double sprev = csp[u];
             double c = sprev + p;
             if (c == 0.0) c = eps * sprev;
@@ -914,6 +914,12 @@ static __device__ __noinline__ void dv_r1v_solve(bool active, int n, const doubl
 #ifndef CK_K
 #define CK_K 4
 #endif
+// 1: the progressive sweep double-buffers the next block's rows in
+// registers; 0: it loads a block's rows when it reaches it, prefetched into
+// L1 two blocks ahead (fewer registers)
+#ifndef MR3_PROGR_DB
+#define MR3_PROGR_DB 1
+#endif
 
 // One lane's checkpoints; element j of each array at [j * 32].
 struct r1c_ck {
@@ -1054,12 +1060,28 @@ static __device__ __noinline__ double dv_r1c_progr(bool active, int n, double la
         }
       }
     };
+#if MR3_PROGR_DB
     load(jtop, cp, cq);
+#endif
     for (int jb = jtop; jb >= jbot; jb--) {
+#if MR3_PROGR_DB
       if (jb - 1 >= jbot) {
         load(jb - 1, np_, nq);
         if (work && search) { nckS = ckS[(size_t)(jb - 1) * 32]; nckI = ckI[(size_t)(jb - 1) * 32]; }
       }
+#else
+      // rows loaded at the block (L1 hits: prefetched two blocks ahead)
+      load(jb, cp, cq);
+      if (work && search) { ckSv = ckS[(size_t)jb * 32]; ckIv = ckI[(size_t)jb * 32]; }
+      if (work && jb - 2 >= jbot) {
+        const int b2 = (jb - 2) * CK_K + 1;
+#pragma unroll
+        for (int u = 0; u < CK_K; u += 2) {
+          pf_l1(&P[(size_t)(b2 + u - 1) * ps]);
+          if (SEARCH && search) pf_l1(&Q[(size_t)(b2 + u - 1) * ps]);
+        }
+      }
+#endif
       const int base = jb * CK_K + 1;
       const int hi = d_imin(base + CK_K - 1, top), lo = d_imax(base, r1);
       const bool bw = work && lo <= hi;
@@ -1096,7 +1118,7 @@ static __device__ __noinline__ double dv_r1c_progr(bool active, int n, double la
           double pn = p * tmp - lambda;
           if (SLOW && tmp == 0.0) pn = cp[u].x - lambda;
           p = pn;
-          if (i > r1 && i <= r2) {        // candidate r = i: S(i-1) + P(i-1)
+          if (SEARCH && i > r1 && i <= r2) {   // candidate r = i: S(i-1) + P(i-1)
             const double sprev = sia[u];
             double c = sprev + p;
             if (c == 0.0) c = eps * sprev;
@@ -1104,13 +1126,15 @@ static __device__ __noinline__ double dv_r1c_progr(bool active, int n, double la
           }
         }
       }
-#pragma unroll
+#if MR3_PROGR_DB
+      #pragma unroll
       for (int u = 0; u < CK_K; u++) {
         cp[u] = np_[u];
         if (SEARCH) cq[u] = nq[u];
       }
       ckSv = nckS;
       ckIv = nckI;
+#endif
     }
   }
   *neg2o = neg2;

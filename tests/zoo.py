@@ -65,4 +65,15 @@ def medium_zoo():
     cases.append(("121_2000", D, E, "V", "A", {}))
     D, E = wl.large_mixed(3000, seed=5, bs=101)
     cases.append(("large_mixed3000", D, E, "V", "A", {}))
+    # high relative accuracy at scale: a matrix graded over 280 decades whose
+    # relative off-diagonals (1/3 each) pass dlarrr, so tryrac survives and
+    # dlarrj refines every eigenvalue (SRC/mrrr.c:452-520)
+    g = 10.0 ** (-np.arange(2000) * (280.0 / 2000))
+    Dg, Eg = 3.0 * g, np.r_[np.sqrt(g[:-1] * g[1:]), 0.0]
+    cases.append(("graded2000_tryrac_V_A", Dg, Eg, "V", "A", dict(tryrac=1)))
+    cases.append(("graded2000_tryrac_N_I", Dg, Eg, "N", "I", dict(il=100, iu=1900, tryrac=1)))
+    # range V and its count at scale
+    D, E = wl.uniform(3000, seed=12)
+    cases.append(("uniform3000_V_V", D, E, "V", "V", dict(vl=-0.7, vu=1.3)))
+    cases.append(("uniform3000_C_V", D, E, "C", "V", dict(vl=-0.7, vu=1.3)))
     return cases

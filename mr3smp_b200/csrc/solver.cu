@@ -42,6 +42,7 @@ struct ProbDev {
   // state and outputs
   int status, m, nvals, nsplit, irange, nwl, nwu, il_out, iu_out, tryrac_out, trivial;
   int zleft;                    // eigenvector columns not yet written
+  int force_bis;                // the reference's route choice forces bisection
   int tbase;                    // first column tile in the tile counters (-1: none)
   double scale, pivmin, spdiam, tnorm, gl, gu, wl, wu, wlu, wul, vl_out, vu_out, split;
 };
@@ -54,6 +55,7 @@ struct BlockDev {
   double gl3, gu3, atoli;       // dlarrd bisection start and abstol
   double wlu, wul;              // dlarrd discard thresholds
   double sigma, spdiam, bl_spdiam;
+  int dqds, sgndef;             // eigenvalues by dqds; sign of the root's definiteness
 };
 
 // A cluster of one level.  Sibling clusters (children of one parent, hence
@@ -129,6 +131,7 @@ __global__ void k_export(const LevelCounters *lc, LevelCounters *hlc, SngCounter
 
 struct Tol {
   double rtol1, rtol2, bsrtol, rqtol;
+  int nthreads;                 // thread count of the reference's route choice
 };
 
 // ------------------------------------------------------------------------
@@ -404,6 +407,8 @@ k_prologue(ProbDev *probs, BlockDev *blocks, int *blk_of_row, double *D, double 
   if (tid == 0) {
     p->nvals = p->iu_out - p->il_out + 1;
     p->m = p->nvals;
+    // SRC/mrrr_val.c:279-282: bisection unless few threads per eigenvalue
+    p->force_bis = (double)tol.nthreads > ceil(12.0 * p->nvals / (double)n);
     if (irange == MR3_RANGE_V) { p->wl = p->vl; p->wu = p->vu; p->vl_out = p->vl; p->vu_out = p->vu; }
     if (irange == MR3_RANGE_A) { p->wl = p->gl; p->wu = p->gu; p->vl_out = p->gl; p->vu_out = p->gu; }
   }
@@ -682,10 +687,16 @@ k_bis_roots(int N, const ProbDev *probs, const BlockDev *blocks, const int *blk_
 // One level: a Sturm count per node; done and single children written out,
 // the number of next-level children per CTA in bcnt.
 __global__ void __launch_bounds__(256)
-k_bis_count(const BisNode *in, int n_in, const ProbDev *probs, const BlockDev *blocks,
+k_bis_count(const BisNode *in, const int *n_in_dev, const ProbDev *probs, const BlockDev *blocks,
             const double2 *TP, Tol tol, int *ccnt, int *bcnt, double *Wt, double *Et, int *It,
             BisState *st, unsigned long long *stats) {
   __shared__ int sint[32];
+  // the level's length is on the device (the grid covers its bound, N/2)
+  const int n_in = *n_in_dev;
+  if (blockIdx.x * blockDim.x >= n_in) {
+    if (threadIdx.x == 0) bcnt[blockIdx.x] = 0;
+    return;
+  }
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   int nnext = 0;
   unsigned long long work = 0;
@@ -736,10 +747,12 @@ __global__ void __launch_bounds__(1024) k_bis_scan(int nblk, int *bcnt, int *n_o
 // stay together).  split: the depth limit is reached and the nodes' eigenvalues
 // leave the tree as single states instead.
 __global__ void __launch_bounds__(256)
-k_bis_scatter(const BisNode *in, int n_in, const ProbDev *probs, const BlockDev *blocks, Tol tol,
-              const int *ccnt, const int *bcnt, BisNode *out, int split, double *Wt, double *Et,
-              int *It, BisState *st) {
+k_bis_scatter(const BisNode *in, const int *n_in_dev, const ProbDev *probs, const BlockDev *blocks,
+              Tol tol, const int *ccnt, const int *bcnt, BisNode *out, int split, double *Wt,
+              double *Et, int *It, BisState *st) {
   __shared__ int sint[32];
+  const int n_in = *n_in_dev;
+  if (blockIdx.x * blockDim.x >= n_in) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   BisNode ch[2];
   int kind[2] = {0, 0}, nnext = 0;
@@ -931,12 +944,30 @@ k_root(ProbDev *probs, BlockDev *blocks, double *D, double *E, const double2 *TP
     if (nbl < 2 || mbl <= 0) continue;
     const int wbgn = B->wbgn, wend = wbgn + mbl - 1;
     const double gl = B->bgl, gu = B->bgu;
-    double isleft = fmax(gl, (W[wbgn] - Werr[wbgn]) - 100.0 * MR3_EPS * fabs(W[wbgn] - Werr[wbgn]));
-    double isright = fmin(gu, (W[wend] + Werr[wend]) + 100.0 * MR3_EPS * fabs(W[wend] - Werr[wend]));
-    double spdiam = gu - gl;
-    double tmp0 = fmin(isright, vup) - fmax(isleft, vlp);
-    double s1 = fmax(isleft, vlp) + 0.25 * tmp0;
-    double s2 = fmin(isright, vup) - 0.25 * tmp0;
+    // the dqds route (SRC/mrrr_val.c:409-412, 758-781): extremal eigenvalues
+    // by dlarrk (lanes 0 and 1), quarter points of [isleft, isright]
+    const bool dqds = mbl > 0.5 * nbl && !p->force_bis;
+    const bool allno = p->irange == MR3_RANGE_A && !p->force_bis;
+    double isleft, isright, spdiam, s1, s2;
+    if (dqds || allno) {
+      double w = 0.0, we = 0.0;
+      if (lane < 2)
+        dv_dlarrk(nbl, lane == 0 ? 1 : nbl, gl, gu, TP + ibgn, pivmin, sqrt(MR3_EPS), &w, &we);
+      const double w0 = __shfl_sync(0xffffffffu, w, 0), e0 = __shfl_sync(0xffffffffu, we, 0);
+      const double w1 = __shfl_sync(0xffffffffu, w, 1), e1 = __shfl_sync(0xffffffffu, we, 1);
+      isleft = fmax(gl, (w0 - e0) - 100.0 * MR3_EPS * fabs(w0 - e0));
+      isright = fmin(gu, (w1 + e1) + 100.0 * MR3_EPS * fabs(w1 + e1));
+      spdiam = isright - isleft;
+      s1 = isleft + 0.25 * spdiam;
+      s2 = isright - 0.25 * spdiam;
+    } else {
+      isleft = fmax(gl, (W[wbgn] - Werr[wbgn]) - 100.0 * MR3_EPS * fabs(W[wbgn] - Werr[wbgn]));
+      isright = fmin(gu, (W[wend] + Werr[wend]) + 100.0 * MR3_EPS * fabs(W[wend] - Werr[wend]));
+      spdiam = gu - gl;
+      const double tmp0 = fmin(isright, vup) - fmax(isleft, vlp);
+      s1 = fmax(isleft, vlp) + 0.25 * tmp0;
+      s2 = fmin(isright, vup) - 0.25 * tmp0;
+    }
     int cnt = 0;
     if (mbl > 1 && lane < 2) {   // dlarrc('T'): lane 0 counts at s1, lane 1 at s2
       const double x = (lane == 0) ? s1 : s2;
@@ -956,10 +987,18 @@ k_root(ProbDev *probs, BlockDev *blocks, double *D, double *E, const double2 *TP
     if (lane == 0) {
       int sgndef;
       if (mbl == 1) { sigma = gl; sgndef = 1; }
-      else if ((lcnt - B->ilow) >= (B->iupp - rcnt)) { sigma = fmax(isleft, vlp); sgndef = 1; }
-      else { sigma = fmin(isright, vup); sgndef = -1; }
+      else if ((lcnt - B->ilow) >= (B->iupp - rcnt)) {
+        sigma = allno ? fmax(isleft, gl) : (dqds ? isleft : fmax(isleft, vlp));
+        sgndef = 1;
+      } else {
+        sigma = allno ? fmin(isright, gu) : (dqds ? isright : fmin(isright, vup));
+        sgndef = -1;
+      }
       double tau;
-      if (mbl > 1) {
+      if (dqds) {
+        tau = spdiam * MR3_EPS * nbl + 2.0 * pivmin;
+        tau = fmax(tau, 2 * MR3_EPS * fabs(sigma));
+      } else if (mbl > 1) {
         double clwdth = W[wend] + Werr[wend] - W[wbgn] - Werr[wbgn];
         double avgap = fabs(clwdth / (double)(wend - wbgn));
         if (sgndef > 0) { tau = fmax(Wgap[wbgn], avgap); tau *= 0.5; tau = fmax(tau, Werr[wbgn]); }
@@ -983,6 +1022,9 @@ k_root(ProbDev *probs, BlockDev *blocks, double *D, double *E, const double2 *TP
           dmax = fmax(dmax, fabs(dpiv));
         }
         bool norep = dmax > MR3_MAX_GROWTH * spdiam;
+        if (dqds && !norep)   // dqds needs a definite representation
+          for (int i = 0; i < nbl; i++)
+            if (sgndef * Dt[ibgn + i] < 0.0) norep = true;
         if (!norep) { ok = 1; break; }
         if (jtry == MR3_MAX_TRY_ROOT - 2) {
           if (sgndef == 1) sigma = gl - 2.0 * spdiam * MR3_EPS * nbl - 2.0 * 2.0 * pivmin;
@@ -997,6 +1039,8 @@ k_root(ProbDev *probs, BlockDev *blocks, double *D, double *E, const double2 *TP
       if (!ok) set_status(p, MR3_EMISC);
       B->sigma = sigma;
       B->spdiam = spdiam;
+      B->dqds = dqds;
+      B->sgndef = sgndef;
     }
     ok = __shfl_sync(0xffffffffu, ok, 0);
     sigma = __shfl_sync(0xffffffffu, sigma, 0);
@@ -1042,7 +1086,7 @@ __device__ __forceinline__ unsigned long long refine_root_body(int s, const Prob
   if (iblk[s] < 0) return 0;
   const BlockDev *B = &blocks[iblk[s]];
   const ProbDev *p = &probs[B->prob];
-  if (p->status || B->nbl < 2) return 0;
+  if (p->status || B->nbl < 2 || B->dqds) return 0;
   const bool onlyW = (p->jobz == MR3_JOB_N);   // rtol1 = rtol2 = 4 eps (SRC/mrrr.c:230-232)
   const int II = s - B->wbgn + 1;
   const int i = B->ilow + II - 1;
@@ -1076,7 +1120,7 @@ k_refine_root(int N, int L, const ProbDev *probs, const BlockDev *blocks, const 
     const bool ok = iblk[s] >= 0;
     const BlockDev *B = ok ? &blocks[iblk[s]] : nullptr;
     const ProbDev *p = ok ? &probs[B->prob] : nullptr;
-    if (ok && !p->status && B->nbl >= 2) {
+    if (ok && !p->status && B->nbl >= 2 && !B->dqds) {
       const bool onlyW = (p->jobz == MR3_JOB_N);
       const int II = s - B->wbgn + 1;
       const int i = B->ilow + II - 1;
@@ -1102,6 +1146,37 @@ k_refine_root(int N, int L, const ProbDev *probs, const BlockDev *blocks, const 
 
 // Final gaps of the root refinement (dlarrb loop 111) and the last gap of the
 // block (SRC/mrrr_val.c:1080-1082).
+// The eigenvalues of a dqds block (SRC/mrrr_val.c:459-506): one thread per
+// block builds the qd array of its definite root representation in qd
+// (4 doubles per row of the block), runs dqds, and writes the wanted ones,
+// shifted as the refined ones are, with Werr = 4 log(nbl) eps |W|.
+__global__ void k_dqds(int N, ProbDev *probs, const BlockDev *blocks, const int *blk_of_row,
+                       const double *D, const double *E, double *W, double *Werr, double *qd) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= N) return;
+  const BlockDev *B = &blocks[blk_of_row[g]];
+  if (g != B->ibgn || !B->dqds || B->nbl < 2 || B->mbl <= 0) return;
+  ProbDev *p = &probs[B->prob];
+  if (p->status || p->trivial || p->jobz == MR3_JOB_C) return;
+  const int nbl = B->nbl, ibgn = B->ibgn;
+  double *z = qd + 4 * (size_t)ibgn;
+  for (int i = 0; i < nbl - 1; i++) {
+    z[2 * i] = fabs(D[ibgn + i]);
+    z[2 * i + 1] = E[ibgn + i] * E[ibgn + i] * z[2 * i];
+  }
+  z[2 * (nbl - 1)] = fabs(D[B->iend]);
+  z[2 * (nbl - 1) + 1] = 0.0;
+  int info = 0;
+  dv_dlasq2(nbl, z, &info);
+  if (info != 0) { set_status(p, MR3_EMISC); return; }
+  const double rtol = 4.0 * dv_log((double)nbl) * MR3_EPS;
+  for (int i = B->ilow, je = B->wbgn; i <= B->iupp; i++, je++) {
+    const double w = B->sgndef > 0 ? z[nbl - i] : -z[i - 1];
+    W[je] = w;
+    Werr[je] = rtol * fabs(w);
+  }
+}
+
 __global__ void k_gaps_root(int N, const ProbDev *probs, const BlockDev *blocks, const int *iblk,
                             const double *W, const double *Werr, double *Wgap) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2581,6 +2656,7 @@ struct mr3_cuda_ctx {
   LevelCounters *lc = nullptr;
   SngCounters *sc = nullptr;
   double *scratch = nullptr, *arena[2] = {nullptr, nullptr};
+  double *qd = nullptr;                     // dqds arrays (4 doubles per row)
   const double **Din = nullptr, **Ein = nullptr;
   double **Wp = nullptr, **Dp = nullptr, **Ep = nullptr;
   // pinned host mirrors
@@ -2709,6 +2785,7 @@ static int ensure_rows(mr3_cuda_ctx *c, size_t N, size_t P) {
     CK(regrow(&c->bis_cnt, n / 2 + 1), "bis cnt");
     CK(regrow(&c->bis_bcnt, (n / 2 + 1) / 256 + 1), "bis bcnt");
     CK(regrow(&c->bis_st, n), "bis st");
+    CK(regrow(&c->qd, 4 * n), "qd");
     c->capN = n;
   }
   if (P > c->capP) {
@@ -2802,7 +2879,7 @@ extern "C" void mr3_cuda_ctx_destroy(mr3_cuda_ctx *c) {
                  c->Dt, c->Lt, c->Wout, c->gers, c->TP, c->TPc, c->RP, c->RQ, c->rec0, c->rec1,
                  c->cl[0], c->cl[1], c->sng, c->sst, c->act[0], c->act[1], c->bsl, c->sflag, c->sbcnt, c->rl, c->rl_n, c->sbk, c->done_list, c->tile_left,
                  c->bis_nodes[0], c->bis_nodes[1], c->bis_cnt, c->bis_bcnt, c->bis_n, c->bis_st, c->lc, c->sc, c->scratch, c->arena[0],
-                 c->cls_ns, c->cls_soff, c->cls_cbase, c->cls_abase,
+                 c->cls_ns, c->cls_soff, c->cls_cbase, c->cls_abase, c->qd,
                  c->arena[1], (void *)c->Din, (void *)c->Ein, c->Wp, c->Dp, c->Ep};
   for (void *q : dev)
     if (q) cudaFree(q);
@@ -3211,6 +3288,12 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
   tol.rtol2 = fmax(fmin(tol.rtol1 * 5.0E-3, 1e-3 * 5.0E-6), 4.0 * 2.220446049250313e-16);
   tol.bsrtol = fmin(1e-3 * 1.0E-2, sqrt(2.220446049250313e-16));
   tol.rqtol = 2.0 * 2.220446049250313e-16;
+  // the reference picks dqds over bisection when its thread count is low
+  // (SRC/mrrr_val.c:279-285); MR3_NTHREADS sets the count that choice sees,
+  // unset the GPU's parallelism, for which the reference bisects
+  tol.nthreads = 1 << 30;
+  if (const char *ev = getenv("MR3_NTHREADS"))
+    if (*ev) tol.nthreads = atoi(ev);
   const int gN = (NN + 255) / 256, gN128 = (NN + 127) / 128;
 
   // ---- stage A: eigenvalues
@@ -3227,21 +3310,19 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
       CK(cudaMemsetAsync(c->bis_n, 0, 2 * sizeof(int), st), "bis n");
       LAUNCH(k_bis_roots, gN, 256, NN, c->probs, c->blocks, c->blk_of_row, c->bis_nodes[0],
              c->bis_n, c->Wt, c->Et, c->It, c->bis_st);
-      CK(cudaMemcpyAsync(c->h_bisn, c->bis_n, sizeof(int), cudaMemcpyDeviceToHost, st), "bis n");
-      CK(cudaStreamSynchronize(st), "bis sync");
-      int nin = c->h_bisn[0], cur = 0;
-      for (int depth = 0; nin > 0; depth++) {
-        const int nb = (nin + 255) / 256, split = depth + 1 >= BIS_DEPTH;
-        LAUNCH(k_bis_count, nb, 256, c->bis_nodes[cur], nin, c->probs, c->blocks, c->TP, tol,
-               c->bis_cnt, c->bis_bcnt, c->Wt, c->Et, c->It, c->bis_st, stats);
-        if (!split) LAUNCH(k_bis_scan, 1, 1024, nb, c->bis_bcnt, c->bis_n + 1);
-        LAUNCH(k_bis_scatter, nb, 256, c->bis_nodes[cur], nin, c->probs, c->blocks, tol, c->bis_cnt,
-               c->bis_bcnt, c->bis_nodes[cur ^ 1], split, c->Wt, c->Et, c->It, c->bis_st);
-        if (split) break;
-        CK(cudaMemcpyAsync(c->h_bisn, c->bis_n + 1, sizeof(int), cudaMemcpyDeviceToHost, st),
-           "bis n");
-        CK(cudaStreamSynchronize(st), "bis sync");
-        nin = c->h_bisn[0];
+      // BIS_DEPTH levels without a host synchronisation: each level's length
+      // stays on the device (bis_n[level parity]); a node holds at least two
+      // eigenvalues, so no level exceeds N/2 nodes, the grid's bound
+      const int nbmax = (int)((N / 2 + 1 + 255) / 256);
+      int cur = 0;
+      for (int depth = 0; depth < BIS_DEPTH; depth++) {
+        const int split = depth + 1 >= BIS_DEPTH;
+        LAUNCH(k_bis_count, nbmax, 256, c->bis_nodes[cur], c->bis_n + cur, c->probs, c->blocks,
+               c->TP, tol, c->bis_cnt, c->bis_bcnt, c->Wt, c->Et, c->It, c->bis_st, stats);
+        if (!split) LAUNCH(k_bis_scan, 1, 1024, nbmax, c->bis_bcnt, c->bis_n + (cur ^ 1));
+        LAUNCH(k_bis_scatter, nbmax, 256, c->bis_nodes[cur], c->bis_n + cur, c->probs, c->blocks,
+               tol, c->bis_cnt, c->bis_bcnt, c->bis_nodes[cur ^ 1], split, c->Wt, c->Et, c->It,
+               c->bis_st);
         cur ^= 1;
       }
       LAUNCH(k_bisect_cont, gN128, 128, NN, c->probs, c->blocks, c->blk_of_row, c->TP, c->Wt,
@@ -3264,6 +3345,9 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
       LAUNCH(k_refine_root<true>, (int)(((long long)NN * Lr + 127) / 128), 128, NN, Lr, c->probs,
              c->blocks, c->iblk, c->RP, c->W, c->Werr, c->Wgap, tol, stats);
   }
+  if (tol.nthreads < (1 << 30))
+    LAUNCH(k_dqds, gN, 256, NN, c->probs, c->blocks, c->blk_of_row, c->D, c->E, c->W, c->Werr,
+           c->qd);
   LAUNCH(k_gaps_root, gN, 256, NN, c->probs, c->blocks, c->iblk, c->W, c->Werr, c->Wgap);
   LAUNCH(k_discard, (L + 127) / 128, 128, c->probs, L, c->blocks, c->W, c->Werr, c->Wgap,
          c->Windex, c->iblk, c->Wcopy);

@@ -961,34 +961,93 @@ typedef struct {
 
 /* compute_root_rrr, bisection branch: SRC/mrrr_val.c:717-948 with
  * allrng_no_bisec = useDQDS = false. */
-static int or_root_rrr(int ibgn, int iend, int wbgn, int wend, int ilow,
-                       int iupp, double gl, double gu, or_in_t *Ds,
-                       or_val_t *Ws, or_tol_t *tol, double *work,
+/* dlarrk (SRC/LAPACK/odrrk.f:120-161): the iw-th eigenvalue of T by
+ * bisection on [gl, gu] to relative tolerance reltol; w, werr. */
+static void or_dlarrk(int n, int iw, double gl, double gu, const double *d, const double *e2,
+                      double pivmin, double reltol, double *w, double *werr)
+{
+  const double eps = OR_EPS, fudge = 2.0;
+  const double tnorm = fmax(fabs(gl), fabs(gu)), atoli = fudge * 2.0 * pivmin;
+  const int itmax = (int)((or_log(tnorm + pivmin) - or_log(pivmin)) / or_log(2.0)) + 2;
+  double left = gl - fudge * tnorm * eps * n - fudge * 2.0 * pivmin;
+  double right = gu + fudge * tnorm * eps * n + fudge * 2.0 * pivmin;
+  int it = 0, i, negcnt;
+  for (;;) {
+    double tmp1 = fabs(right - left), tmp2 = fmax(fabs(right), fabs(left)), mid;
+    if (tmp1 < fmax(fmax(atoli, pivmin), reltol * tmp2)) break;
+    if (it > itmax) break;
+    it++;
+    mid = 0.5 * (left + right);
+    negcnt = 0;
+    tmp1 = d[0] - mid;
+    if (fabs(tmp1) < pivmin) tmp1 = -pivmin;
+    if (tmp1 <= 0.0) negcnt++;
+    for (i = 2; i <= n; i++) {
+      tmp1 = d[i - 1] - e2[i - 2] / tmp1 - mid;
+      if (fabs(tmp1) < pivmin) tmp1 = -pivmin;
+      if (tmp1 <= 0.0) negcnt++;
+    }
+    if (negcnt >= iw) right = mid;
+    else left = mid;
+  }
+  *w = 0.5 * (left + right);
+  *werr = 0.5 * fabs(right - left);
+}
+
+/* compute_root_rrr (SRC/mrrr_val.c:717-948).  allrng_no_bisec / useDQDS:
+ * the branches of the dqds route (extremal eigenvalues by dlarrk, the shift
+ * at an end of [isleft, isright], a definite representation). */
+static int or_root_rrr(int allrng_no_bisec, int useDQDS, int ibgn, int iend, int wbgn,
+                       int wend, int ilow, int iupp, double gl, double gu, or_in_t *Ds,
+                       or_val_t *Ws, or_tol_t *tol, double *work, int *sgndefp,
                        double *sigmap, double *spdiamp)
 {
   int nbl = iend - ibgn + 1, mbl = wend - wbgn + 1, n = Ds->n, i, j, jtry;
   double *D = Ds->D, *E = Ds->E, *W = Ws->W, *Werr = Ws->Werr, *Wgap = Ws->Wgap;
-  double pivmin = tol->pivmin, isleft, isright, spdiam, tmp0, s1, s2, sigma;
+  double pivmin = tol->pivmin, isleft, isright, spdiam, tmp0, tmp1, s1, s2, sigma;
   double clwdth, avgap, tau, Dpivot, Dmax;
   int cnt = 0, negcnt_lft = 0, negcnt_rgt = 0, sgndef, noREP;
   int off_L = n, off_invD = 2 * n;
 
-  isleft = fmax(gl, (W[wbgn] - Werr[wbgn]) - 100.0 * OR_EPS * fabs(W[wbgn] - Werr[wbgn]));
-  isright = fmin(gu, (W[wend] + Werr[wend]) + 100.0 * OR_EPS * fabs(W[wend] - Werr[wend]));
-  spdiam = gu - gl;
-  tmp0 = fmin(isright, *Ws->vup) - fmax(isleft, *Ws->vlp);
-  s1 = fmax(isleft, *Ws->vlp) + 0.25 * tmp0;
-  s2 = fmin(isright, *Ws->vup) - 0.25 * tmp0;
+  if (allrng_no_bisec || useDQDS) {
+    const double rtl = sqrt(OR_EPS);
+    or_dlarrk(nbl, 1, gl, gu, &D[ibgn], &Ds->E2[ibgn], pivmin, rtl, &tmp0, &tmp1);
+    isleft = fmax(gl, (tmp0 - tmp1) - 100.0 * OR_EPS * fabs(tmp0 - tmp1));
+    or_dlarrk(nbl, nbl, gl, gu, &D[ibgn], &Ds->E2[ibgn], pivmin, rtl, &tmp0, &tmp1);
+    isright = fmin(gu, (tmp0 + tmp1) + 100.0 * OR_EPS * fabs(tmp0 + tmp1));
+    spdiam = isright - isleft;
+  } else {
+    isleft = fmax(gl, (W[wbgn] - Werr[wbgn]) - 100.0 * OR_EPS * fabs(W[wbgn] - Werr[wbgn]));
+    isright = fmin(gu, (W[wend] + Werr[wend]) + 100.0 * OR_EPS * fabs(W[wend] - Werr[wend]));
+    spdiam = gu - gl;
+  }
+  if (allrng_no_bisec || useDQDS) {
+    s1 = isleft + 0.25 * spdiam;
+    s2 = isright - 0.25 * spdiam;
+  } else {
+    tmp0 = fmin(isright, *Ws->vup) - fmax(isleft, *Ws->vlp);
+    s1 = fmax(isleft, *Ws->vlp) + 0.25 * tmp0;
+    s2 = fmin(isright, *Ws->vup) - 0.25 * tmp0;
+  }
   if (mbl > 1)
     or_dlarrc_t(nbl, s1, s2, &D[ibgn], &E[ibgn], pivmin, &cnt, &negcnt_lft, &negcnt_rgt);
   if (mbl == 1) {
     sigma = gl; sgndef = 1;
   } else if ((negcnt_lft - ilow) >= (iupp - negcnt_rgt)) {
-    sigma = fmax(isleft, *Ws->vlp); sgndef = 1;
+    if (allrng_no_bisec) sigma = fmax(isleft, gl);
+    else if (useDQDS) sigma = isleft;
+    else sigma = fmax(isleft, *Ws->vlp);
+    sgndef = 1;
   } else {
-    sigma = fmin(isright, *Ws->vup); sgndef = -1;
+    if (allrng_no_bisec) sigma = fmin(isright, gu);
+    else if (useDQDS) sigma = isright;
+    else sigma = fmin(isright, *Ws->vup);
+    sgndef = -1;
   }
-  if (mbl > 1) {
+  if (useDQDS) {
+    tau = spdiam * OR_EPS * nbl + 2.0 * pivmin;
+    tau = fmax(tau, 2 * OR_EPS * fabs(sigma));
+  } else if (mbl > 1) {
     clwdth = W[wend] + Werr[wend] - W[wbgn] - Werr[wbgn];
     avgap = fabs(clwdth / (double)(wend - wbgn));
     if (sgndef > 0) {
@@ -1014,6 +1073,9 @@ static int or_root_rrr(int ibgn, int iend, int wbgn, int wend, int ilow,
       j++;
     }
     noREP = (Dmax > MAX_GROWTH * spdiam);
+    if (useDQDS && !noREP)   /* dqds needs a definite representation */
+      for (i = 0; i < nbl; i++)
+        if (sgndef * work[i] < 0.0) noREP = 1;
     if (noREP) {
       if (jtry == MAX_TRY_ROOT - 2) {
         if (sgndef == 1)
@@ -1033,7 +1095,7 @@ static int or_root_rrr(int ibgn, int iend, int wbgn, int wend, int ilow,
   }
   E[iend] = sigma;
   memcpy(&D[ibgn], &work[0], sizeof(double) * (size_t)nbl);
-  memcpy(&E[ibgn], &work[n], sizeof(double) * (size_t)(nbl - 1));
+  if (nbl > 1) memcpy(&E[ibgn], &work[n], sizeof(double) * (size_t)(nbl - 1));
   if (mbl > 1) {
     int iseed[4] = {1, 1, 1, 1};
     or_dlarnv2(iseed, 2 * nbl, work);
@@ -1043,14 +1105,19 @@ static int or_root_rrr(int ibgn, int iend, int wbgn, int wend, int ilow,
     }
     D[iend] *= 1.0 + OR_EPS * 8.0 * work[2 * nbl - 1];
   }
+  *sgndefp = sgndef;
   *sigmap = sigma;
   *spdiamp = spdiam;
   return 0;
 }
 
 /* mrrr_val with force_bisection: SRC/mrrr_val.c:110-639. */
+/* mrrr_val (SRC/mrrr_val.c:110-639).  nthreads plays the part of the
+ * reference's thread count in its route choice (SRC/mrrr_val.c:279-285,
+ * 409-412): bisection is forced when nthreads > ceil(12 nvals / n); else a
+ * block with more than half of its eigenvalues wanted takes dqds. */
 static int or_mrrr_val(const char *jobz, const char *range, or_in_t *Ds,
-                       or_val_t *Ws, or_tol_t *tol)
+                       or_val_t *Ws, or_tol_t *tol, int nthreads)
 {
   int n = Ds->n, i, info = 0;
   double *D = Ds->D, *E = Ds->E, *E2, *work, *Wcopy;
@@ -1059,7 +1126,7 @@ static int or_mrrr_val(const char *jobz, const char *range, or_in_t *Ds,
   int *mp = Ws->mp;
   enum { allrng = 1, valrng = 2, indrng = 3 } irange;
   double gl, gu, eold, emax, eabs, tmp1, tnorm, wl = 0, wu = 0, wlu = 0, wul = 0;
-  int nwl = 0, nwu = 0, nvals, ibgn, wbgn, jbl;
+  int nwl = 0, nwu = 0, nvals, ibgn, wbgn, jbl, force_bisection = 1;
 
   if (range[0] == 'A' || range[0] == 'a') irange = allrng;
   else if (range[0] == 'V' || range[0] == 'v') irange = valrng;
@@ -1103,6 +1170,7 @@ static int or_mrrr_val(const char *jobz, const char *range, or_in_t *Ds,
   nvals = *Ws->iup - *Ws->ilp + 1;
   *mp = nvals;
   if (jobz[0] == 'C' || jobz[0] == 'c') { info = 0; goto done; }
+  force_bisection = (double)nthreads > ceil(12.0 * nvals / (double)n);
 
   if (irange == indrng) {
     int itmax = (int)((or_log(tnorm + tol->pivmin) - or_log(tol->pivmin)) / or_log(2.0) + 2);
@@ -1159,8 +1227,40 @@ static int or_mrrr_val(const char *jobz, const char *range, or_in_t *Ds,
     for (i = wbgn; i < wend; i++) Wgap[i] = fmax(0.0, (W[i + 1] - Werr[i + 1]) - (W[i] + Werr[i]));
     Wgap[wend] = fmax(0.0, wu - (W[wend] + Werr[wend]));
 
-    if (or_root_rrr(ibgn, iend, wbgn, wend, ilow, iupp, bgl, bgu, Ds, Ws, tol, work, &sigma, &spdiam)) {
-      info = 2; goto done;
+    {
+      const int useDQDS = mbl > 0.5 * nbl && !force_bisection;
+      const int allrng_no_bisec = irange == allrng && !force_bisection;
+      int sgndef = 1;
+      if (or_root_rrr(allrng_no_bisec, useDQDS, ibgn, iend, wbgn, wend, ilow, iupp, bgl, bgu,
+                      Ds, Ws, tol, work, &sgndef, &sigma, &spdiam)) {
+        info = 2; goto done;
+      }
+      if (useDQDS) {
+        /* all eigenvalues of the definite root representation by dqds:
+         * SRC/mrrr_val.c:459-506 (the tolerance's log is or_log) */
+        const double rtol = 4.0 * or_log((double)nbl) * OR_EPS;
+        int j = ibgn, je = wbgn, qinfo = 0;
+        for (i = 0; i < nbl - 1; i++) {
+          work[2 * i] = fabs(D[j]);
+          work[2 * i + 1] = E[j] * E[j] * work[2 * i];
+          j++;
+        }
+        work[2 * (nbl - 1)] = fabs(D[iend]);
+        work[2 * (nbl - 1) + 1] = 0.0;
+        or_dlasq2(nbl, work, &qinfo);
+        if (qinfo != 0) { info = 2; goto done; }
+        for (i = ilow; i <= iupp; i++, je++) {
+          W[je] = sgndef > 0 ? work[nbl - i] : -work[i - 1];
+          iblock[je] = jbl + 1;
+          Windex[je] = i;
+        }
+        for (i = wbgn; i <= wend; i++) Werr[i] = rtol * fabs(W[i]);
+        for (i = wbgn; i < wend; i++) Wgap[i] = fmax(0.0, (W[i + 1] - Werr[i + 1]) - (W[i] + Werr[i]));
+        Wgap[wend] = fmax(0.0, (*Ws->vup - sigma) - (W[wend] + Werr[wend]));
+        ibgn = iend + 1;
+        wbgn = wend + 1;
+        continue;
+      }
     }
     /* refine_eigval_approx, unchunked branch: SRC/mrrr_val.c:992-1001, 1070-1082 */
     for (i = wbgn; i <= wend; i++) { W[i] -= sigma; Werr[i] += fabs(W[i]) * OR_EPS; }
@@ -1719,7 +1819,13 @@ int or_mrrr(const char *jobz, const char *range, int *np, double *D, double *E,
   tol.bsrtol = fmin(MIN_RELGAP * 1.0E-2, sqrt(DBL_EPSILON));
   tol.RQtol = 2.0 * DBL_EPSILON;
 
-  info = or_mrrr_val(jobz, range, &Ds, &Ws, &tol);
+  {
+    /* the thread count of the reference's route choice: MR3_NTHREADS, as
+     * the product reads it; unset, bisection (a GPU's parallelism) */
+    const char *ev = getenv("MR3_NTHREADS");
+    const int nthreads = (ev && *ev) ? atoi(ev) : 1 << 30;
+    info = or_mrrr_val(jobz, range, &Ds, &Ws, &tol, nthreads);
+  }
   if (info != 0) { rc = 2; goto out; }
   if (cntval) goto out;
   if (wantZ) {
@@ -1766,3 +1872,687 @@ out:
   free(Dcopy); free(E2copy);
   return rc;
 }
+
+/* ------------------------------------------------------------------------
+ * dqds: all eigenvalues of a positive definite L D L^T to high relative
+ * accuracy (LAPACK 3.2.2 dlasq2-dlasq6, vendored as SRC/LAPACK/odsq2.f -
+ * odsq6.f; the reference calls it at SRC/mrrr_val.c:464-477).  Z is the qd
+ * array in Fortran's 1-based numbering, Zq(i) = z[i-1].  IEEE arithmetic is
+ * assumed (odsq2.f's IEEE flag from ilaenv 10/11 is true on this hardware);
+ * MIN and MAX propagate a NaN so that dlasq3's NaN test sees it.
+ * ------------------------------------------------------------------------ */
+#define Zq(i) z[(i) - 1]
+
+static double or_fmin2(double a, double b) { return (a != a || b != b) ? NAN : (a < b ? a : b); }
+static double or_fmax2(double a, double b) { return (a != a || b != b) ? NAN : (a > b ? a : b); }
+
+/* odsq5.f: one dqds transform with shift tau (IEEE form). */
+static void or_dlasq5(int i0, int n0, double *z, int pp, double tau, double *dmin,
+                      double *dmin1, double *dmin2, double *dn, double *dnm1, double *dnm2)
+{
+  int j4, j4p2;
+  double d, emin, temp;
+  if (n0 - i0 - 1 <= 0) return;
+  j4 = 4 * i0 + pp - 3;
+  emin = Zq(j4 + 4);
+  d = Zq(j4) - tau;
+  *dmin = d;
+  *dmin1 = -Zq(j4);
+  if (pp == 0) {
+    for (j4 = 4 * i0; j4 <= 4 * (n0 - 3); j4 += 4) {
+      Zq(j4 - 2) = d + Zq(j4 - 1);
+      temp = Zq(j4 + 1) / Zq(j4 - 2);
+      d = d * temp - tau;
+      *dmin = or_fmin2(*dmin, d);
+      Zq(j4) = Zq(j4 - 1) * temp;
+      emin = or_fmin2(Zq(j4), emin);
+    }
+  } else {
+    for (j4 = 4 * i0; j4 <= 4 * (n0 - 3); j4 += 4) {
+      Zq(j4 - 3) = d + Zq(j4);
+      temp = Zq(j4 + 2) / Zq(j4 - 3);
+      d = d * temp - tau;
+      *dmin = or_fmin2(*dmin, d);
+      Zq(j4 - 1) = Zq(j4) * temp;
+      emin = or_fmin2(Zq(j4 - 1), emin);
+    }
+  }
+  *dnm2 = d;
+  *dmin2 = *dmin;
+  j4 = 4 * (n0 - 2) - pp;
+  j4p2 = j4 + 2 * pp - 1;
+  Zq(j4 - 2) = *dnm2 + Zq(j4p2);
+  Zq(j4) = Zq(j4p2 + 2) * (Zq(j4p2) / Zq(j4 - 2));
+  *dnm1 = Zq(j4p2 + 2) * (*dnm2 / Zq(j4 - 2)) - tau;
+  *dmin = or_fmin2(*dmin, *dnm1);
+  *dmin1 = *dmin;
+  j4 = j4 + 4;
+  j4p2 = j4 + 2 * pp - 1;
+  Zq(j4 - 2) = *dnm1 + Zq(j4p2);
+  Zq(j4) = Zq(j4p2 + 2) * (Zq(j4p2) / Zq(j4 - 2));
+  *dn = Zq(j4p2 + 2) * (*dnm1 / Zq(j4 - 2)) - tau;
+  *dmin = or_fmin2(*dmin, *dn);
+  Zq(j4 + 2) = *dn;
+  Zq(4 * n0 - pp) = emin;
+}
+
+/* odsq6.f: one dqd transform (no shift), guarded against underflow. */
+static void or_dlasq6(int i0, int n0, double *z, int pp, double *dmin, double *dmin1,
+                      double *dmin2, double *dn, double *dnm1, double *dnm2)
+{
+  int j4, j4p2;
+  double d, emin, temp;
+  const double safmin = OR_SAFMIN;
+  if (n0 - i0 - 1 <= 0) return;
+  j4 = 4 * i0 + pp - 3;
+  emin = Zq(j4 + 4);
+  d = Zq(j4);
+  *dmin = d;
+  if (pp == 0) {
+    for (j4 = 4 * i0; j4 <= 4 * (n0 - 3); j4 += 4) {
+      Zq(j4 - 2) = d + Zq(j4 - 1);
+      if (Zq(j4 - 2) == 0.0) {
+        Zq(j4) = 0.0;
+        d = Zq(j4 + 1);
+        *dmin = d;
+        emin = 0.0;
+      } else if (safmin * Zq(j4 + 1) < Zq(j4 - 2) && safmin * Zq(j4 - 2) < Zq(j4 + 1)) {
+        temp = Zq(j4 + 1) / Zq(j4 - 2);
+        Zq(j4) = Zq(j4 - 1) * temp;
+        d = d * temp;
+      } else {
+        Zq(j4) = Zq(j4 + 1) * (Zq(j4 - 1) / Zq(j4 - 2));
+        d = Zq(j4 + 1) * (d / Zq(j4 - 2));
+      }
+      *dmin = or_fmin2(*dmin, d);
+      emin = or_fmin2(emin, Zq(j4));
+    }
+  } else {
+    for (j4 = 4 * i0; j4 <= 4 * (n0 - 3); j4 += 4) {
+      Zq(j4 - 3) = d + Zq(j4);
+      if (Zq(j4 - 3) == 0.0) {
+        Zq(j4 - 1) = 0.0;
+        d = Zq(j4 + 2);
+        *dmin = d;
+        emin = 0.0;
+      } else if (safmin * Zq(j4 + 2) < Zq(j4 - 3) && safmin * Zq(j4 - 3) < Zq(j4 + 2)) {
+        temp = Zq(j4 + 2) / Zq(j4 - 3);
+        Zq(j4 - 1) = Zq(j4) * temp;
+        d = d * temp;
+      } else {
+        Zq(j4 - 1) = Zq(j4 + 2) * (Zq(j4) / Zq(j4 - 3));
+        d = Zq(j4 + 2) * (d / Zq(j4 - 3));
+      }
+      *dmin = or_fmin2(*dmin, d);
+      emin = or_fmin2(emin, Zq(j4 - 1));
+    }
+  }
+  *dnm2 = d;
+  *dmin2 = *dmin;
+  j4 = 4 * (n0 - 2) - pp;
+  j4p2 = j4 + 2 * pp - 1;
+  Zq(j4 - 2) = *dnm2 + Zq(j4p2);
+  if (Zq(j4 - 2) == 0.0) {
+    Zq(j4) = 0.0;
+    *dnm1 = Zq(j4p2 + 2);
+    *dmin = *dnm1;
+    emin = 0.0;
+  } else if (safmin * Zq(j4p2 + 2) < Zq(j4 - 2) && safmin * Zq(j4 - 2) < Zq(j4p2 + 2)) {
+    temp = Zq(j4p2 + 2) / Zq(j4 - 2);
+    Zq(j4) = Zq(j4p2) * temp;
+    *dnm1 = *dnm2 * temp;
+  } else {
+    Zq(j4) = Zq(j4p2 + 2) * (Zq(j4p2) / Zq(j4 - 2));
+    *dnm1 = Zq(j4p2 + 2) * (*dnm2 / Zq(j4 - 2));
+  }
+  *dmin = or_fmin2(*dmin, *dnm1);
+  *dmin1 = *dmin;
+  j4 = j4 + 4;
+  j4p2 = j4 + 2 * pp - 1;
+  Zq(j4 - 2) = *dnm1 + Zq(j4p2);
+  if (Zq(j4 - 2) == 0.0) {
+    Zq(j4) = 0.0;
+    *dn = Zq(j4p2 + 2);
+    *dmin = *dn;
+    emin = 0.0;
+  } else if (safmin * Zq(j4p2 + 2) < Zq(j4 - 2) && safmin * Zq(j4 - 2) < Zq(j4p2 + 2)) {
+    temp = Zq(j4p2 + 2) / Zq(j4 - 2);
+    Zq(j4) = Zq(j4p2) * temp;
+    *dn = *dnm1 * temp;
+  } else {
+    Zq(j4) = Zq(j4p2 + 2) * (Zq(j4p2) / Zq(j4 - 2));
+    *dn = Zq(j4p2 + 2) * (*dnm1 / Zq(j4 - 2));
+  }
+  *dmin = or_fmin2(*dmin, *dn);
+  Zq(j4 + 2) = *dn;
+  Zq(4 * n0 - pp) = emin;
+}
+
+/* dqds shift state carried between calls of dlasq3 (odsq2.f's locals). */
+typedef struct {
+  int ttype;
+  double dmin1, dmin2, dn, dn1, dn2, g, tau;
+} or_sq_t;
+
+/* odsq4.f: the shift. */
+static void or_dlasq4(int i0, int n0, const double *z, int pp, int n0in, double dmin,
+                      or_sq_t *q)
+{
+  const double cnst1 = 0.5630, cnst2 = 1.010, cnst3 = 1.050;
+  const double qurtr = 0.250, third = 0.3330, half = 0.50, hundrd = 100.0;
+  int i4, nn, np;
+  double a2, b1, b2, gam, gap1, gap2, s = 0.0;
+  const double dmin1 = q->dmin1, dmin2 = q->dmin2, dn = q->dn, dn1 = q->dn1, dn2 = q->dn2;
+  if (dmin <= 0.0) {
+    q->tau = -dmin;
+    q->ttype = -1;
+    return;
+  }
+  nn = 4 * n0 + pp;
+  if (n0in == n0) {
+    if (dmin == dn || dmin == dn1) {
+      b1 = sqrt(Zq(nn - 3)) * sqrt(Zq(nn - 5));
+      b2 = sqrt(Zq(nn - 7)) * sqrt(Zq(nn - 9));
+      a2 = Zq(nn - 7) + Zq(nn - 5);
+      if (dmin == dn && dmin1 == dn1) {
+        gap2 = dmin2 - a2 - dmin2 * qurtr;
+        if (gap2 > 0.0 && gap2 > b2) gap1 = a2 - dn - (b2 / gap2) * b2;
+        else gap1 = a2 - dn - (b1 + b2);
+        if (gap1 > 0.0 && gap1 > b1) {
+          s = or_fmax2(dn - (b1 / gap1) * b1, half * dmin);
+          q->ttype = -2;
+        } else {
+          s = 0.0;
+          if (dn > b1) s = dn - b1;
+          if (a2 > (b1 + b2)) s = or_fmin2(s, a2 - (b1 + b2));
+          s = or_fmax2(s, third * dmin);
+          q->ttype = -3;
+        }
+      } else {
+        q->ttype = -4;
+        s = qurtr * dmin;
+        if (dmin == dn) {
+          gam = dn;
+          a2 = 0.0;
+          if (Zq(nn - 5) > Zq(nn - 7)) return;   /* tau unchanged, as odsq4.f returns */
+          b2 = Zq(nn - 5) / Zq(nn - 7);
+          np = nn - 9;
+        } else {
+          np = nn - 2 * pp;
+          b2 = Zq(np - 2);
+          gam = dn1;
+          if (Zq(np - 4) > Zq(np - 2)) return;   /* tau unchanged, as odsq4.f returns */
+          a2 = Zq(np - 4) / Zq(np - 2);
+          if (Zq(nn - 9) > Zq(nn - 11)) return;   /* tau unchanged, as odsq4.f returns */
+          b2 = Zq(nn - 9) / Zq(nn - 11);
+          np = nn - 13;
+        }
+        a2 = a2 + b2;
+        for (i4 = np; i4 >= 4 * i0 - 1 + pp; i4 -= 4) {
+          if (b2 == 0.0) break;
+          b1 = b2;
+          if (Zq(i4) > Zq(i4 - 2)) return;   /* tau unchanged, as odsq4.f returns */
+          b2 = b2 * (Zq(i4) / Zq(i4 - 2));
+          a2 = a2 + b2;
+          if (hundrd * or_fmax2(b2, b1) < a2 || cnst1 < a2) break;
+        }
+        a2 = cnst3 * a2;
+        if (a2 < cnst1) s = gam * (1.0 - sqrt(a2)) / (1.0 + a2);
+      }
+    } else if (dmin == dn2) {
+      q->ttype = -5;
+      s = qurtr * dmin;
+      np = nn - 2 * pp;
+      b1 = Zq(np - 2);
+      b2 = Zq(np - 6);
+      gam = dn2;
+      if (Zq(np - 8) > b2 || Zq(np - 4) > b1) return;   /* tau unchanged, as odsq4.f returns */
+      a2 = (Zq(np - 8) / b2) * (1.0 + Zq(np - 4) / b1);
+      if (n0 - i0 > 2) {
+        b2 = Zq(nn - 13) / Zq(nn - 15);
+        a2 = a2 + b2;
+        for (i4 = nn - 17; i4 >= 4 * i0 - 1 + pp; i4 -= 4) {
+          if (b2 == 0.0) break;
+          b1 = b2;
+          if (Zq(i4) > Zq(i4 - 2)) return;   /* tau unchanged, as odsq4.f returns */
+          b2 = b2 * (Zq(i4) / Zq(i4 - 2));
+          a2 = a2 + b2;
+          if (hundrd * or_fmax2(b2, b1) < a2 || cnst1 < a2) break;
+        }
+        a2 = cnst3 * a2;
+      }
+      if (a2 < cnst1) s = gam * (1.0 - sqrt(a2)) / (1.0 + a2);
+    } else {
+      if (q->ttype == -6) q->g = q->g + third * (1.0 - q->g);
+      else if (q->ttype == -18) q->g = qurtr * third;
+      else q->g = qurtr;
+      s = q->g * dmin;
+      q->ttype = -6;
+    }
+  } else if (n0in == n0 + 1) {
+    if (dmin1 == dn1 && dmin2 == dn2) {
+      q->ttype = -7;
+      s = third * dmin1;
+      if (Zq(nn - 5) > Zq(nn - 7)) return;   /* tau unchanged, as odsq4.f returns */
+      b1 = Zq(nn - 5) / Zq(nn - 7);
+      b2 = b1;
+      if (b2 != 0.0) {
+        for (i4 = 4 * n0 - 9 + pp; i4 >= 4 * i0 - 1 + pp; i4 -= 4) {
+          a2 = b1;
+          if (Zq(i4) > Zq(i4 - 2)) return;   /* tau unchanged, as odsq4.f returns */
+          b1 = b1 * (Zq(i4) / Zq(i4 - 2));
+          b2 = b2 + b1;
+          if (hundrd * or_fmax2(b1, a2) < b2) break;
+        }
+      }
+      b2 = sqrt(cnst3 * b2);
+      a2 = dmin1 / (1.0 + b2 * b2);
+      gap2 = half * dmin2 - a2;
+      if (gap2 > 0.0 && gap2 > b2 * a2) {
+        s = or_fmax2(s, a2 * (1.0 - cnst2 * a2 * (b2 / gap2) * b2));
+      } else {
+        s = or_fmax2(s, a2 * (1.0 - cnst2 * b2));
+        q->ttype = -8;
+      }
+    } else {
+      s = qurtr * dmin1;
+      if (dmin1 == dn1) s = half * dmin1;
+      q->ttype = -9;
+    }
+  } else if (n0in == n0 + 2) {
+    if (dmin2 == dn2 && 2.0 * Zq(nn - 5) < Zq(nn - 7)) {
+      q->ttype = -10;
+      s = third * dmin2;
+      if (Zq(nn - 5) > Zq(nn - 7)) return;   /* tau unchanged, as odsq4.f returns */
+      b1 = Zq(nn - 5) / Zq(nn - 7);
+      b2 = b1;
+      if (b2 != 0.0) {
+        for (i4 = 4 * n0 - 9 + pp; i4 >= 4 * i0 - 1 + pp; i4 -= 4) {
+          if (Zq(i4) > Zq(i4 - 2)) return;   /* tau unchanged, as odsq4.f returns */
+          b1 = b1 * (Zq(i4) / Zq(i4 - 2));
+          b2 = b2 + b1;
+          if (hundrd * b1 < b2) break;
+        }
+      }
+      b2 = sqrt(cnst3 * b2);
+      a2 = dmin2 / (1.0 + b2 * b2);
+      gap2 = Zq(nn - 7) + Zq(nn - 9) - sqrt(Zq(nn - 11)) * sqrt(Zq(nn - 9)) - a2;
+      if (gap2 > 0.0 && gap2 > b2 * a2) s = or_fmax2(s, a2 * (1.0 - cnst2 * a2 * (b2 / gap2) * b2));
+      else s = or_fmax2(s, a2 * (1.0 - cnst2 * b2));
+    } else {
+      s = qurtr * dmin2;
+      q->ttype = -11;
+    }
+  } else if (n0in > n0 + 2) {
+    s = 0.0;
+    q->ttype = -12;
+  }
+  q->tau = s;
+}
+
+/* odsq3.f: deflation, the shift and one dqds step (with retries). */
+static void or_dlasq3(int i0, int *n0p, double *z, int *ppp, double *dminp, double *sigmap,
+                      double *desigp, double *qmaxp, int *nfail, int *iter, int *ndiv,
+                      or_sq_t *q)
+{
+  const double cbias = 1.50, qurtr = 0.250, half = 0.5, hundrd = 100.0;
+  const double eps = OR_EPS, tol = eps * hundrd, tol2 = tol * tol;
+  int n0 = *n0p, pp = *ppp, ipn4, j4, nn;
+  const int n0in = n0;
+  double dmin = *dminp, sigma = *sigmap, desig = *desigp, qmax = *qmaxp, s, t, temp;
+  for (;;) {   /* label 10: deflation */
+    if (n0 < i0) goto out;
+    if (n0 == i0) goto l20;
+    nn = 4 * n0 + pp;
+    if (n0 == i0 + 1) goto l40;
+    if (Zq(nn - 5) > tol2 * (sigma + Zq(nn - 3)) && Zq(nn - 2 * pp - 4) > tol2 * Zq(nn - 7))
+      goto l30;
+  l20:
+    Zq(4 * n0 - 3) = Zq(4 * n0 + pp - 3) + sigma;
+    n0 = n0 - 1;
+    continue;
+  l30:
+    if (Zq(nn - 9) > tol2 * sigma && Zq(nn - 2 * pp - 8) > tol2 * Zq(nn - 11)) break;
+  l40:
+    if (Zq(nn - 3) > Zq(nn - 7)) {
+      s = Zq(nn - 3);
+      Zq(nn - 3) = Zq(nn - 7);
+      Zq(nn - 7) = s;
+    }
+    if (Zq(nn - 5) > Zq(nn - 3) * tol2) {
+      t = half * ((Zq(nn - 7) - Zq(nn - 3)) + Zq(nn - 5));
+      s = Zq(nn - 3) * (Zq(nn - 5) / t);
+      if (s <= t) s = Zq(nn - 3) * (Zq(nn - 5) / (t * (1.0 + sqrt(1.0 + s / t))));
+      else s = Zq(nn - 3) * (Zq(nn - 5) / (t + sqrt(t) * sqrt(t + s)));
+      t = Zq(nn - 7) + (s + Zq(nn - 5));
+      Zq(nn - 3) = Zq(nn - 3) * (Zq(nn - 7) / t);
+      Zq(nn - 7) = t;
+    }
+    Zq(4 * n0 - 7) = Zq(nn - 7) + sigma;
+    Zq(4 * n0 - 3) = Zq(nn - 3) + sigma;
+    n0 = n0 - 2;
+  }
+  /* label 50 */
+  if (pp == 2) pp = 0;
+  if (dmin <= 0.0 || n0 < n0in) {
+    if (cbias * Zq(4 * i0 + pp - 3) < Zq(4 * n0 + pp - 3)) {
+      ipn4 = 4 * (i0 + n0);
+      for (j4 = 4 * i0; j4 <= 2 * (i0 + n0 - 1); j4 += 4) {
+        temp = Zq(j4 - 3); Zq(j4 - 3) = Zq(ipn4 - j4 - 3); Zq(ipn4 - j4 - 3) = temp;
+        temp = Zq(j4 - 2); Zq(j4 - 2) = Zq(ipn4 - j4 - 2); Zq(ipn4 - j4 - 2) = temp;
+        temp = Zq(j4 - 1); Zq(j4 - 1) = Zq(ipn4 - j4 - 5); Zq(ipn4 - j4 - 5) = temp;
+        temp = Zq(j4); Zq(j4) = Zq(ipn4 - j4 - 4); Zq(ipn4 - j4 - 4) = temp;
+      }
+      if (n0 - i0 <= 4) {
+        Zq(4 * n0 + pp - 1) = Zq(4 * i0 + pp - 1);
+        Zq(4 * n0 - pp) = Zq(4 * i0 - pp);
+      }
+      q->dmin2 = or_fmin2(q->dmin2, Zq(4 * n0 + pp - 1));
+      Zq(4 * n0 + pp - 1) =
+          or_fmin2(or_fmin2(Zq(4 * n0 + pp - 1), Zq(4 * i0 + pp - 1)), Zq(4 * i0 + pp + 3));
+      Zq(4 * n0 - pp) = or_fmin2(or_fmin2(Zq(4 * n0 - pp), Zq(4 * i0 - pp)), Zq(4 * i0 - pp + 4));
+      qmax = or_fmax2(or_fmax2(qmax, Zq(4 * i0 + pp - 3)), Zq(4 * i0 + pp + 1));
+      dmin = -0.0;
+    }
+  }
+  or_dlasq4(i0, n0, z, pp, n0in, dmin, q);
+  for (;;) {   /* label 70 */
+    or_dlasq5(i0, n0, z, pp, q->tau, &dmin, &q->dmin1, &q->dmin2, &q->dn, &q->dn1, &q->dn2);
+    *ndiv = *ndiv + (n0 - i0 + 2);
+    *iter = *iter + 1;
+    if (dmin >= 0.0 && q->dmin1 > 0.0) {
+      goto l90;
+    } else if (dmin < 0.0 && q->dmin1 > 0.0 && Zq(4 * (n0 - 1) - pp) < tol * (sigma + q->dn1) &&
+               fabs(q->dn) < tol * sigma) {
+      Zq(4 * (n0 - 1) - pp + 2) = 0.0;
+      dmin = 0.0;
+      goto l90;
+    } else if (dmin < 0.0) {
+      *nfail = *nfail + 1;
+      if (q->ttype < -22) {
+        q->tau = 0.0;
+      } else if (q->dmin1 > 0.0) {
+        q->tau = (q->tau + dmin) * (1.0 - 2.0 * eps);
+        q->ttype = q->ttype - 11;
+      } else {
+        q->tau = qurtr * q->tau;
+        q->ttype = q->ttype - 12;
+      }
+      continue;
+    } else if (dmin != dmin) {
+      if (q->tau == 0.0) break;
+      q->tau = 0.0;
+      continue;
+    } else {
+      break;
+    }
+  }
+  /* label 80 */
+  or_dlasq6(i0, n0, z, pp, &dmin, &q->dmin1, &q->dmin2, &q->dn, &q->dn1, &q->dn2);
+  *ndiv = *ndiv + (n0 - i0 + 2);
+  *iter = *iter + 1;
+  q->tau = 0.0;
+l90:
+  if (q->tau < sigma) {
+    desig = desig + q->tau;
+    t = sigma + desig;
+    desig = desig - (t - sigma);
+  } else {
+    t = sigma + q->tau;
+    desig = sigma - (t - q->tau) + desig;
+  }
+  sigma = t;
+out:
+  *n0p = n0;
+  *ppp = pp;
+  *dminp = dmin;
+  *sigmap = sigma;
+  *desigp = desig;
+  *qmaxp = qmax;
+}
+
+/* Sort of x[0..n-1] in decreasing order (dlasrt('D'), SRC/LAPACK/odsrt.f;
+ * the order of equal values is immaterial). */
+static int or_cmp_desc(const void *a, const void *b)
+{
+  const double x = *(const double *)a, y = *(const double *)b;
+  return (x < y) - (x > y);
+}
+
+/* odsq2.f: the eigenvalues of the qd array z (z[2k-2] = q_k, z[2k-1] = e_k,
+ * 4n doubles of room) in z[0..n-1], decreasing; info as LAPACK's. */
+void or_dlasq2(int n, double *z, int *info)
+{
+  const double cbias = 1.50, half = 0.5, four = 4.0, hundrd = 100.0;
+  const double eps = OR_EPS, safmin = OR_SAFMIN, tol = eps * hundrd, tol2 = tol * tol;
+  int i0, i4, ipn4, iter, iwhila, iwhilb, k, kmin, n0, n1, i1, nbig, ndiv, nfail, pp, splt;
+  double d, dee, deemin, desig, dmin, e, emax, emin, oldemn, qmax, qmin, s, sigma, t, temp,
+      trace, zmax, tempe, tempq;
+  or_sq_t q;
+  *info = 0;
+  if (n < 0) { *info = -1; return; }
+  if (n == 0) return;
+  if (n == 1) {
+    if (Zq(1) < 0.0) *info = -201;
+    return;
+  }
+  if (n == 2) {
+    if (Zq(2) < 0.0 || Zq(3) < 0.0) { *info = -2; return; }
+    if (Zq(3) > Zq(1)) { d = Zq(3); Zq(3) = Zq(1); Zq(1) = d; }
+    Zq(5) = Zq(1) + Zq(2) + Zq(3);
+    if (Zq(2) > Zq(3) * tol2) {
+      t = half * ((Zq(1) - Zq(3)) + Zq(2));
+      s = Zq(3) * (Zq(2) / t);
+      if (s <= t) s = Zq(3) * (Zq(2) / (t * (1.0 + sqrt(1.0 + s / t))));
+      else s = Zq(3) * (Zq(2) / (t + sqrt(t) * sqrt(t + s)));
+      t = Zq(1) + (s + Zq(2));
+      Zq(3) = Zq(3) * (Zq(1) / t);
+      Zq(1) = t;
+    }
+    Zq(2) = Zq(3);
+    Zq(6) = Zq(2) + Zq(1);
+    return;
+  }
+  Zq(2 * n) = 0.0;
+  emin = Zq(2);
+  qmax = 0.0;
+  zmax = 0.0;
+  d = 0.0;
+  e = 0.0;
+  for (k = 1; k <= 2 * (n - 1); k += 2) {
+    if (Zq(k) < 0.0) { *info = -(200 + k); return; }
+    if (Zq(k + 1) < 0.0) { *info = -(200 + k + 1); return; }
+    d = d + Zq(k);
+    e = e + Zq(k + 1);
+    qmax = or_fmax2(qmax, Zq(k));
+    emin = or_fmin2(emin, Zq(k + 1));
+    zmax = or_fmax2(or_fmax2(qmax, zmax), Zq(k + 1));
+  }
+  if (Zq(2 * n - 1) < 0.0) { *info = -(200 + 2 * n - 1); return; }
+  d = d + Zq(2 * n - 1);
+  qmax = or_fmax2(qmax, Zq(2 * n - 1));
+  zmax = or_fmax2(qmax, zmax);
+  if (e == 0.0) {
+    for (k = 2; k <= n; k++) Zq(k) = Zq(2 * k - 1);
+    qsort(z, (size_t)n, sizeof(double), or_cmp_desc);
+    Zq(2 * n - 1) = d;
+    return;
+  }
+  trace = d + e;
+  if (trace == 0.0) { Zq(2 * n - 1) = 0.0; return; }
+  for (k = 2 * n; k >= 2; k -= 2) {
+    Zq(2 * k) = 0.0;
+    Zq(2 * k - 1) = Zq(k);
+    Zq(2 * k - 2) = 0.0;
+    Zq(2 * k - 3) = Zq(k - 1);
+  }
+  i0 = 1;
+  n0 = n;
+  if (cbias * Zq(4 * i0 - 3) < Zq(4 * n0 - 3)) {
+    ipn4 = 4 * (i0 + n0);
+    for (i4 = 4 * i0; i4 <= 2 * (i0 + n0 - 1); i4 += 4) {
+      temp = Zq(i4 - 3); Zq(i4 - 3) = Zq(ipn4 - i4 - 3); Zq(ipn4 - i4 - 3) = temp;
+      temp = Zq(i4 - 1); Zq(i4 - 1) = Zq(ipn4 - i4 - 5); Zq(ipn4 - i4 - 5) = temp;
+    }
+  }
+  pp = 0;
+  for (k = 1; k <= 2; k++) {
+    d = Zq(4 * n0 + pp - 3);
+    for (i4 = 4 * (n0 - 1) + pp; i4 >= 4 * i0 + pp; i4 -= 4) {
+      if (Zq(i4 - 1) <= tol2 * d) {
+        Zq(i4 - 1) = -0.0;
+        d = Zq(i4 - 3);
+      } else {
+        d = Zq(i4 - 3) * (d / (d + Zq(i4 - 1)));
+      }
+    }
+    emin = Zq(4 * i0 + pp + 1);
+    d = Zq(4 * i0 + pp - 3);
+    for (i4 = 4 * i0 + pp; i4 <= 4 * (n0 - 1) + pp; i4 += 4) {
+      Zq(i4 - 2 * pp - 2) = d + Zq(i4 - 1);
+      if (Zq(i4 - 1) <= tol2 * d) {
+        Zq(i4 - 1) = -0.0;
+        Zq(i4 - 2 * pp - 2) = d;
+        Zq(i4 - 2 * pp) = 0.0;
+        d = Zq(i4 + 1);
+      } else if (safmin * Zq(i4 + 1) < Zq(i4 - 2 * pp - 2) &&
+                 safmin * Zq(i4 - 2 * pp - 2) < Zq(i4 + 1)) {
+        temp = Zq(i4 + 1) / Zq(i4 - 2 * pp - 2);
+        Zq(i4 - 2 * pp) = Zq(i4 - 1) * temp;
+        d = d * temp;
+      } else {
+        Zq(i4 - 2 * pp) = Zq(i4 + 1) * (Zq(i4 - 1) / Zq(i4 - 2 * pp - 2));
+        d = Zq(i4 + 1) * (d / Zq(i4 - 2 * pp - 2));
+      }
+      emin = or_fmin2(emin, Zq(i4 - 2 * pp));
+    }
+    Zq(4 * n0 - pp - 2) = d;
+    qmax = Zq(4 * i0 - pp - 2);
+    for (i4 = 4 * i0 - pp + 2; i4 <= 4 * n0 - pp - 2; i4 += 4) qmax = or_fmax2(qmax, Zq(i4));
+    pp = 1 - pp;
+  }
+  q.ttype = 0;
+  q.dmin1 = 0.0; q.dmin2 = 0.0; q.dn = 0.0; q.dn1 = 0.0; q.dn2 = 0.0; q.g = 0.0; q.tau = 0.0;
+  iter = 2;
+  nfail = 0;
+  ndiv = 2 * (n0 - i0);
+  for (iwhila = 1; iwhila <= n + 1; iwhila++) {
+    if (n0 < 1) goto l170;
+    desig = 0.0;
+    if (n0 == n) sigma = 0.0;
+    else sigma = -Zq(4 * n0 - 1);
+    if (sigma < 0.0) { *info = 1; return; }
+    emax = 0.0;
+    if (n0 > i0) emin = fabs(Zq(4 * n0 - 5));
+    else emin = 0.0;
+    qmin = Zq(4 * n0 - 3);
+    qmax = qmin;
+    for (i4 = 4 * n0; i4 >= 8; i4 -= 4) {
+      if (Zq(i4 - 5) <= 0.0) goto l100;
+      if (qmin >= four * emax) {
+        qmin = or_fmin2(qmin, Zq(i4 - 3));
+        emax = or_fmax2(emax, Zq(i4 - 5));
+      }
+      qmax = or_fmax2(qmax, Zq(i4 - 7) + Zq(i4 - 5));
+      emin = or_fmin2(emin, Zq(i4 - 5));
+    }
+    i4 = 4;
+  l100:
+    i0 = i4 / 4;
+    pp = 0;
+    if (n0 - i0 > 1) {
+      dee = Zq(4 * i0 - 3);
+      deemin = dee;
+      kmin = i0;
+      for (i4 = 4 * i0 + 1; i4 <= 4 * n0 - 3; i4 += 4) {
+        dee = Zq(i4) * (dee / (dee + Zq(i4 - 2)));
+        if (dee <= deemin) {
+          deemin = dee;
+          kmin = (i4 + 3) / 4;
+        }
+      }
+      if ((kmin - i0) * 2 < n0 - kmin && deemin <= half * Zq(4 * n0 - 3)) {
+        ipn4 = 4 * (i0 + n0);
+        pp = 2;
+        for (i4 = 4 * i0; i4 <= 2 * (i0 + n0 - 1); i4 += 4) {
+          temp = Zq(i4 - 3); Zq(i4 - 3) = Zq(ipn4 - i4 - 3); Zq(ipn4 - i4 - 3) = temp;
+          temp = Zq(i4 - 2); Zq(i4 - 2) = Zq(ipn4 - i4 - 2); Zq(ipn4 - i4 - 2) = temp;
+          temp = Zq(i4 - 1); Zq(i4 - 1) = Zq(ipn4 - i4 - 5); Zq(ipn4 - i4 - 5) = temp;
+          temp = Zq(i4); Zq(i4) = Zq(ipn4 - i4 - 4); Zq(ipn4 - i4 - 4) = temp;
+        }
+      }
+    }
+    dmin = -or_fmax2(0.0, qmin - 2.0 * sqrt(qmin) * sqrt(emax));
+    nbig = 100 * (n0 - i0 + 1);
+    for (iwhilb = 1; iwhilb <= nbig; iwhilb++) {
+      if (i0 > n0) goto l150;
+      or_dlasq3(i0, &n0, z, &pp, &dmin, &sigma, &desig, &qmax, &nfail, &iter, &ndiv, &q);
+      pp = 1 - pp;
+      if (pp == 0 && n0 - i0 >= 3) {
+        if (Zq(4 * n0) <= tol2 * qmax || Zq(4 * n0 - 1) <= tol2 * sigma) {
+          splt = i0 - 1;
+          qmax = Zq(4 * i0 - 3);
+          emin = Zq(4 * i0 - 1);
+          oldemn = Zq(4 * i0);
+          for (i4 = 4 * i0; i4 <= 4 * (n0 - 3); i4 += 4) {
+            if (Zq(i4) <= tol2 * Zq(i4 - 3) || Zq(i4 - 1) <= tol2 * sigma) {
+              Zq(i4 - 1) = -sigma;
+              splt = i4 / 4;
+              qmax = 0.0;
+              emin = Zq(i4 + 3);
+              oldemn = Zq(i4 + 4);
+            } else {
+              qmax = or_fmax2(qmax, Zq(i4 + 1));
+              emin = or_fmin2(emin, Zq(i4 - 1));
+              oldemn = or_fmin2(oldemn, Zq(i4));
+            }
+          }
+          Zq(4 * n0 - 1) = emin;
+          Zq(4 * n0) = oldemn;
+          i0 = splt + 1;
+        }
+      }
+    }
+    /* maximum number of iterations exceeded: restore the shift and return
+     * the unconverged block in z (info 2) */
+    *info = 2;
+    i1 = i0;
+    n1 = n0;
+  l145:
+    tempq = Zq(4 * i0 - 3);
+    Zq(4 * i0 - 3) = Zq(4 * i0 - 3) + sigma;
+    for (k = i0 + 1; k <= n0; k++) {
+      tempe = Zq(4 * k - 5);
+      Zq(4 * k - 5) = Zq(4 * k - 5) * (tempq / Zq(4 * k - 7));
+      tempq = Zq(4 * k - 3);
+      Zq(4 * k - 3) = Zq(4 * k - 3) + sigma + tempe - Zq(4 * k - 5);
+    }
+    if (i1 > 1) {
+      n1 = i1 - 1;
+      while (i1 >= 2 && Zq(4 * i1 - 5) >= 0.0) i1 = i1 - 1;
+      sigma = -Zq(4 * n1 - 1);
+      goto l145;
+    }
+    for (k = 1; k <= n; k++) {
+      Zq(2 * k - 1) = Zq(4 * k - 3);
+      if (k < n0) Zq(2 * k) = Zq(4 * k - 1);
+      else Zq(2 * k) = 0;
+    }
+    return;
+  l150:;
+  }
+  *info = 3;
+  return;
+l170:
+  for (k = 2; k <= n; k++) Zq(k) = Zq(4 * k - 3);
+  qsort(z, (size_t)n, sizeof(double), or_cmp_desc);
+  e = 0.0;
+  for (k = n; k >= 1; k--) e = e + Zq(k);
+  Zq(2 * n + 1) = trace;
+  Zq(2 * n + 2) = e;
+  Zq(2 * n + 3) = (double)iter;
+  Zq(2 * n + 4) = (double)ndiv / (double)((long long)n * n);
+  Zq(2 * n + 5) = hundrd * nfail / (double)iter;
+  (void)zmax; (void)n1; (void)oldemn; (void)emin;
+}
+#undef Zq

@@ -64,6 +64,7 @@ int    or_count_ijob1(int n, const double *d, const double *e2, double pivmin,
 int    or_count_bisect(int n, const double *d, const double *e2,
                        double pivmin, double x);
 void   or_dlarnv2(int iseed[4], int n, double *x);
+void   or_dlasq2(int n, double *z, int *info);
 int    or_dlarrr(int n, const double *d, const double *e);
 void   or_dlarra(int n, const double *d, double *e, double *e2, double spltol,
                  double tnrm, int *nsplit, int *isplit);

@@ -2258,6 +2258,174 @@ static __device__ __noinline__ void dv_r1w_solve(bool active, int n, double lamb
   o->sawnan = slow;
 }
 
+// ------------------------------------------------------------------------
+// dlar1v for one eigenvector on a whole warp (the short lists at the end of
+// a level, where latency rather than throughput counts).  The stationary
+// sweep (lane 0) and the progressive sweep (lane 1) are independent chains
+// and run at the same time, each keeping every row's values in the warp's
+// scratch (SI and LPLUS of the stationary rows, P and UMINUS of the
+// progressive ones); the twist index is then chosen by all 32 lanes (the
+// smallest |gamma(i)|, the largest i among equal ones: what odr1v.f's upward
+// scan with .LE. selects); the back-substitution runs upward on lane 0 and
+// downward on lane 1, and lane 0 adds the downward squares to ztz after its
+// own, in odr1v.f's order.  Every value is computed by the operations of
+// odr1v.f:158-362 in their order, so the results are those of
+// dv_r1c_factor + dv_r1c_solve bit for bit.
+// Scratch per warp (nmax doubles each): SI, LP, PA, UM, ZV, rows 1-based at
+// [row]: SI[i], LP[i] of stationary row i; PA[i] the progressive value after
+// row i (PA[n] = D(n) - lambda); UM[i] of row i; ZV[i] the vector.
+// ------------------------------------------------------------------------
+struct r1s_buf {
+  double *SI, *LP, *PA, *UM, *ZV;
+};
+
+static __device__ __noinline__ void dv_r1s_call(int n, double lambda, const double2 *__restrict__ P,
+                                         const double2 *__restrict__ Q, int ps, double pivmin,
+                                         bool wantnc, int r_in, double gaptol, r1s_buf b,
+                                         int *negcnt_o, dlar1v_out *o) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const double eps = MR3_EPS;
+  int r1 = 1, r2 = n;
+  if (r_in != 0) { r1 = r_in; r2 = r_in; }
+  // ---- the two sweeps, rerun with the NaN-safe formulas where needed
+  int neg1 = 0, neg2 = 0;
+  bool slowA = false, slowB = false;
+  double sr1 = 0.0;   // SI of row r1-1 (0 for r1 = 1)
+  if (lane == 0) {
+    for (int pass = 0; pass < 2; pass++) {
+      const bool SLOW = pass == 1;
+      double s = 0.0 - lambda;
+      bool sawnan = false;
+      neg1 = 0;
+      sr1 = 0.0;
+#pragma unroll 4
+      for (int i = 1; i <= r2 - 1; i++) {
+        const double2 pp = P[(size_t)(i - 1) * ps], q = Q[(size_t)(i - 1) * ps];
+        double dplus = pp.x + s;
+        if (SLOW && fabs(dplus) < pivmin) dplus = -pivmin;
+        const double lp = q.y / dplus;
+        if (i <= r1 - 1) neg1 += (dplus < 0.0);
+        double si = s * lp * q.x;
+        if (SLOW && lp == 0.0) si = pp.y;
+        s = si - lambda;
+        b.LP[i] = lp;
+        b.SI[i] = si;
+        if (i == r1 - 1) {
+          sr1 = si;
+          if (!SLOW && isnan(s)) sawnan = true;
+        }
+        if (sawnan) break;
+      }
+      if (!SLOW && !sawnan) sawnan = isnan(s);
+      if (SLOW || !sawnan) break;
+      slowA = true;
+    }
+  } else if (lane == 1) {
+    for (int pass = 0; pass < 2; pass++) {
+      const bool SLOW = pass == 1;
+      double p = P[(size_t)(n - 1) * ps].x - lambda;
+      b.PA[n] = p;
+      neg2 = 0;
+#pragma unroll 4
+      for (int i = n - 1; i >= r1; i--) {
+        const double2 pp = P[(size_t)(i - 1) * ps];
+        double dminus = pp.y + p;
+        if (SLOW && fabs(dminus) < pivmin) dminus = -pivmin;
+        const double tmp = pp.x / dminus;
+        neg2 += (dminus < 0.0);
+        b.UM[i] = Q[(size_t)(i - 1) * ps].x * tmp;
+        double pn = p * tmp - lambda;
+        if (SLOW && tmp == 0.0) pn = pp.x - lambda;
+        p = pn;
+        b.PA[i] = p;
+      }
+      if (SLOW || !isnan(p)) break;
+      slowB = true;
+    }
+  }
+  neg1 = __shfl_sync(full, neg1, 0);
+  sr1 = __shfl_sync(full, sr1, 0);
+  slowA = __shfl_sync(full, slowA, 0);
+  neg2 = __shfl_sync(full, neg2, 1);
+  slowB = __shfl_sync(full, slowB, 1);
+  __syncwarp();
+  // ---- the twist index: gamma(i) = SI(i-1) + P(i-1) for i in (r1, r2]
+  double best = 0.0;
+  int rbest = 0;
+  for (int i = r1 + 1 + lane; i <= r2; i += 32) {
+    const double sprev = b.SI[i - 1];
+    double c = sprev + b.PA[i];
+    if (c == 0.0) c = eps * sprev;
+    if (isnan(c)) continue;
+    if (rbest == 0 || fabs(c) <= fabs(best)) { best = c; rbest = i; }   // i increases
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ob = __shfl_xor_sync(full, best, o);
+    const int orb = __shfl_xor_sync(full, rbest, o);
+    if (orb != 0 && (rbest == 0 || fabs(ob) < fabs(best) || (fabs(ob) == fabs(best) && orb > rbest))) {
+      best = ob;
+      rbest = orb;
+    }
+  }
+  const double pr1 = b.PA[r1];
+  double mg = sr1 + pr1;
+  if (mg < 0.0) neg1++;
+  *negcnt_o = wantnc ? neg1 + neg2 : -1;
+  if (fabs(mg) == 0.0) mg = eps * sr1;
+  int r = r1;
+  if (rbest != 0 && fabs(best) <= fabs(mg)) { mg = best; r = rbest; }
+  const bool slow = slowA || slowB;
+  // ---- back-substitution: upward on lane 0, downward on lane 1
+  int is1 = 1, is2 = n;
+  double ztz = 1.0;
+  if (lane == 0) {
+    b.ZV[r] = 1.0;
+    double zp = 1.0, zpp = 0.0;
+    for (int i = r - 1; i >= 1; i--) {
+      const double ldi = Q[(size_t)(i - 1) * ps].y;
+      double zi;
+      if (!slow) zi = -(b.LP[i] * zp);
+      else if (zp == 0.0) zi = -(Q[(size_t)i * ps].y / ldi) * zpp;
+      else zi = -(b.LP[i] * zp);
+      if ((fabs(zi) + fabs(zp)) * fabs(ldi) < gaptol) { is1 = i + 1; break; }
+      ztz = ztz + zi * zi;
+      b.ZV[i] = zi;
+      zpp = zp;
+      zp = zi;
+    }
+  } else if (lane == 1) {
+    double zc = 1.0, zcp = 0.0;
+    for (int i = r; i <= n - 1; i++) {
+      const double ldi = Q[(size_t)(i - 1) * ps].y;
+      double zn;
+      if (!slow) zn = -(b.UM[i] * zc);
+      else if (zc == 0.0) zn = -(Q[(size_t)(i - 2) * ps].y / ldi) * zcp;
+      else zn = -(b.UM[i] * zc);
+      if ((fabs(zc) + fabs(zn)) * fabs(ldi) < gaptol) { is2 = i; break; }
+      b.ZV[i + 1] = zn;
+      zcp = zc;
+      zc = zn;
+    }
+  }
+  is2 = __shfl_sync(full, is2, 1);
+  __syncwarp();
+  if (lane == 0)
+    for (int i = r + 1; i <= is2; i++) ztz = ztz + b.ZV[i] * b.ZV[i];
+  ztz = __shfl_sync(full, ztz, 0);
+  is1 = __shfl_sync(full, is1, 0);
+  o->r = r;
+  o->mingma = mg;
+  o->isupp1 = is1;
+  o->isupp2 = is2;
+  o->ztz = ztz;
+  const double tmp = 1.0 / ztz;
+  o->nrminv = sqrt(tmp);
+  o->resid = fabs(mg) * o->nrminv;
+  o->rqcorr = mg * tmp;
+  o->sawnan = slow;
+}
+
 // The factorisation L+ D+ L+^T = L D L^T - sigma I of dlarrf
 // (SRC/LAPACK/odrrf.f:226-252) for one shift: DPLUS into dp[i*os], LPLUS
 // into lp[i*os]; returns max |DPLUS|, sawnan when a pivot was replaced by

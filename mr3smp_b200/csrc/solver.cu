@@ -2356,12 +2356,17 @@ k_sng_bisect(int out, const SngDev *sng, const ClusterDev *cl, const ProbDev *pr
 // sequence (round, compaction, bisection, sort) between calls.  Every call
 // and every state update is the one the rounds make, so the results are the
 // same bits.  The last block to finish empties the list (mode 2).
+// SPLIT: each dlar1v is dv_r1s_call (the two sweeps on two lanes at once,
+// the twist chosen by the warp, the vector in the warp's row scratch
+// fscratch, 5 (nmax + 2) doubles per warp) instead of lane 0's checkpointed
+// dlar1v; the results are the same bits.
+template <bool SPLIT>
 __global__ void __launch_bounds__(SNG_WARPS * 32, 2)
 k_sng_finish(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
              const BlockDev *blocks, const double2 *RP, const double2 *RQ, const double *arena,
              double *W, double *Wsh, double *Werr, double *Wgap, const int *Windex,
              const int *Zindex, SngState *sst, const int *act0, const int *act1, SngCounters *sc,
-             double *scratch, long long nmax, int2 *done_list, int *tile_left,
+             double *scratch, double *fscratch, long long nmax, int2 *done_list, int *tile_left,
              unsigned long long *stats) {
   if (sc->mode != 1) return;
   const unsigned full = 0xffffffffu;
@@ -2372,6 +2377,15 @@ k_sng_finish(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
   ck.S = scratch + gw * 3 * nck * 32 + lane;
   ck.I = ck.S + nck * 32;
   ck.P = ck.I + nck * 32;
+  r1s_buf rb;
+  {
+    const long long len = nmax + 2;
+    rb.SI = (SPLIT ? fscratch : scratch) + gw * 5 * len;
+    rb.LP = rb.SI + len;
+    rb.PA = rb.LP + len;
+    rb.UM = rb.PA + len;
+    rb.ZV = rb.UM + len;
+  }
   const int *Ain = in ? act1 : act0;
   const int nin = sc->nin;
   const double rqtol = 2.0 * MR3_EPS;
@@ -2414,14 +2428,18 @@ k_sng_finish(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
       const double lam_call = (st.flags & SF_STEP2) ? st.bstw : st.lambda;
       const int r_in = (st.flags & SF_REWRITE) ? 0 : st.r;
       const bool write = (st.flags & (SF_REWRITE | SF_STEP2 | SF_USEDBS)) || st.k > 1;
-      r1c_state rs;
-      rs.r = 0; rs.mingma = 0.0; rs.sawnan = false; rs.slowA = false; rs.slowB = false;
       int negc = 0;
-      dv_r1c_factor(lane == 0, nb, lam_call, P, Q, ps, pivmin, !usedBS, r_in, ck, &negc, &rs);
       o.isupp1 = 1; o.isupp2 = nb; o.nrminv = 0.0; o.r = 0; o.resid = 0.0; o.rqcorr = 0.0;
-      if (lane == 0)
-        dv_r1c_solve(nb, lam_call, P, Q, ps, pivmin, st.gaptol, rs.r, rs.sawnan, rs.slowA,
-                     rs.slowB, ck.S, ck.P, rs.mingma, write ? zcol : nullptr, 1.0, &o);
+      if (SPLIT) {
+        dv_r1s_call(nb, lam_call, P, Q, ps, pivmin, !usedBS, r_in, st.gaptol, rb, &negc, &o);
+      } else {
+        r1c_state rs;
+        rs.r = 0; rs.mingma = 0.0; rs.sawnan = false; rs.slowA = false; rs.slowB = false;
+        dv_r1c_factor(lane == 0, nb, lam_call, P, Q, ps, pivmin, !usedBS, r_in, ck, &negc, &rs);
+        if (lane == 0)
+          dv_r1c_solve(nb, lam_call, P, Q, ps, pivmin, st.gaptol, rs.r, rs.sawnan, rs.slowA,
+                       rs.slowB, ck.S, ck.P, rs.mingma, write ? zcol : nullptr, 1.0, &o);
+      }
       o.r = __shfl_sync(full, o.r, 0);
       o.isupp1 = __shfl_sync(full, o.isupp1, 0);
       o.isupp2 = __shfl_sync(full, o.isupp2, 0);
@@ -2486,7 +2504,10 @@ k_sng_finish(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
     double *Zc = p->Z + (size_t)zind * p->ldz;
     __syncwarp();
     for (int row = lane; row < a; row += 32) Zc[row] = 0.0;
-    for (int row = a + lane; row < b; row += 32) Zc[row] = Zc[row] * o.nrminv;
+    if (SPLIT)   // the vector is in the warp's scratch (rows of the block, 1-based)
+      for (int row = a + lane; row < b; row += 32) Zc[row] = rb.ZV[row - bl0 + 1] * o.nrminv;
+    else
+      for (int row = a + lane; row < b; row += 32) Zc[row] = Zc[row] * o.nrminv;
     for (int row = b + lane; row < p->n; row += 32) Zc[row] = 0.0;
     __syncwarp();
     if (lane == 0) {
@@ -2657,6 +2678,8 @@ struct mr3_cuda_ctx {
   SngCounters *sc = nullptr;
   double *scratch = nullptr, *arena[2] = {nullptr, nullptr};
   double *qd = nullptr;                     // dqds arrays (4 doubles per row)
+  double *fscratch = nullptr;               // row scratch of the split finish
+  size_t capFscratch = 0;
   const double **Din = nullptr, **Ein = nullptr;
   double **Wp = nullptr, **Dp = nullptr, **Ep = nullptr;
   // pinned host mirrors
@@ -2879,7 +2902,7 @@ extern "C" void mr3_cuda_ctx_destroy(mr3_cuda_ctx *c) {
                  c->Dt, c->Lt, c->Wout, c->gers, c->TP, c->TPc, c->RP, c->RQ, c->rec0, c->rec1,
                  c->cl[0], c->cl[1], c->sng, c->sst, c->act[0], c->act[1], c->bsl, c->sflag, c->sbcnt, c->rl, c->rl_n, c->sbk, c->done_list, c->tile_left,
                  c->bis_nodes[0], c->bis_nodes[1], c->bis_cnt, c->bis_bcnt, c->bis_n, c->bis_st, c->lc, c->sc, c->scratch, c->arena[0],
-                 c->cls_ns, c->cls_soff, c->cls_cbase, c->cls_abase, c->qd,
+                 c->cls_ns, c->cls_soff, c->cls_cbase, c->cls_abase, c->qd, c->fscratch,
                  c->arena[1], (void *)c->Din, (void *)c->Ein, c->Wp, c->Dp, c->Ep};
   for (void *q : dev)
     if (q) cudaFree(q);
@@ -3453,14 +3476,38 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
         // (k_sng_finish), a warp each; MR3_FINISH_MAX overrides it (0: never)
         int finish_max = (int)nwarps;
         if (const char *ev = getenv("MR3_FINISH_MAX")) finish_max = atoi(ev);
+        // the split form of the finish (two sweeps at once): MR3_FINISH_SPLIT=1
+        bool split = false;
+        if (const char *ev = getenv("MR3_FINISH_SPLIT")) split = atoi(ev) != 0;
+        int fin_ctas = ctas_all;
+        if (split) {
+          // warps of the split finish: their row scratch (5 (nmax + 2) doubles
+          // each) kept within 2 GB, at least one CTA per SM
+          const size_t per = 5ull * ((size_t)nmaxV + 2) * sizeof(double);
+          size_t fw = std::min<size_t>(nwarps, std::max<size_t>((size_t)c->nsm * SNG_WARPS,
+                                                                ((size_t)2 << 30) / per));
+          fw = fw / SNG_WARPS * SNG_WARPS;
+          fin_ctas = (int)(fw / SNG_WARPS);
+          if (fw * per > c->capFscratch) {
+            CK(cudaStreamSynchronize(c->own), "fscratch sync");
+            CK(cudaStreamSynchronize(c->rnd), "fscratch sync");
+            CK(regrow(&c->fscratch, fw * per / sizeof(double)), "fscratch");
+            c->capFscratch = fw * per;
+          }
+        }
         for (int rd = 0; rd < SNG_ROUNDS; rd++) {
           const int in = rd & 1, last = rd == SNG_ROUNDS - 1;
           LAUNCH(k_round_reset, 1, 1, c->sc, in, rd == 0);
-          if (rd > 0)
-            LAUNCH(k_sng_finish, ctas_all, SNG_WARPS * 32, in, c->sng, c->cl[cur], c->probs,
-                   c->blocks, c->RP, c->RQ, c->arena[cur], c->W, c->Wsh, c->Werr, c->Wgap,
-                   c->Windex, c->Zindex, c->sst, c->act[0], c->act[1], c->sc, c->scratch,
-                   (long long)nmaxV, c->done_list, c->tile_left, stats);
+          if (rd > 0 && split)
+            LAUNCH(k_sng_finish<true>, fin_ctas, SNG_WARPS * 32, in, c->sng, c->cl[cur],
+                   c->probs, c->blocks, c->RP, c->RQ, c->arena[cur], c->W, c->Wsh, c->Werr,
+                   c->Wgap, c->Windex, c->Zindex, c->sst, c->act[0], c->act[1], c->sc,
+                   c->scratch, c->fscratch, (long long)nmaxV, c->done_list, c->tile_left, stats);
+          else if (rd > 0)
+            LAUNCH(k_sng_finish<false>, ctas_all, SNG_WARPS * 32, in, c->sng, c->cl[cur],
+                   c->probs, c->blocks, c->RP, c->RQ, c->arena[cur], c->W, c->Wsh, c->Werr,
+                   c->Wgap, c->Windex, c->Zindex, c->sst, c->act[0], c->act[1], c->sc,
+                   c->scratch, nullptr, (long long)nmaxV, c->done_list, c->tile_left, stats);
           if (rd == 0)
             LAUNCH_SMEM(k_sng_round<true>, ctas_first, SNG_WARPS * 32, smem, in, c->sng,
                         c->cl[cur], c->probs, c->blocks, c->RP, c->RQ, c->arena[cur], c->W, c->Wsh,

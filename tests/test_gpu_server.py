@@ -166,3 +166,24 @@ def test_server_budget_admits_in_turn():
     for k, (p, r) in enumerate(zip(reqs, res)):
         alone = M.mrrr(p["jobz"], p["range"], p["D"], p["E"], **_kw(p))
         assert_same(r, alone, f"request {k}")
+
+
+def test_server_bad_request_does_not_poison_its_batch():
+    """A request with a NaN in D, submitted among good ones, gets info 2; the
+    others, batched with it, equal their results alone."""
+    reqs = _c4_requests(10, seed=29)
+    bad = dict(reqs[4], D=reqs[4]["D"].copy())
+    bad["D"][3] = np.nan
+    reqs[4] = bad
+    S = M.Server()
+    try:
+        tickets = [S.submit(p) for p in reqs]
+        res = [S.poll(t, wait=True)[0] for t in tickets]
+    finally:
+        S.close()
+    for k, (p, r) in enumerate(zip(reqs, res)):
+        if k == 4:
+            assert r["info"] == 2 and r["m"] == 0
+            continue
+        alone = M.mrrr(p["jobz"], p["range"], p["D"], p["E"], **_kw(p))
+        assert_same(r, alone, f"request {k}")

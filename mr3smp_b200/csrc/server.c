@@ -56,6 +56,13 @@ __attribute__((visibility("hidden"))) int mr3__batched_on(mr3_cuda_ctx *ctx, int
 enum { T_QUEUED = 1, T_RUNNING = 2, T_DONE = 3 };
 enum { K_HOST = 0, K_DEVICE = 1 };
 
+/* One queued request as admission sees it. */
+typedef struct {
+  int kind, n;
+  size_t bytes;
+  double work;
+} mr3__srv_view;
+
 typedef struct {
   int kind, n;
   mr3_host_prob *hreq;
@@ -73,6 +80,9 @@ typedef struct {
   mr3_host_prob *hbatch;
   mr3_cuda_prob *dbatch;
   long long *ids;
+  mr3__srv_view *view;   /* the queued requests admission looks at */
+  long long *vpos;       /* and their queue positions */
+  int *pick;
 } srv_lane;
 
 struct mr3_server {
@@ -187,6 +197,30 @@ static int q_has_work(mr3_server *s, const srv_lane *L)
   return 0;
 }
 
+/* Admission of one batch, on its own so that it can be tested without a
+ * device: from nq queued requests in arrival order, the positions (in out,
+ * at most maxk) of those a lane takes -- requests of the kind of the first
+ * one taken, that the lane may take (small_only: n <= SRV_SMALL_N), that fit
+ * the budget left (budget - used) and that keep the batch's work within
+ * work_cap (the first one always does).  Returns their number. */
+int mr3__srv_admit(const mr3__srv_view *v, int nq, int small_only, size_t budget, size_t used,
+                   double work_cap, int maxk, int *out)
+{
+  int i, k = 0, kind = -1;
+  double work = 0.0;
+  for (i = 0; i < nq && k < maxk; i++) {
+    if (small_only && v[i].n > SRV_SMALL_N) continue;
+    if (kind >= 0 && v[i].kind != kind) continue;
+    if (used + v[i].bytes > budget) continue;
+    if (k > 0 && work + v[i].work > work_cap) continue;
+    kind = v[i].kind;
+    used += v[i].bytes;
+    work += v[i].work;
+    out[k++] = i;
+  }
+  return k;
+}
+
 typedef struct {
   mr3_server *s;
   int lane;
@@ -214,24 +248,30 @@ static void *lane_main(void *p)
     /* admission: queued requests in arrival order, of one kind, that fit the
      * budget left and the batch's work cap; a batch takes at least one */
     t0 = now_ms();
-    for (j = s->qhead; j < s->qtail && seen < SRV_SCAN && k < SRV_MAXBATCH; j++) {
-      srv_ticket *t = &s->t[s->q[j] - 1];
+    for (j = s->qhead; j < s->qtail && seen < SRV_SCAN; j++) {
+      const srv_ticket *t = &s->t[s->q[j] - 1];
       if (t->state != T_QUEUED) continue;
+      L->view[seen].kind = t->kind;
+      L->view[seen].n = t->n;
+      L->view[seen].bytes = t->bytes;
+      L->view[seen].work = t->work;
+      L->vpos[seen] = j;
       seen++;
-      if (!lane_wants(L, t)) continue;
-      if (kind >= 0 && t->kind != kind) continue;
-      if (s->used + t->bytes > s->budget) continue;
-      if (k > 0 && work + t->work > s->work_cap) continue;
+    }
+    k = mr3__srv_admit(L->view, (int)seen, L->small_only, s->budget, s->used, s->work_cap,
+                       SRV_MAXBATCH, L->pick);
+    for (i = 0; i < k; i++) {
+      const long long id = s->q[L->vpos[L->pick[i]]];
+      srv_ticket *t = &s->t[id - 1];
       kind = t->kind;
       t->state = T_RUNNING;
       t->t_admit = t0;
       s->used += t->bytes;
       bytes += t->bytes;
       work += t->work;
-      L->ids[k] = s->q[j];
-      if (kind == K_HOST) L->hbatch[k] = *t->hreq;
-      else L->dbatch[k] = *t->dreq;
-      k++;
+      L->ids[i] = id;
+      if (kind == K_HOST) L->hbatch[i] = *t->hreq;
+      else L->dbatch[i] = *t->dreq;
     }
     if (k == 0) {
       /* everything this lane may take waits for budget: sleep until a
@@ -314,7 +354,10 @@ int mr3_server_create(int device, size_t budget_bytes, mr3_server **out)
     L->hbatch = (mr3_host_prob *)malloc(SRV_MAXBATCH * sizeof(mr3_host_prob));
     L->dbatch = (mr3_cuda_prob *)malloc(SRV_MAXBATCH * sizeof(mr3_cuda_prob));
     L->ids = (long long *)malloc(SRV_MAXBATCH * sizeof(long long));
-    if (!L->hbatch || !L->dbatch || !L->ids) goto fail;
+    L->view = (mr3__srv_view *)malloc(SRV_SCAN * sizeof(mr3__srv_view));
+    L->vpos = (long long *)malloc(SRV_SCAN * sizeof(long long));
+    L->pick = (int *)malloc(SRV_SCAN * sizeof(int));
+    if (!L->hbatch || !L->dbatch || !L->ids || !L->view || !L->vpos || !L->pick) goto fail;
     if (mr3_cuda_ctx_create_prio(device, L->small_only ? 1 : 0, &L->ctx) != MR3_OK) goto fail;
     a = (lane_arg *)malloc(sizeof(lane_arg));
     if (!a) goto fail;
@@ -452,6 +495,9 @@ void mr3_server_destroy(mr3_server *s)
     free(L->hbatch);
     free(L->dbatch);
     free(L->ids);
+    free(L->view);
+    free(L->vpos);
+    free(L->pick);
   }
   free(s->q);
   free(s->t);

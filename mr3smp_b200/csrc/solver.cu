@@ -1936,6 +1936,9 @@ __global__ void k_bucket_scan(int *bk) {
 // support in coalesced rows.
 // ------------------------------------------------------------------------
 #define SNG_WARPS 8
+#ifndef SNG_MINB
+#define SNG_MINB 2     // resident round blocks per SM the register budget is sized for
+#endif
 #define SNG_ROUNDS (MR3_MAXITER + 1)   // MAXITER loop calls and the step-2 call
 #define SNG_TILE_BYTES (SNG_WARPS * 32 * 33 * (int)sizeof(double))   // k_sng_round's z tiles
 enum { SF_USEDBS = 1, SF_USEDRQ = 2, SF_NEEDBS = 4, SF_STEP2 = 8, SF_REWRITE = 16 };
@@ -2104,7 +2107,7 @@ __global__ void __launch_bounds__(256) k_list_scatter(int first, const SngCounte
 }
 
 template <bool FIRST>
-__global__ void __launch_bounds__(SNG_WARPS * 32, 2)
+__global__ void __launch_bounds__(SNG_WARPS * 32, SNG_MINB)
 k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
             const BlockDev *blocks, const double2 *RP, const double2 *RQ, const double *arena,
             double *W, double *Wsh, double *Werr, double *Wgap, const int *Windex,

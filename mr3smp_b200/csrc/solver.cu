@@ -29,6 +29,24 @@
 #include "mr3_device.cuh"
 
 #define MR3_THREADS 256
+// resident 128-thread blocks per SM that the bisection and refinement
+// kernels' register budgets are sized for (0: the compiler's choice)
+#ifndef MR3_BIS_MINB
+#define MR3_BIS_MINB 0
+#endif
+#ifndef MR3_REF_MINB
+#define MR3_REF_MINB 0
+#endif
+#if MR3_BIS_MINB > 0
+#define LB_BIS __launch_bounds__(128, MR3_BIS_MINB)
+#else
+#define LB_BIS __launch_bounds__(128)
+#endif
+#if MR3_REF_MINB > 0
+#define LB_REF __launch_bounds__(128, MR3_REF_MINB)
+#else
+#define LB_REF __launch_bounds__(128)
+#endif
 
 // ------------------------------------------------------------------------
 // Device-side records
@@ -778,7 +796,7 @@ k_bis_scatter(const BisNode *in, const int *n_in_dev, const ProbDev *probs, cons
 
 // The single eigenvalues that left the tree, a thread each, continued with
 // dv_bisect_one from their state.
-__global__ void __launch_bounds__(128)
+__global__ void LB_BIS
 k_bisect_cont(int N, const ProbDev *probs, const BlockDev *blocks, const int *blk_of_row,
               const double2 *TP, double *Wt, double *Et, int *It, const BisState *st, Tol tol,
               unsigned long long *stats) {
@@ -1106,7 +1124,7 @@ __device__ __forceinline__ unsigned long long refine_root_body(int s, const Prob
 }
 
 template <bool TREE>
-__global__ void __launch_bounds__(128)
+__global__ void LB_REF
 k_refine_root(int N, int L, const ProbDev *probs, const BlockDev *blocks, const int *iblk,
               const double2 *RP, double *W, double *Werr, const double *Wgap, Tol tol,
               unsigned long long *stats) {
@@ -1499,7 +1517,7 @@ __device__ __forceinline__ void own_rrr(const ClusterDev &C, const BlockDev &B, 
 // Both calls see a zero right gap, so their convergence test does not depend
 // on any other gap and the two ends are independent.
 template <bool TREE>
-__global__ void __launch_bounds__(128)
+__global__ void LB_REF
 k_cl_ext(int ncl, int L, const ClusterDev *cl, const ProbDev *probs, const BlockDev *blocks,
          const double2 *RP, const double2 *RQ, const double *arena_prev, const double *Wsh,
          const double *Werr, const int *Windex, double *xw, double *xe, Tol tol,
@@ -1665,7 +1683,7 @@ __host__ __device__ __forceinline__ int tree_lanes(long long items, long long la
 }
 
 template <bool TREE>
-__global__ void __launch_bounds__(128)
+__global__ void LB_REF
 k_refine_cl(const int *rl, const int *rl_n, const ClusterDev *cl, const ProbDev *probs,
             const BlockDev *blocks, const double *arena_cur, double *Wsh, double *Werr,
             const double *Wgap, const int *Windex, const int *cl_of_slot, const int *lvl_of_slot,

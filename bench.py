@@ -165,7 +165,7 @@ def cpu_reference(problems, budget_s: float):
     import oracle
     if oracle.ref_lib() is None:
         return None, {"unavailable": "reference library oracle/_ref not built"}
-    cores, logical = host_cores()
+    phys, cores = host_cores()   # all the host threads the reference can use
     os.environ["PMR_NUM_THREADS"] = str(cores)
     os.environ["OPENBLAS_NUM_THREADS"] = "1"
     ns = [len(D) for D, E in problems]
@@ -195,11 +195,12 @@ def cpu_reference(problems, budget_s: float):
             pairs += r["m"]
         else:
             bad += 1
-    info = {"value": pairs / el, "unit": "eigenpairs/s", "cores": cores, "logical_cpus": logical,
+    info = {"value": pairs / el, "unit": "eigenpairs/s", "cores": cores, "physical_cores": phys,
             "kind": "reference",
             "sample": f"{len(sample)} of {len(ns)} problems stratified by n "
                       f"({pairs} checked eigenpairs, {el:.1f} s in mrrr()), "
-                      f"PMR_NUM_THREADS={cores} (physical cores), OPENBLAS_NUM_THREADS=1",
+                      f"PMR_NUM_THREADS={cores} (every host thread; {phys} physical cores), "
+                      "OPENBLAS_NUM_THREADS=1",
             "mrrr_seconds": el, "checked": True, "checked_problems": len(sample), "checked_bad": bad,
             "checked_worst_resid_orth": worst,
             "check": "every sampled result: info, count, residual; orthogonality of all "

@@ -157,7 +157,7 @@ def check_host_result(D, E, r, rng):
 def cpu_reference(problems, budget_s: float):
     """Time the reference mrrr() (oracle/_ref) problem by problem on a
     stratified sample whose predicted cost is about budget_s seconds, with
-    PMR_NUM_THREADS = the physical cores.  Every result is checked outside
+    PMR_NUM_THREADS = every host thread.  Every result is checked outside
     the timed calls (the reference's asserts are compiled out): a problem
     with info != 0, a wrong count, or residual or orthogonality above 10
     (units n eps ||T||, n eps) is a failure and its eigenpairs do not count.

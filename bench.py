@@ -774,8 +774,10 @@ def main():
         del PT, precs, single
 
     # end to end through the C ABI with pinned host buffers
-    # the batch's device arrays (56 GB of Z) are no longer needed
+    # the batch's device arrays (56 GB of Z) and the timed solver's
+    # workspaces are no longer needed
     del T, recs
+    S.close()
     torch.cuda.empty_cache()
 
     large = None

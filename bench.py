@@ -259,35 +259,52 @@ class _ZPool:
 
     def __init__(self, budget):
         import threading
-        self.budget, self.held = budget, 0
+        self.budget, self.held, self.out = budget, 0, 0
         self.free = {}
         self.cv = threading.Condition()
 
+    def _drop_idle(self, need):
+        for k, v in self.free.items():
+            while v and (need is None or self.held + need > self.budget):
+                v.pop()
+                self.held -= 8 * k
+
     def get(self, size):
         import torch
-        with self.cv:
-            while True:
-                lst = self.free.get(size)
-                if lst:
-                    return lst.pop()
-                if self.held + 8 * size <= self.budget:
-                    self.held += 8 * size
-                    break
-                # drop idle buffers of other sizes before waiting
-                dropped = False
-                for k, v in self.free.items():
-                    while v and self.held + 8 * size > self.budget:
-                        v.pop()
-                        self.held -= 8 * k
-                        dropped = True
-                if dropped and self.held + 8 * size <= self.budget:
-                    self.held += 8 * size
-                    break
-                self.cv.wait()
-        return torch.empty(max(size, 1), dtype=torch.float64, device="cuda")
+        while True:
+            with self.cv:
+                while True:
+                    lst = self.free.get(size)
+                    if lst:
+                        self.out += 1
+                        return lst.pop()
+                    if self.held + 8 * size <= self.budget:
+                        self.held += 8 * size
+                        break
+                    self._drop_idle(8 * size)   # idle buffers of other sizes first
+                    if self.held + 8 * size <= self.budget:
+                        self.held += 8 * size
+                        break
+                    self.cv.wait()
+            try:
+                buf = torch.empty(max(size, 1), dtype=torch.float64, device="cuda")
+                with self.cv:
+                    self.out += 1
+                return buf
+            except torch.OutOfMemoryError:
+                # the device holds less than the budget: give the bytes back,
+                # drop idle buffers, and wait for a request in flight to finish
+                with self.cv:
+                    self.held -= 8 * size
+                    self._drop_idle(None)
+                    torch.cuda.empty_cache()
+                    if self.out == 0:
+                        raise
+                    self.cv.wait(timeout=1.0)
 
     def put(self, size, buf):
         with self.cv:
+            self.out -= 1
             self.free.setdefault(size, []).append(buf)
             self.cv.notify_all()
 
@@ -341,6 +358,14 @@ def run_serving(M, wl, rates, count: int, seed: int, budget: int):
                 for t in ts:
                     S.poll(t, wait=True)
                 pool.put(n * c, z)
+        # the lanes' workspaces now hold their largest sizes: the eigenvector
+        # budget is what the device has left beside them (at most the
+        # configured budget), with 6 GB of headroom for growing work arrays
+        with pool.cv:
+            pool._drop_idle(None)
+        torch.cuda.empty_cache()
+        free_b = int(torch.cuda.mem_get_info()[0])
+        pool.budget = max(1 << 30, min(budget, free_b - (6 << 30)))
         for rate in rates:
             Dt.copy_(D0t)
             Et.copy_(E0t)
@@ -365,11 +390,16 @@ def run_serving(M, wl, rates, count: int, seed: int, budget: int):
             qwait = np.zeros(count)
             done_t = np.zeros(count)
             bad = [0]
+            okm = np.zeros(count, dtype=np.int64)
             ready = threading.Semaphore(0)
+
+            stop = [False, count]   # a failed submission ends the stream at stop[1]
 
             def poller():
                 for k in range(count):
                     ready.acquire()
+                    if stop[0] and k >= stop[1]:
+                        break
                     t, t_arr, t_sub = sub[k]
                     (info, m, _), l = S.poll(t, wait=True, raw=True)
                     done_t[k] = time.perf_counter()
@@ -378,48 +408,66 @@ def run_serving(M, wl, rates, count: int, seed: int, budget: int):
                     qwait[k] = (t_sub - t_arr) * 1e3 + (tq[0] if tq else 0.0)
                     if info != 0 or m != cols[k]:
                         bad[0] += 1
+                    else:
+                        okm[k] = 1
                     pool.put(int(ns[k] * cols[k]), zbuf[k])
                     zbuf[k] = None
 
-            th = threading.Thread(target=poller)
+            th = threading.Thread(target=poller, daemon=True)
             th.start()
             t0 = time.perf_counter()
-            for k in range(count):
-                ta = t0 + arrivals[k]
-                d = ta - time.perf_counter()
-                if d > 0:
-                    time.sleep(d)
-                z = pool.get(int(ns[k] * cols[k]))   # waits while the budget is full
-                zbuf[k] = z
-                reqs[k].Z = z.data_ptr()
-                ts = time.perf_counter()
-                sub[k] = (S.submit_device(None, req=reqs[k]), ta, ts)
+            error = None
+            try:
+                for k in range(count):
+                    ta = t0 + arrivals[k]
+                    d = ta - time.perf_counter()
+                    if d > 0:
+                        time.sleep(d)
+                    z = pool.get(int(ns[k] * cols[k]))   # waits while the budget is full
+                    zbuf[k] = z
+                    reqs[k].Z = z.data_ptr()
+                    ts = time.perf_counter()
+                    sub[k] = (S.submit_device(None, req=reqs[k]), ta, ts)
+                    ready.release()
+            except Exception as ex:   # record it; the requests already in flight finish
+                error = f"{type(ex).__name__}: {ex}"[:300]
+                stop[0], stop[1] = True, k
                 ready.release()
             th.join()
+            done_n = count if error is None else stop[1]
+            if done_n == 0:
+                out.append({"rate_per_s": rate, "error": error})
+                continue
+            lat, qwait, done_t = lat[:done_n], qwait[:done_n], done_t[:done_n]
             el = float(done_t.max() - t0)
             b1 = S.stats()
             by_n = {}
+            nsd = ns[:done_n]
             for n in SERVE_SIZES:
-                sel = lat[ns == n]
+                sel = lat[nsd == n]
                 if len(sel):
                     by_n[str(n)] = {"count": int(len(sel)),
                                     "p50_ms": round(float(np.percentile(sel, 50)), 3),
                                     "p99_ms": round(float(np.percentile(sel, 99)), 3)}
             nb = b1["batches"] - b0["batches"]
-            out.append({"rate_per_s": rate, "requests": count,
-                        "p50_ms": round(float(np.percentile(lat, 50)), 3),
-                        "p99_ms": round(float(np.percentile(lat, 99)), 3),
-                        "queue_p50_ms": round(float(np.percentile(qwait, 50)), 3),
-                        "eigenpairs_per_s": float(pairs.sum() / el),
-                        "requests_per_s": count / el, "failed": bad[0],
-                        "batches": nb, "requests_per_batch": round(count / max(nb, 1), 2),
-                        "batches_overlapping_others": b1["batches_overlapping_others"]
-                        - b0["batches_overlapping_others"],
-                        "by_n": by_n})
+            rec = {"rate_per_s": rate, "requests": done_n,
+                   "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                   "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                   "queue_p50_ms": round(float(np.percentile(qwait, 50)), 3),
+                   "eigenpairs_per_s": float((pairs[:done_n] * okm[:done_n]).sum() / el),
+                   "requests_per_s": done_n / el, "failed": bad[0],
+                   "batches": nb, "requests_per_batch": round(done_n / max(nb, 1), 2),
+                   "batches_overlapping_others": b1["batches_overlapping_others"]
+                   - b0["batches_overlapping_others"],
+                   "by_n": by_n}
+            if error:
+                rec["error"] = error
+            out.append(rec)
         lanes = S.stats()["lanes"]
     finally:
         S.close()
-    return {"streams": out, "lanes": lanes, "budget_gb": budget / 2**30,
+    return {"streams": out, "lanes": lanes, "budget_gb_configured": budget / 2**30,
+            "budget_gb": round(pool.budget / 2**30, 1),
             "mix": "n in {64,256,1024,4096,16384} w.p. {.4,.3,.2,.08,.02}; range A/I alternating "
                    "(I: il=1, iu=ceil(n/10)); D,E U(-1,1); jobz V",
             "api": "mr3_server_submit_device/poll (C ABI): D, E staged in HBM, W, Z, Zsupp "

@@ -61,6 +61,12 @@ int  mr3_cuda_ctx_create(int device, mr3_cuda_ctx **out);
  * blocks ahead of those of normal-priority streams (no preemption of
  * blocks already running).  The serving lanes for small requests use it. */
 int  mr3_cuda_ctx_create_prio(int device, int high, mr3_cuda_ctx **out);
+
+/* Bound (bytes, at least 64 MB; default 8 GB) of the checkpoint scratch of
+ * the eigenvector rounds' persistent warps: fewer warps run the rounds when
+ * 3 (n_max/4 + 1) 32 doubles per warp do not fit it.  Serving lanes, several
+ * contexts on one device, use a smaller bound. */
+int  mr3_cuda_ctx_set_round_scratch(mr3_cuda_ctx *ctx, size_t bytes);
 void mr3_cuda_ctx_destroy(mr3_cuda_ctx *ctx);
 
 /* Solve nprob problems in one batched pass on `stream` (a cudaStream_t, or

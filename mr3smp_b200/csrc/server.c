@@ -359,6 +359,9 @@ int mr3_server_create(int device, size_t budget_bytes, mr3_server **out)
     L->pick = (int *)malloc(SRV_SCAN * sizeof(int));
     if (!L->hbatch || !L->dbatch || !L->ids || !L->view || !L->vpos || !L->pick) goto fail;
     if (mr3_cuda_ctx_create_prio(device, L->small_only ? 1 : 0, &L->ctx) != MR3_OK) goto fail;
+    /* several lanes share the device: 2 GB of round scratch each (enough
+     * warps for a 16384-row request's singletons) */
+    mr3_cuda_ctx_set_round_scratch(L->ctx, (size_t)2 << 30);
     a = (lane_arg *)malloc(sizeof(lane_arg));
     if (!a) goto fail;
     a->s = s;

@@ -2701,6 +2701,7 @@ struct mr3_cuda_ctx {
   double *qd = nullptr;                     // dqds arrays (4 doubles per row)
   double *fscratch = nullptr;               // row scratch of the split finish
   size_t capFscratch = 0;
+  size_t round_scratch = (size_t)8 << 30;   // bound of the round warps' checkpoint scratch
   const double **Din = nullptr, **Ein = nullptr;
   double **Wp = nullptr, **Dp = nullptr, **Ep = nullptr;
   // pinned host mirrors
@@ -2945,6 +2946,12 @@ extern "C" void mr3_cuda_ctx_destroy(mr3_cuda_ctx *c) {
   if (c->rnd_done) cudaEventDestroy(c->rnd_done);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
+}
+
+extern "C" int mr3_cuda_ctx_set_round_scratch(mr3_cuda_ctx *c, size_t bytes) {
+  if (!c || bytes < ((size_t)64 << 20)) return MR3_EARG;
+  c->round_scratch = bytes;
+  return MR3_OK;
 }
 
 extern "C" void *mr3_cuda_ws(mr3_cuda_ctx *c, int slot, size_t bytes) {
@@ -3413,7 +3420,7 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
              c->Zindex, c->done_list, c->tile_left);
     // singleton scratch: the checkpoints of 32 lanes per persistent warp
     const size_t per_warp = 3ull * ((size_t)nmaxV / CK_K + 1) * 32ull;
-    const size_t budget = (size_t)8 << 30;   // bytes
+    const size_t budget = c->round_scratch;   // bytes
     // persistent warps: no more than can be resident at once
     const size_t resident = (size_t)c->nsm * (size_t)c->sng_ctas_per_sm * SNG_WARPS;
     size_t nwarps = std::min<size_t>(resident, std::max<size_t>(c->nsm, budget / (per_warp * 8)));

@@ -34,7 +34,9 @@
  * Settings (environment, read at create): MR3_SERVE_LANES (lanes, default
  * 4, at most 16), MR3_SERVE_SMALL_LANES (lanes reserved for small
  * requests, default 2), MR3_SERVE_BATCH_WORK (work cap of a batch in units
- * of eigenvector entries n*m, default 2^27).
+ * of eigenvector entries n*m, default 2^27, for the small-request lanes;
+ * the other lanes take 8 times as much, so that several large solves --
+ * each latency-bound alone -- share one pass).
  */
 #include <pthread.h>
 #include <stdlib.h>
@@ -258,8 +260,10 @@ static void *lane_main(void *p)
       L->vpos[seen] = j;
       seen++;
     }
-    k = mr3__srv_admit(L->view, (int)seen, L->small_only, s->budget, s->used, s->work_cap,
-                       SRV_MAXBATCH, L->pick);
+    /* large requests are latency-bound solves that batch well together:
+     * lanes of any size take 8 times the work of the small-request lanes */
+    k = mr3__srv_admit(L->view, (int)seen, L->small_only, s->budget, s->used,
+                       L->small_only ? s->work_cap : 8.0 * s->work_cap, SRV_MAXBATCH, L->pick);
     for (i = 0; i < k; i++) {
       const long long id = s->q[L->vpos[L->pick[i]]];
       srv_ticket *t = &s->t[id - 1];

@@ -47,6 +47,14 @@
 #else
 #define LB_REF __launch_bounds__(128)
 #endif
+#ifndef MR3_RRF_MINB
+#define MR3_RRF_MINB 0
+#endif
+#if MR3_RRF_MINB > 0
+#define LB_RRF __launch_bounds__(128, MR3_RRF_MINB)
+#else
+#define LB_RRF __launch_bounds__(128)
+#endif
 
 // ------------------------------------------------------------------------
 // Device-side records
@@ -1563,7 +1571,7 @@ k_cl_ext(int ncl, int L, const ClusterDev *cl, const ProbDev *probs, const Block
 // thread per cluster, after storing the refined extremes and the gap right of
 // the first eigenvalue (computed against its neighbour's value before the
 // second extreme was refined).
-__global__ void __launch_bounds__(128)
+__global__ void LB_RRF
 k_cl_rrf(int ncl, ClusterDev *cl, const ProbDev *probs, const BlockDev *blocks, const double2 *RP,
          const double2 *RQ, const double *arena_prev, double *arena_cur, const double *xw,
          const double *xe, double *Wsh, double *Werr, double *Wgap, unsigned long long *stats) {

@@ -1170,8 +1170,6 @@ k_refine_root(int N, int L, const ProbDev *probs, const BlockDev *blocks, const 
   stat_add(stats, KID_REFROOT * 4 + 1, work);
 }
 
-// Final gaps of the root refinement (dlarrb loop 111) and the last gap of the
-// block (SRC/mrrr_val.c:1080-1082).
 // The eigenvalues of a dqds block (SRC/mrrr_val.c:459-506): one thread per
 // block builds the qd array of its definite root representation in qd
 // (4 doubles per row of the block), runs dqds, and writes the wanted ones,
@@ -1203,6 +1201,8 @@ __global__ void k_dqds(int N, ProbDev *probs, const BlockDev *blocks, const int 
   }
 }
 
+// Final gaps of the root refinement (dlarrb loop 111) or of a dqds block, and
+// the last gap of the block (SRC/mrrr_val.c:1080-1082).
 __global__ void k_gaps_root(int N, const ProbDev *probs, const BlockDev *blocks, const int *iblk,
                             const double *W, const double *Werr, double *Wgap) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1211,7 +1211,10 @@ __global__ void k_gaps_root(int N, const ProbDev *probs, const BlockDev *blocks,
   const ProbDev *p = &probs[B->prob];
   if (p->status || B->nbl < 2) return;
   int wend = B->wbgn + B->mbl - 1;
-  if (s < wend) Wgap[s] = fmax(0.0, W[s + 1] - Werr[s + 1] - W[s] - Werr[s]);
+  // dlarrb's loop 111 subtracts term by term; the dqds branch groups the
+  // bounds (SRC/mrrr_val.c:501-503)
+  if (s < wend) Wgap[s] = B->dqds ? fmax(0.0, (W[s + 1] - Werr[s + 1]) - (W[s] + Werr[s]))
+                                  : fmax(0.0, W[s + 1] - Werr[s + 1] - W[s] - Werr[s]);
   else Wgap[s] = fmax(0.0, (p->vu_out - B->sigma) - (W[s] + Werr[s]));
 }
 

@@ -1969,7 +1969,19 @@ __global__ void k_bucket_scan(int *bk) {
 #define SNG_MINB 2     // resident round blocks per SM the register budget is sized for
 #endif
 #define SNG_ROUNDS (MR3_MAXITER + 1)   // MAXITER loop calls and the step-2 call
+// The back-substitution of a round: each lane on its own rows from its own
+// twist index (default), or the warp in lock-step through shared-memory z
+// tiles written as coalesced column segments (MR3_SNG_LOCKSTEP=1).  The
+// lock-step form sweeps the union of its lanes' ranges; with the localized
+// supports of most eigenvectors that is many times each lane's own range.
+#ifndef MR3_SNG_LOCKSTEP
+#define MR3_SNG_LOCKSTEP 0
+#endif
+#if MR3_SNG_LOCKSTEP
 #define SNG_TILE_BYTES (SNG_WARPS * 32 * 33 * (int)sizeof(double))   // k_sng_round's z tiles
+#else
+#define SNG_TILE_BYTES 0
+#endif
 enum { SF_USEDBS = 1, SF_USEDRQ = 2, SF_NEEDBS = 4, SF_STEP2 = 8, SF_REWRITE = 16 };
 
 // Loop variables of one singleton between rounds
@@ -2155,7 +2167,9 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
   const int nin = sc->nin;
   const double rqtol = 2.0 * MR3_EPS;
   __shared__ SngState sm_st[SNG_WARPS * 32];
+#if MR3_SNG_LOCKSTEP
   extern __shared__ double ztile[];   // SNG_WARPS tiles of 32 x 33 doubles
+#endif
   unsigned long long w_r1v = 0, w_sweep = 0, w_chunks = 0;
   for (;;) {
     int base = 0;
@@ -2220,12 +2234,17 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
     dv_r1c_factor(active, nb, lam_call, P, Q, ps, pivmin, !usedBS, r_in, ck, &negc, &rs);
     dlar1v_out o;
     o.isupp1 = 1; o.isupp2 = nb; o.nrminv = 0.0; o.r = 0; o.resid = 0.0; o.rqcorr = 0.0;
-    // z of the support goes to the column unscaled (through the warp's
-    // tile, in coalesced column segments); an accepted vector is scaled
-    // below (z * nrminv, the reference's dscal after dlar1v)
+    // z of the support goes to the column unscaled; an accepted vector is
+    // scaled below (z * nrminv, the reference's dscal after dlar1v)
+#if MR3_SNG_LOCKSTEP
     dv_r1w_solve(active, nb, lam_call, P, Q, ps, pivmin, gaptol, rs.r, rs.sawnan, rs.slowA,
                  rs.slowB, ck.S, ck.P, rs.mingma, zcol, write, ztile + (threadIdx.x >> 5) * 32 * 33,
                  &o);
+#else
+    if (active)
+      dv_r1c_solve(nb, lam_call, P, Q, ps, pivmin, gaptol, rs.r, rs.sawnan, rs.slowA, rs.slowB,
+                   ck.S, ck.P, rs.mingma, write ? zcol : nullptr, 1.0, &o);
+#endif
     SngState st = sm_st[threadIdx.x];
     const bool step2 = (st.flags & SF_STEP2) != 0;
     const bool rewrite = (st.flags & SF_REWRITE) != 0;

@@ -1659,6 +1659,12 @@ static __device__ __noinline__ void dv_r1v_solve(bool active, int n, const doubl
 #ifndef MR3_PROGR_DB
 #define MR3_PROGR_DB 1
 #endif
+// checkpoint blocks prefetched ahead (into L1) by the progressive sweep and
+// the back-substitution: the checkpoints of a round's warps are far larger
+// than L2, so each block's checkpoint comes from DRAM (0: none)
+#ifndef MR3_CKPF
+#define MR3_CKPF 0
+#endif
 
 // One lane's checkpoints; element j of each array at [j * 32].
 struct r1c_ck {
@@ -1686,7 +1692,7 @@ static __device__ __noinline__ bool dv_r1c_statio(double lambda, const double2 *
                                            int r1, int r2, double *__restrict__ ckS,
                                            double *__restrict__ ckI, int *neg1o, double *sr1o,
                                            double *silasto) {
-  constexpr int U = MR3_U;
+  constexpr int U = (MR3_U < CK_K) ? MR3_U : CK_K;
   static_assert(CK_K % U == 0, "chunks must not straddle checkpoint blocks");
   const int last = r2 - 1;
   int neg1 = 0;
@@ -1803,6 +1809,20 @@ static __device__ __noinline__ double dv_r1c_progr(bool active, int n, double la
     load(jtop, cp, cq);
 #endif
     for (int jb = jtop; jb >= jbot; jb--) {
+#if MR3_CKPF > 0
+      // only blocks inside this lane's own rows [r1, top]
+      if (work && (jb - MR3_CKPF) * CK_K + 1 >= r1 && (jb - MR3_CKPF + 1) * CK_K <= top) {
+        const int jf = jb - MR3_CKPF, bf = jf * CK_K + 1;
+        pf_l1(&P[(size_t)(bf - 1) * ps]);
+        pf_l1(&P[(size_t)(bf + CK_K - 2) * ps]);
+        if (SEARCH && search) {
+          pf_l1(&Q[(size_t)(bf - 1) * ps]);
+          pf_l1(&Q[(size_t)(bf + CK_K - 2) * ps]);
+          pf_l1(&ckS[(size_t)jf * 32]);
+          pf_l1(&ckI[(size_t)jf * 32]);
+        }
+      }
+#endif
 #if MR3_PROGR_DB
       if (jb - 1 >= jbot) {
         load(jb - 1, np_, nq);
@@ -1963,6 +1983,9 @@ static __device__ __noinline__ void dv_r1c_solve(int n, double lambda, const dou
       double lpa[CK_K], lda[CK_K];
       double s = s_next;
       if (jb > 0) s_next = ckS[(size_t)(jb - 1) * 32];
+#if MR3_CKPF > 0
+      if (jb - MR3_CKPF >= 0) pf_l1(&ckS[(size_t)(jb - MR3_CKPF) * 32]);
+#endif
 #pragma unroll
       for (int u = 0; u < CK_K; u++) {
         const int i = base + u;
@@ -2018,6 +2041,9 @@ static __device__ __noinline__ void dv_r1c_solve(int n, double lambda, const dou
       double uma[CK_K], lda[CK_K];
       double p = p_next;
       if (jb < jlast) p_next = ckP[(size_t)(jb + 1) * 32];
+#if MR3_CKPF > 0
+      if (jb + MR3_CKPF <= jlast) pf_l1(&ckP[(size_t)(jb + MR3_CKPF) * 32]);
+#endif
 #pragma unroll
       for (int u = CK_K - 1; u >= 0; u--) {
         const int i = base + u;

@@ -126,7 +126,10 @@ void *mr3_cuda_host_ws(mr3_cuda_ctx *ctx, size_t bytes);
 
 /* Profiling switch: with on = 1 every kernel launch is bracketed by CUDA
  * events on the solve's stream and the kernels add their work to device
- * counters; the accumulators are reset by every call of this function. */
+ * counters; the accumulators are reset by every call of this function.
+ * on = 2 also serialises the streams (the singleton rounds run on the
+ * solve's stream instead of beside the next level's cluster kernels), so
+ * that each kernel's time is its own, not shared with a concurrent one. */
 void mr3_cuda_profile(mr3_cuda_ctx *ctx, int on);
 
 /* Accumulated profile: up to `max` kernels (names as 32-byte strings, total

@@ -2071,7 +2071,7 @@ __global__ void __launch_bounds__(256) k_list_count(const SngCounters *sc,
 // Exclusive scan of the block counts (one block of 1024 threads); the totals
 // become the next list's length and the bisection list's length.
 __global__ void __launch_bounds__(1024) k_list_scan(int nblk, SngCounters *sc, int *bcnt, int out,
-                                                    int last_round, int finish_max) {
+                                                    int last_round, int finish_max, int iter_max) {
   __shared__ int wa[32], wb[32];
   __shared__ int carry[2];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -2107,9 +2107,13 @@ __global__ void __launch_bounds__(1024) k_list_scan(int nblk, SngCounters *sc, i
     sc->act_n[out] = carry[0];
     sc->bs_n = carry[1];
     if (last_round && (carry[0] | carry[1])) sc->err = 1;
-    // a short list is finished in one launch, a warp per singleton
+    // a short list is finished in one launch, a warp per singleton (mode 1)
+    // or a lane per singleton (mode 3: no more than a chunk per warp)
     const int left = carry[0] + carry[1];
-    if (!last_round && sc->mode == 0 && left > 0 && left <= finish_max) sc->mode = 1;
+    if (!last_round && sc->mode == 0 && left > 0) {
+      if (left <= finish_max) sc->mode = 1;
+      else if (left <= iter_max) sc->mode = 3;
+    }
   }
 }
 
@@ -2147,7 +2151,19 @@ __global__ void __launch_bounds__(256) k_list_scatter(int first, const SngCounte
   }
 }
 
-template <bool FIRST>
+// ITER (SngCounters.mode 3, a level's tail): every lane runs its singleton's
+// remaining Rayleigh-quotient loop to the end in this launch -- one dlar1v
+// call per pass of the warp, a bisection (SRC/process_singleton.c:178-192)
+// by the whole warp with the tree bisection when a lane's step left its
+// interval -- instead of one call per round.  A tail round lasts as long as
+// the largest block's dlar1v whatever the list's length; here the tail's
+// calls follow one another without the rounds' launches between them.
+// Every call and state update is the one the rounds make (the same bits).
+// The last block to finish empties the list (mode 2).
+// KIND: SNG_LATER (rounds after the first), SNG_FIRST (the first round of a
+// level: the state starts from the eigenvalue's refinement), SNG_ITER.
+enum { SNG_LATER = 0, SNG_FIRST = 1, SNG_ITER = 2 };
+template <int KIND>
 __global__ void __launch_bounds__(SNG_WARPS * 32, SNG_MINB)
 k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
             const BlockDev *blocks, const double2 *RP, const double2 *RQ, const double *arena,
@@ -2155,6 +2171,8 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
             const int *Zindex, SngState *sst, const int *act0, const int *act1,
             unsigned char *flag, SngCounters *sc, double *scratch, long long nmax,
             int2 *done_list, int *tile_left, unsigned long long *stats) {
+  constexpr bool FIRST = KIND == SNG_FIRST, ITER = KIND == SNG_ITER;
+  if (ITER && sc->mode != 3) return;
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
@@ -2170,7 +2188,7 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
 #if MR3_SNG_LOCKSTEP
   extern __shared__ double ztile[];   // SNG_WARPS tiles of 32 x 33 doubles
 #endif
-  unsigned long long w_r1v = 0, w_sweep = 0, w_chunks = 0;
+  unsigned long long w_r1v = 0, w_sweep = 0, w_chunks = 0, w_neg = 0;
   for (;;) {
     int base = 0;
     if (lane == 0) base = atomicAdd(&sc->act_next[in], 32);
@@ -2182,8 +2200,10 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
     const int j = active ? base + lane : base;
     const int idx = FIRST ? j : Ain[j];
     const int s = sng[idx].slot;
+    bool live = active;   // ITER: this lane's singleton is not finished yet
+    do {
     int nb;
-    double pivmin, lam_call, gaptol;
+    double pivmin, lam_call, gaptol, bspd;
     const double2 *P, *Q;
     double *zcol;   // the eigenvector's column of Z at the block's first row
     int ps, r_in;
@@ -2197,6 +2217,7 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
       nb = B.nbl;
       const ProbDev *pd = &probs[B.prob];
       pivmin = pd->pivmin;
+      bspd = C.bl_spdiam;
       zcol = pd->Z + (size_t)Zindex[s] * pd->ldz + (B.ibgn - pd->off);
       own_rrr(C, B, RP, RQ, arena, &P, &Q, &ps);
       SngState st;
@@ -2225,37 +2246,37 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
       // before it) is practically never accepted: its eigenvalue carries
       // the refinement's error, far above the acceptance test's tolerance.
       // Its vector is not written; in the rare case that it is accepted,
-      // the next round repeats the identical call and writes the vector.
+      // the next call repeats the identical call and writes the vector.
       write = (st.flags & (SF_REWRITE | SF_STEP2 | SF_USEDBS)) || st.k > 1;
     }
     r1c_state rs;
     rs.r = 0; rs.mingma = 0.0; rs.sawnan = false; rs.slowA = false; rs.slowB = false;
     int negc = 0;
-    dv_r1c_factor(active, nb, lam_call, P, Q, ps, pivmin, !usedBS, r_in, ck, &negc, &rs);
+    dv_r1c_factor(live, nb, lam_call, P, Q, ps, pivmin, !usedBS, r_in, ck, &negc, &rs);
     dlar1v_out o;
     o.isupp1 = 1; o.isupp2 = nb; o.nrminv = 0.0; o.r = 0; o.resid = 0.0; o.rqcorr = 0.0;
     // z of the support goes to the column unscaled; an accepted vector is
     // scaled below (z * nrminv, the reference's dscal after dlar1v)
 #if MR3_SNG_LOCKSTEP
-    dv_r1w_solve(active, nb, lam_call, P, Q, ps, pivmin, gaptol, rs.r, rs.sawnan, rs.slowA,
+    dv_r1w_solve(live, nb, lam_call, P, Q, ps, pivmin, gaptol, rs.r, rs.sawnan, rs.slowA,
                  rs.slowB, ck.S, ck.P, rs.mingma, zcol, write, ztile + (threadIdx.x >> 5) * 32 * 33,
                  &o);
 #else
-    if (active)
+    if (live)
       dv_r1c_solve(nb, lam_call, P, Q, ps, pivmin, gaptol, rs.r, rs.sawnan, rs.slowA, rs.slowB,
                    ck.S, ck.P, rs.mingma, write ? zcol : nullptr, 1.0, &o);
 #endif
     SngState st = sm_st[threadIdx.x];
     const bool step2 = (st.flags & SF_STEP2) != 0;
     const bool rewrite = (st.flags & SF_REWRITE) != 0;
-    const int nb_sweep = __reduce_max_sync(full, active ? nb : 0);
+    const int nb_sweep = __reduce_max_sync(full, live ? nb : 0);
     if (lane == 0) { w_chunks++; w_sweep += nb_sweep; }
     bool done = false, tobs = false;
-    if (active) {
+    if (live) {
       w_r1v += nb;
       st.r = o.r;
       if (rewrite) {
-        done = true;   // the decision was taken in the round before
+        done = true;   // the decision was taken in the call before
       } else if (step2) {
         st.lambda = st.bstw;
         done = true;
@@ -2292,54 +2313,98 @@ k_sng_round(int in, const SngDev *sng, const ClusterDev *cl, ProbDev *probs,
         }
       }
     }
-    // unfinished singletons: state saved, flagged for the next round's list
-    // (or the bisection list); the compaction keeps the list order
-    if (active && !done) sst[idx] = st;
-    if (active) flag[base + lane] = done ? 0 : (tobs ? 2 : 1);
+    if (!ITER) {
+      // unfinished singletons: state saved, flagged for the next round's
+      // list (or the bisection list); the compaction keeps the list order
+      if (live && !done) sst[idx] = st;
+      if (live) flag[base + lane] = done ? 0 : (tobs ? 2 : 1);
+    } else {
+      // the bisections the rounds would send to k_sng_bisect, one lane's
+      // singleton at a time by the whole warp (same bits as k_sng_bisect)
+      for (unsigned bm = __ballot_sync(full, tobs); bm; bm &= bm - 1) {
+        const int v = __ffs(bm) - 1;
+        const int nbv = __shfl_sync(full, nb, v), psv = __shfl_sync(full, ps, v);
+        const int wiv = __shfl_sync(full, Windex[s], v);
+        const double pvm = __shfl_sync(full, pivmin, v), spd = __shfl_sync(full, bspd, v);
+        const double2 *Pv = (const double2 *)__shfl_sync(full, (unsigned long long)P, v);
+        const int rv = __shfl_sync(full, st.r, v);
+        double wsh = __shfl_sync(full, st.wsh, v), werr = __shfl_sync(full, st.werr, v);
+        const int maxitr = dv_itmax(spd + pvm, pvm);
+        const int tw = (rv < 1 || rv > nbv) ? nbv : rv;
+        int nc = 0;
+        dv_dlarrb_tree(32, nbv, Pv, psv, wiv, 1, 0, 0.0, 0.0, 0.0, 2.0 * MR3_EPS, pvm, maxitr, tw,
+                       &wsh, &werr, &nc);
+        wsh = __shfl_sync(full, wsh, 0);
+        werr = __shfl_sync(full, werr, 0);
+        if (lane == 0) w_neg += (unsigned long long)nc * nbv;
+        if (lane == v) {
+          st.wsh = wsh;
+          st.werr = werr;
+          st.flags = (st.flags | SF_USEDBS) & ~SF_NEEDBS;
+          st.lambda = st.wsh;
+          st.r = 0;
+        }
+      }
+      if (live && !done) sst[idx] = st;
+    }
     // finished eigenvectors out
     const unsigned fin = __ballot_sync(full, done);
-    if (!fin) continue;
-    const ClusterDev &Cf = cl[sng[idx].cl];
-    const BlockDev &B = blocks[Cf.blk];
-    ProbDev *p = &probs[B.prob];
-    const int bl0 = B.ibgn - p->off;   // block's first row inside the problem
-    int zind = 0;
-    if (done) {
-      Wsh[s] = st.lambda;
-      Werr[s] = st.werr;
-      Wgap[s] = st.gap;
-      W[s] = st.lambda + Cf.sigma;
-      zind = Zindex[s];
-      p->Zsupp[2 * (size_t)zind] = o.isupp1 + bl0;
-      p->Zsupp[2 * (size_t)zind + 1] = o.isupp2 + bl0;
+    live = live && !done;
+    if (fin) {
+      const ClusterDev &Cf = cl[sng[idx].cl];
+      const BlockDev &B = blocks[Cf.blk];
+      ProbDev *p = &probs[B.prob];
+      const int bl0 = B.ibgn - p->off;   // block's first row inside the problem
+      int zind = 0;
+      if (done) {
+        Wsh[s] = st.lambda;
+        Werr[s] = st.werr;
+        Wgap[s] = st.gap;
+        W[s] = st.lambda + Cf.sigma;
+        zind = Zindex[s];
+        p->Zsupp[2 * (size_t)zind] = o.isupp1 + bl0;
+        p->Zsupp[2 * (size_t)zind + 1] = o.isupp2 + bl0;
+      }
+      // the accepted vectors, one column at a time by the whole warp: the
+      // support scaled by nrminv, the rows outside the support (and outside
+      // the block) zero
+      const int ldz = p->ldz, np = p->n;
+      const int z1 = bl0 + o.isupp1 - 1, z2 = bl0 + o.isupp2;   // support rows [z1, z2)
+      __syncwarp();
+      for (unsigned m = fin; m; m &= m - 1) {
+        const int v = __ffs(m) - 1;
+        const int npv = __shfl_sync(full, np, v), zc = __shfl_sync(full, zind, v);
+        const int a = __shfl_sync(full, z1, v), b = __shfl_sync(full, z2, v);
+        const int ldv = __shfl_sync(full, ldz, v);
+        const double nv = __shfl_sync(full, o.nrminv, v);
+        double *Zc = (double *)__shfl_sync(full, (unsigned long long)p->Z, v) + (size_t)zc * ldv;
+        for (int row = lane; row < a; row += 32) Zc[row] = 0.0;
+        for (int row = a + lane; row < b; row += 32) Zc[row] = Zc[row] * nv;
+        for (int row = b + lane; row < npv; row += 32) Zc[row] = 0.0;
+      }
+      __syncwarp();
+      if (done) {   // this lane's column is complete (its zero rows included)
+        __threadfence();
+        column_done(p, B.prob, zind, sc, done_list, tile_left);
+      }
     }
-    // the accepted vectors, one column at a time by the whole warp: the
-    // support scaled by nrminv, the rows outside the support (and outside
-    // the block) zero
-    const int ldz = p->ldz, np = p->n;
-    const int z1 = bl0 + o.isupp1 - 1, z2 = bl0 + o.isupp2;   // support rows [z1, z2)
-    __syncwarp();
-    for (unsigned m = fin; m; m &= m - 1) {
-      const int v = __ffs(m) - 1;
-      const int npv = __shfl_sync(full, np, v), zc = __shfl_sync(full, zind, v);
-      const int a = __shfl_sync(full, z1, v), b = __shfl_sync(full, z2, v);
-      const int ldv = __shfl_sync(full, ldz, v);
-      const double nv = __shfl_sync(full, o.nrminv, v);
-      double *Zc = (double *)__shfl_sync(full, (unsigned long long)p->Z, v) + (size_t)zc * ldv;
-      for (int row = lane; row < a; row += 32) Zc[row] = 0.0;
-      for (int row = a + lane; row < b; row += 32) Zc[row] = Zc[row] * nv;
-      for (int row = b + lane; row < npv; row += 32) Zc[row] = 0.0;
-    }
-    __syncwarp();
-    if (done) {   // this lane's column is complete (its zero rows included)
-      __threadfence();
-      column_done(p, B.prob, zind, sc, done_list, tile_left);
-    }
+    } while (ITER && __any_sync(full, live));
   }
   stat_add(stats, KID_SNG * 4 + 2, w_r1v);
+  if (ITER) stat_add(stats, KID_SNG * 4 + 1, w_neg);
   // diagnostics: warp-level row sweeps and warp chunks
   stat_add(stats, KID_OTHER * 4 + 0, w_sweep);
   stat_add(stats, KID_OTHER * 4 + 1, w_chunks);
+  if (ITER) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      if (atomicAdd(&sc->fin_ctas, 1) == (int)gridDim.x - 1) {
+        sc->nin = 0;
+        sc->mode = 2;
+      }
+    }
+  }
 }
 
 // The bisection of a singleton whose Rayleigh-quotient step left its
@@ -2927,14 +2992,16 @@ extern "C" int mr3_cuda_ctx_create_prio(int device, int high, mr3_cuda_ctx **out
     return MR3_EMISC;
   }
   int nb = 0;
-  if (cudaFuncSetAttribute(k_sng_round<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (cudaFuncSetAttribute(k_sng_round<SNG_LATER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            SNG_TILE_BYTES) != cudaSuccess ||
-      cudaFuncSetAttribute(k_sng_round<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(k_sng_round<SNG_ITER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           SNG_TILE_BYTES) != cudaSuccess ||
+      cudaFuncSetAttribute(k_sng_round<SNG_FIRST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            SNG_TILE_BYTES) != cudaSuccess) {
     mr3_cuda_ctx_destroy(c);
     return MR3_EMISC;
   }
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_sng_round<false>, SNG_WARPS * 32,
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_sng_round<SNG_LATER>, SNG_WARPS * 32,
                                                     SNG_TILE_BYTES) == cudaSuccess &&
       nb > 0)
     c->sng_ctas_per_sm = nb;
@@ -3521,8 +3588,11 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
         // the level's singletons in rounds (see k_sng_round), on their own
         // stream: the next level's cluster kernels (which read and write
         // neither their records nor their eigenvalue slots) run beside the
-        // rounds' short tail
-        cudaStream_t st = c->rnd;
+        // rounds' short tail.  Profiling with serialised streams (prof 2)
+        // keeps them on the solve's stream, so that every kernel's events
+        // bracket that kernel alone.
+        const cudaStream_t st_solve = st;
+        cudaStream_t st = (c->prof == 2) ? st_solve : c->rnd;
         rounds_pending = true;
         const int nsng = c->h_sc->n_sng;
         const int ctas_all = (int)(nwarps / SNG_WARPS);
@@ -3530,12 +3600,19 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
         const size_t smem = SNG_TILE_BYTES;
         const int bis_ctas = c->nsm * 4;
         const int nblk = (nsng + LIST_T - 1) / LIST_T;
-        // a list of at most this many singletons is finished in one launch
-        // (k_sng_finish), a warp each; MR3_FINISH_MAX overrides it (0: never)
-        int finish_max = (int)nwarps;
+        // a list of at most this many singletons (one per SM) is finished in
+        // one launch (k_sng_finish), a warp each; MR3_FINISH_MAX overrides it
+        // (0: never)
+        int finish_max = c->nsm;
         if (const char *ev = getenv("MR3_FINISH_MAX")) finish_max = atoi(ev);
-        // the split form of the finish (two sweeps at once): MR3_FINISH_SPLIT=1
-        bool split = false;
+        // a list of at most this many (a chunk of 32 per persistent warp) is
+        // finished in one launch, a lane each (k_sng_round<SNG_ITER>);
+        // MR3_ITER_MAX overrides it (0: never)
+        int iter_max = (int)std::min<size_t>(32 * nwarps, 1u << 30);
+        if (const char *ev = getenv("MR3_ITER_MAX")) iter_max = atoi(ev);
+        // the split form of the finish (two sweeps at once, half the latency
+        // of a call); MR3_FINISH_SPLIT=0 gives lane 0's checkpointed form
+        bool split = true;
         if (const char *ev = getenv("MR3_FINISH_SPLIT")) split = atoi(ev) != 0;
         int fin_ctas = ctas_all;
         if (split) {
@@ -3566,14 +3643,20 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
                    c->probs, c->blocks, c->RP, c->RQ, c->arena[cur], c->W, c->Wsh, c->Werr,
                    c->Wgap, c->Windex, c->Zindex, c->sst, c->act[0], c->act[1], c->sc,
                    c->scratch, nullptr, (long long)nmaxV, c->done_list, c->tile_left, stats);
+          if (rd > 0)
+            LAUNCH_SMEM(k_sng_round<SNG_ITER>, ctas_all, SNG_WARPS * 32, smem, in, c->sng,
+                        c->cl[cur], c->probs, c->blocks, c->RP, c->RQ, c->arena[cur], c->W, c->Wsh,
+                        c->Werr, c->Wgap, c->Windex, c->Zindex, c->sst, c->act[0], c->act[1],
+                        c->sflag, c->sc, c->scratch, (long long)nmaxV, c->done_list, c->tile_left,
+                        stats);
           if (rd == 0)
-            LAUNCH_SMEM(k_sng_round<true>, ctas_first, SNG_WARPS * 32, smem, in, c->sng,
+            LAUNCH_SMEM(k_sng_round<SNG_FIRST>, ctas_first, SNG_WARPS * 32, smem, in, c->sng,
                         c->cl[cur], c->probs, c->blocks, c->RP, c->RQ, c->arena[cur], c->W, c->Wsh,
                         c->Werr, c->Wgap, c->Windex, c->Zindex, c->sst, c->act[0], c->act[1],
                         c->sflag, c->sc, c->scratch, (long long)nmaxV, c->done_list, c->tile_left,
                         stats);
           else
-            LAUNCH_SMEM(k_sng_round<false>, ctas_all, SNG_WARPS * 32, smem, in, c->sng,
+            LAUNCH_SMEM(k_sng_round<SNG_LATER>, ctas_all, SNG_WARPS * 32, smem, in, c->sng,
                         c->cl[cur], c->probs, c->blocks, c->RP, c->RQ, c->arena[cur], c->W, c->Wsh,
                         c->Werr, c->Wgap, c->Windex, c->Zindex, c->sst, c->act[0], c->act[1],
                         c->sflag, c->sc, c->scratch, (long long)nmaxV, c->done_list, c->tile_left,
@@ -3585,7 +3668,7 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
             npend++;
           }
           LAUNCH(k_list_count, nblk, 256, c->sc, c->sflag, c->sbcnt);
-          LAUNCH(k_list_scan, 1, 1024, nblk, c->sc, c->sbcnt, in ^ 1, last, finish_max);
+          LAUNCH(k_list_scan, 1, 1024, nblk, c->sc, c->sbcnt, in ^ 1, last, finish_max, iter_max);
           LAUNCH(k_list_scatter, nblk, 256, rd == 0, c->sc, c->sflag, c->sbcnt, c->act[0],
                  c->act[1], in, c->bsl);
           if (!last) {

@@ -1610,7 +1610,7 @@ k_cl_rrf(int ncl, ClusterDev *cl, const ProbDev *probs, const BlockDev *blocks, 
 // one CTA per sibling group, rows of the group's members interleaved.
 __global__ void k_cl_pack(int ncl, const ClusterDev *cl, const BlockDev *blocks, double *arena_cur,
                           double *Wsh, double *Werr, int *cl_of_slot, int *lvl_of_slot, int level,
-                          int *rl, int *rl_n) {
+                          int *rl_n) {
   for (int w = blockIdx.x; w < ncl; w += gridDim.x) {
     const ClusterDev L0 = cl[w];
     if (L0.g != 0) continue;   // the group's first member packs the group
@@ -1631,14 +1631,10 @@ __global__ void k_cl_pack(int ncl, const ClusterDev *cl, const BlockDev *blocks,
         Werr[k] += f;
         cl_of_slot[k] = w + m;
         lvl_of_slot[k] = level;
-        // the level's refinement list (warp-aggregated, neighbours stay together)
-        const unsigned am = __activemask();
-        const int lead = __ffs(am) - 1, lane = threadIdx.x & 31;
-        int o = 0;
-        if (lane == lead) o = atomicAdd(rl_n, __popc(am));
-        o = __shfl_sync(am, o, lead);
-        rl[o + __popc(am & ((1u << lane) - 1u))] = k;
       }
+      // the level's refinement list is built in slot order from
+      // lvl_of_slot afterwards (k_rl_*); here only its length
+      if (threadIdx.x == 0) atomicAdd(rl_n, C.end - C.begin + 1);
     }
     for (long long idx = threadIdx.x; idx < nG; idx += blockDim.x) {
       const int i = (int)(idx / G);
@@ -1738,6 +1734,87 @@ k_refine_cl(const int *rl, const int *rl_n, const ClusterDev *cl, const ProbDev 
     }
   }
   stat_add(stats, KID_REFCL * 4 + 1, work);
+}
+
+// The level's refinement list in slot order: the slots that k_cl_pack
+// marked with this level.  Consecutive threads of k_refine_cl then take
+// neighbouring eigenvalues -- of one cluster, or of sibling clusters whose
+// representations are interleaved row by row in the arena -- so that a
+// warp's Sturm sweeps read common or adjacent rows, instead of the rows of
+// a dozen unrelated representations.  Count per 1024 slots, exclusive scan,
+// stable scatter.
+#define RL_T 1024
+__global__ void __launch_bounds__(256) k_rl_count(int N, const int *lvl, int level, int *bcnt) {
+  __shared__ int red[8];
+  const int base = blockIdx.x * RL_T;
+  int c = 0;
+  for (int q = 0; q < RL_T / 256; q++) {
+    const int k = base + q * 256 + threadIdx.x;
+    c += (k < N && lvl[k] == level);
+  }
+  c = __reduce_add_sync(0xffffffffu, c);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int a = 0;
+    for (int w = 0; w < 8; w++) a += red[w];
+    bcnt[blockIdx.x] = a;
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_rl_scan(int nblk, int *bcnt) {
+  __shared__ int wsum[32];
+  __shared__ int carry;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int b0 = 0; b0 < nblk; b0 += 1024) {
+    const int b = b0 + threadIdx.x;
+    const int a = b < nblk ? bcnt[b] : 0;
+    int x = a;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      int v = wsum[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += y;
+      }
+      wsum[lane] = v;
+    }
+    __syncthreads();
+    if (b < nblk) bcnt[b] = carry + (wid ? wsum[wid - 1] : 0) + x - a;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += wsum[31];
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) k_rl_scatter(int N, const int *lvl, int level,
+                                                    const int *bcnt, int *rl) {
+  __shared__ int wcnt[8];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int base = blockIdx.x * RL_T;
+  int pos = bcnt[blockIdx.x];
+  for (int q = 0; q < RL_T / 256; q++) {
+    const int k = base + q * 256 + threadIdx.x;
+    const bool f = k < N && lvl[k] == level;
+    const unsigned b = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) wcnt[wid] = __popc(b);
+    __syncthreads();
+    int before = 0, total = 0;
+    for (int w = 0; w < 8; w++) {
+      before += (w < wid) ? wcnt[w] : 0;
+      total += wcnt[w];
+    }
+    if (f) rl[pos + before + __popc(b & ((1u << lane) - 1u))] = k;
+    pos += total;
+    __syncthreads();
+  }
 }
 
 __global__ void k_gaps_cl(int N, const ClusterDev *cl, const double *Wsh, const double *Werr,
@@ -2775,7 +2852,7 @@ struct mr3_cuda_ctx {
   ClusterDev *cl[2] = {nullptr, nullptr};
   SngDev *sng = nullptr;
   SngState *sst = nullptr;
-  int *act[2] = {nullptr, nullptr}, *bsl = nullptr, *sbcnt = nullptr;
+  int *act[2] = {nullptr, nullptr}, *bsl = nullptr, *sbcnt = nullptr, *rlcnt = nullptr;
   int *rl = nullptr, *rl_n = nullptr;       // a level's cluster eigenvalues to refine
   int *sbk = nullptr;                       // singleton size buckets (3 x 16)
   BisNode *bis_nodes[2] = {nullptr, nullptr}; // shared-interval bisection: levels
@@ -2920,6 +2997,7 @@ static int ensure_rows(mr3_cuda_ctx *c, size_t N, size_t P) {
     CK(regrow(&c->rl, n), "rl");
     CK(regrow(&c->sflag, n), "sflag");
     CK(regrow(&c->sbcnt, 2 * (n / LIST_T + 1)), "sbcnt");
+    CK(regrow(&c->rlcnt, n / RL_T + 1), "rlcnt");
     CK(regrow(&c->bis_nodes[0], n / 2 + 1), "bis nodes");
     CK(regrow(&c->bis_nodes[1], n / 2 + 1), "bis nodes");
     CK(regrow(&c->bis_cnt, n / 2 + 1), "bis cnt");
@@ -3019,7 +3097,7 @@ extern "C" void mr3_cuda_ctx_destroy(mr3_cuda_ctx *c) {
                  c->prob_of_slot, c->cl_of_slot, c->lvl_of_slot, c->unit_list, c->flag, c->tmp2,
                  c->D, c->E, c->E2, c->Wt, c->Et, c->W, c->Werr, c->Wgap, c->Wcopy, c->Wsh,
                  c->Dt, c->Lt, c->Wout, c->gers, c->TP, c->TPc, c->RP, c->RQ, c->rec0, c->rec1,
-                 c->cl[0], c->cl[1], c->sng, c->sst, c->act[0], c->act[1], c->bsl, c->sflag, c->sbcnt, c->rl, c->rl_n, c->sbk, c->done_list, c->tile_left,
+                 c->cl[0], c->cl[1], c->sng, c->sst, c->act[0], c->act[1], c->bsl, c->sflag, c->sbcnt, c->rlcnt, c->rl, c->rl_n, c->sbk, c->done_list, c->tile_left,
                  c->bis_nodes[0], c->bis_nodes[1], c->bis_cnt, c->bis_bcnt, c->bis_n, c->bis_st, c->lc, c->sc, c->scratch, c->arena[0],
                  c->cls_ns, c->cls_soff, c->cls_cbase, c->cls_abase, c->qd, c->fscratch,
                  c->arena[1], (void *)c->Din, (void *)c->Ein, c->Wp, c->Dp, c->Ep};
@@ -3550,7 +3628,13 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
                c->arena[nxt], c->arena[cur], c->Wt, c->Et, c->Wsh, c->Werr, c->Wgap, stats);
         CK(cudaMemsetAsync(c->rl_n, 0, sizeof(int), st), "rl_n");
         LAUNCH(k_cl_pack, std::min(ncl, 65535 * 16), 256, ncl, c->cl[cur], c->blocks, c->arena[cur],
-               c->Wsh, c->Werr, c->cl_of_slot, c->lvl_of_slot, level, c->rl, c->rl_n);
+               c->Wsh, c->Werr, c->cl_of_slot, c->lvl_of_slot, level, c->rl_n);
+        {
+          const int nrb = (int)((NN + RL_T - 1) / RL_T);
+          LAUNCH(k_rl_count, nrb, 256, NN, c->lvl_of_slot, level, c->rlcnt);
+          LAUNCH(k_rl_scan, 1, 1024, nrb, c->rlcnt);
+          LAUNCH(k_rl_scatter, nrb, 256, NN, c->lvl_of_slot, level, c->rlcnt, c->rl);
+        }
         // both forms are launched; the one that does not match the list's
         // length returns at once (the length is known on the device only)
         LAUNCH(k_refine_cl<false>, gN128, 128, c->rl, c->rl_n, c->cl[cur], c->probs, c->blocks,
@@ -3600,19 +3684,21 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
         const size_t smem = SNG_TILE_BYTES;
         const int bis_ctas = c->nsm * 4;
         const int nblk = (nsng + LIST_T - 1) / LIST_T;
-        // a list of at most this many singletons (one per SM) is finished in
-        // one launch (k_sng_finish), a warp each; MR3_FINISH_MAX overrides it
-        // (0: never)
-        int finish_max = c->nsm;
+        // a list of at most this many singletons (one per persistent warp) is
+        // finished in one launch (k_sng_finish), a warp each; MR3_FINISH_MAX
+        // overrides it (0: never)
+        int finish_max = (int)nwarps;
         if (const char *ev = getenv("MR3_FINISH_MAX")) finish_max = atoi(ev);
-        // a list of at most this many (a chunk of 32 per persistent warp) is
-        // finished in one launch, a lane each (k_sng_round<SNG_ITER>);
-        // MR3_ITER_MAX overrides it (0: never)
-        int iter_max = (int)std::min<size_t>(32 * nwarps, 1u << 30);
+        // MR3_ITER_MAX: a list of at most this many is finished in one launch,
+        // a lane each (k_sng_round<SNG_ITER>).  Off by default: a warp then
+        // waits for its slowest lane and runs its lanes' bisections one after
+        // another, and the step took longer than with the rounds (1049 ms
+        // against 1009 ms on the 4096-problem batch, 279 ms against 178 ms on
+        // a 256-problem one).
+        int iter_max = 0;
         if (const char *ev = getenv("MR3_ITER_MAX")) iter_max = atoi(ev);
-        // the split form of the finish (two sweeps at once, half the latency
-        // of a call); MR3_FINISH_SPLIT=0 gives lane 0's checkpointed form
-        bool split = true;
+        // the split form of the finish (two sweeps at once): MR3_FINISH_SPLIT=1
+        bool split = false;
         if (const char *ev = getenv("MR3_FINISH_SPLIT")) split = atoi(ev) != 0;
         int fin_ctas = ctas_all;
         if (split) {

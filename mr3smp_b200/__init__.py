@@ -481,8 +481,10 @@ class Solver:
     def last_launches(self) -> int:
         return int(self._L.mr3_cuda_last_launches(self._ctx))
 
-    def profile(self, on: bool):
-        self._L.mr3_cuda_profile(self._ctx, 1 if on else 0)
+    def profile(self, on: int | bool):
+        """0/False off; 1/True per-kernel events and work counters; 2 the
+        same with the streams serialised (each kernel's time its own)."""
+        self._L.mr3_cuda_profile(self._ctx, int(on))
 
     def profile_read(self):
         """-> (dict kernel -> (ms_total, launches), counters[6][4])."""

@@ -1651,7 +1651,7 @@ static __device__ __noinline__ void dv_r1v_solve(bool active, int n, const doubl
 // column of Z when asked to (a second call after the vector is accepted).
 // ------------------------------------------------------------------------
 #ifndef CK_K
-#define CK_K 4
+#define CK_K 2   // 4 keeps a quarter of the checkpoints but spills in the search sweep
 #endif
 // 1: the progressive sweep double-buffers the next block's rows in
 // registers; 0: it loads a block's rows when it reaches it, prefetched into

@@ -3697,8 +3697,10 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
         // a 256-problem one).
         int iter_max = 0;
         if (const char *ev = getenv("MR3_ITER_MAX")) iter_max = atoi(ev);
-        // the split form of the finish (two sweeps at once): MR3_FINISH_SPLIT=1
-        bool split = false;
+        // the split form of the finish (two sweeps at once, about half the
+        // latency of a call); MR3_FINISH_SPLIT=0 gives lane 0's checkpointed
+        // form
+        bool split = true;
         if (const char *ev = getenv("MR3_FINISH_SPLIT")) split = atoi(ev) != 0;
         int fin_ctas = ctas_all;
         if (split) {

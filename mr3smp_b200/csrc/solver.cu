@@ -22,6 +22,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <string>
 #include <vector>
 
@@ -120,7 +121,8 @@ struct SngCounters {
                                // rounds; nin: entries of this round's list
   int done_n, done_exp;        // finished column tiles: listed, exported to the host
   int mode, fin_ctas;          // 0 rounds; 1 the next list is finished by k_sng_finish;
-                               // 2 finished (later rounds are empty)
+                               // 3 by k_sng_round<SNG_ITER>; 2 finished (later
+                               // rounds are empty)
 };
 
 // Output column zind of a problem is written.  Columns are counted in tiles
@@ -3718,6 +3720,10 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
             c->capFscratch = fw * per;
           }
         }
+        const bool trace_rounds = getenv("MR3_TRACE_ROUNDS") != nullptr;
+        auto trace_t0 = std::chrono::steady_clock::now();
+        if (trace_rounds) CK(cudaStreamSynchronize(st), "trace sync");
+        trace_t0 = std::chrono::steady_clock::now();
         for (int rd = 0; rd < SNG_ROUNDS; rd++) {
           const int in = rd & 1, last = rd == SNG_ROUNDS - 1;
           LAUNCH(k_round_reset, 1, 1, c->sc, in, rd == 0);
@@ -3757,6 +3763,18 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
           }
           LAUNCH(k_list_count, nblk, 256, c->sc, c->sflag, c->sbcnt);
           LAUNCH(k_list_scan, 1, 1024, nblk, c->sc, c->sbcnt, in ^ 1, last, finish_max, iter_max);
+          if (trace_rounds) {
+            // MR3_TRACE_ROUNDS=1: each round's list lengths and wall time on
+            // stderr (synchronises after every round; diagnostics only)
+            SngCounters h;
+            CK(cudaStreamSynchronize(st), "trace sync");
+            CK(cudaMemcpy(&h, c->sc, sizeof(SngCounters), cudaMemcpyDeviceToHost), "trace copy");
+            const auto now = std::chrono::steady_clock::now();
+            fprintf(stderr, "mr3 trace: level %d round %d: in %d, next %d, bisection %d, mode %d, "
+                    "%.2f ms\n", level, rd, h.nin, h.act_n[in ^ 1], h.bs_n, h.mode,
+                    std::chrono::duration<double, std::milli>(now - trace_t0).count());
+            trace_t0 = now;
+          }
           LAUNCH(k_list_scatter, nblk, 256, rd == 0, c->sc, c->sflag, c->sbcnt, c->act[0],
                  c->act[1], in, c->bsl);
           if (!last) {

@@ -249,92 +249,83 @@ static __device__ __noinline__ int dv_dlaneg(int n, const double2 *__restrict__ 
     if (gamma < 0.0) negcnt++;
     return negcnt;
   }
-  // The stationary rows 1..r-1 and the progressive rows n-1..r are two
-  // independent recurrences: block k of one runs beside block k of the
-  // other, row by row, so that their divisions overlap.  Each chain's
-  // operations, its NaN re-runs (per 128-row block, from the block's saved
-  // state) and its counts are those of the loops above; only integers are
-  // added in another order.
-  const int lastA = r - 1;
-  const int nA = lastA >= 1 ? (lastA + blklen - 1) / blklen : 0;
-  const int nB = (n - 1 >= r) ? (n - r + blklen - 1) / blklen : 0;
-  double p = P[(size_t)(n - 1) * ps].x - sigma;
-  double2 ca[U], na[U], cb[U], nb2[U];
-  if (nA > 0) {
+  if (r - 1 >= 1) {
+    const int last = r - 1;
+    double2 c[U], nx[U];
 #pragma unroll
-    for (int u = 0; u < U; u++) ca[u] = P[(size_t)(d_imin(1 + u, lastA) - 1) * ps];
-  }
-  if (nB > 0) {
+    for (int u = 0; u < U; u++) c[u] = P[(size_t)(d_imin(1 + u, last) - 1) * ps];
+    for (int bj = 1; bj <= last; bj += blklen) {
+      const int jend = d_imin(bj + blklen - 1, last);
+      int neg1 = 0;
+      const double bsav = t;
+      for (int j0 = bj; j0 <= jend; j0 += U) {
 #pragma unroll
-    for (int u = 0; u < U; u++) cb[u] = P[(size_t)(d_imax(n - 1 - u, r) - 1) * ps];
-  }
-  const int nk = d_imax(nA, nB);
-  for (int k = 0; k < nk; k++) {
-    const bool ha = k < nA, hb = k < nB;
-    const int bjA = 1 + k * blklen, jendA = d_imin(bjA + blklen - 1, lastA);
-    const int bjB = n - 1 - k * blklen, jendB = d_imax(bjB - blklen + 1, r);
-    const int lenA = ha ? jendA - bjA + 1 : 0, lenB = hb ? bjB - jendB + 1 : 0;
-    const int len = d_imax(lenA, lenB);
-    int neg1 = 0, neg2 = 0;
-    const double tsav = t, psav = p;
-    for (int o = 0; o < len; o += U) {
-      if (ha) {
+        for (int u = 0; u < U; u++) nx[u] = P[(size_t)(d_imin(j0 + U + u, last) - 1) * ps];
 #pragma unroll
-        for (int u = 0; u < U; u++) na[u] = P[(size_t)(d_imin(bjA + o + U + u, lastA) - 1) * ps];
+        for (int u = 0; u < U; u++) {
+          if (j0 + u <= jend) {
+            double dplus = c[u].x + t;
+            neg1 += (dplus < 0.0);
+            double tmp = t / dplus;
+            t = tmp * c[u].y - sigma;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) c[u] = nx[u];
       }
-      if (hb) {
-#pragma unroll
-        for (int u = 0; u < U; u++) nb2[u] = P[(size_t)(d_imax(bjB - o - U - u, r) - 1) * ps];
-      }
-#pragma unroll
-      for (int u = 0; u < U; u++) {
-        if (o + u < lenA) {
-          double dplus = ca[u].x + t;
+      if (isnan(t)) {
+        neg1 = 0;
+        t = bsav;
+        for (int j = bj; j <= jend; j++) {
+          const double2 v = P[(size_t)(j - 1) * ps];
+          double dplus = v.x + t;
           neg1 += (dplus < 0.0);
           double tmp = t / dplus;
-          t = tmp * ca[u].y - sigma;
+          if (isnan(tmp)) tmp = 1.0;
+          t = tmp * v.y - sigma;
         }
-        if (o + u < lenB) {
-          double dminus = cb[u].y + p;
+      }
+      negcnt += neg1;
+    }
+  }
+  double p = P[(size_t)(n - 1) * ps].x - sigma;
+  if (n - 1 >= r) {
+    double2 c[U], nx[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) c[u] = P[(size_t)(d_imax(n - 1 - u, r) - 1) * ps];
+    for (int bj = n - 1; bj >= r; bj -= blklen) {
+      const int jend = d_imax(bj - blklen + 1, r);
+      int neg2 = 0;
+      const double bsav = p;
+      for (int j0 = bj; j0 >= jend; j0 -= U) {
+#pragma unroll
+        for (int u = 0; u < U; u++) nx[u] = P[(size_t)(d_imax(j0 - U - u, r) - 1) * ps];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          if (j0 - u >= jend) {
+            double dminus = c[u].y + p;
+            neg2 += (dminus < 0.0);
+            double tmp = p / dminus;
+            p = tmp * c[u].x - sigma;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) c[u] = nx[u];
+      }
+      if (isnan(p)) {
+        neg2 = 0;
+        p = bsav;
+        for (int j = bj; j >= jend; j--) {
+          const double2 v = P[(size_t)(j - 1) * ps];
+          double dminus = v.y + p;
           neg2 += (dminus < 0.0);
           double tmp = p / dminus;
-          p = tmp * cb[u].x - sigma;
+          if (isnan(tmp)) tmp = 1.0;
+          p = tmp * v.x - sigma;
         }
       }
-      if (ha) {
-#pragma unroll
-        for (int u = 0; u < U; u++) ca[u] = na[u];
-      }
-      if (hb) {
-#pragma unroll
-        for (int u = 0; u < U; u++) cb[u] = nb2[u];
-      }
+      negcnt += neg2;
     }
-    if (ha && isnan(t)) {
-      neg1 = 0;
-      t = tsav;
-      for (int j = bjA; j <= jendA; j++) {
-        const double2 v = P[(size_t)(j - 1) * ps];
-        double dplus = v.x + t;
-        neg1 += (dplus < 0.0);
-        double tmp = t / dplus;
-        if (isnan(tmp)) tmp = 1.0;
-        t = tmp * v.y - sigma;
-      }
-    }
-    if (hb && isnan(p)) {
-      neg2 = 0;
-      p = psav;
-      for (int j = bjB; j >= jendB; j--) {
-        const double2 v = P[(size_t)(j - 1) * ps];
-        double dminus = v.y + p;
-        neg2 += (dminus < 0.0);
-        double tmp = p / dminus;
-        if (isnan(tmp)) tmp = 1.0;
-        p = tmp * v.x - sigma;
-      }
-    }
-    negcnt += neg1 + neg2;
   }
   double gamma = (t + sigma) + p;
   if (gamma < 0.0) negcnt++;

@@ -3686,10 +3686,14 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
         const size_t smem = SNG_TILE_BYTES;
         const int bis_ctas = c->nsm * 4;
         const int nblk = (nsng + LIST_T - 1) / LIST_T;
-        // a list of at most this many singletons (one per persistent warp) is
-        // finished in one launch (k_sng_finish), a warp each; MR3_FINISH_MAX
-        // overrides it (0: never)
-        int finish_max = (int)nwarps;
+        // a list of at most this many singletons (four per persistent warp)
+        // is finished in one launch (k_sng_finish), a warp each in turn;
+        // MR3_FINISH_MAX overrides it (0: never).  A level's last few
+        // thousand singletons are mostly ones that run all MAXITER calls and
+        // the bisection; one round per call for them cost more than their
+        // warps running the calls back to back (4096-problem batch: 44 ms
+        // less per step with four per warp than with one)
+        int finish_max = (int)std::min<size_t>(4 * nwarps, 1u << 30);
         if (const char *ev = getenv("MR3_FINISH_MAX")) finish_max = atoi(ev);
         // MR3_ITER_MAX: a list of at most this many is finished in one launch,
         // a lane each (k_sng_round<SNG_ITER>).  Off by default: a warp then

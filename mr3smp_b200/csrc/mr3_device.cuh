@@ -135,67 +135,6 @@ static __device__ __noinline__ int dv_bisect_one(int n, const double2 *__restric
   return 0;
 }
 
-// Two Sturm counts of the same T at two points in one pass over the rows:
-// each chain is dv_count_bisect's, operation for operation; the rows are
-// loaded once and the two chains' divisions overlap.
-static __device__ __forceinline__ void dv_count_bisect2(int n, const double2 *__restrict__ tp,
-                                                 double pivmin, double c0, double c1,
-                                                 int *cnt0, int *cnt1) {
-  double2 v = tp[0];
-  double t0 = v.x - c0, t1 = v.x - c1;
-  int k0 = 0, k1 = 0;
-  if (t0 <= pivmin) { k0 = 1; t0 = fmin(t0, -pivmin); }
-  if (t1 <= pivmin) { k1 = 1; t1 = fmin(t1, -pivmin); }
-  for (int j = 1; j < n; j++) {
-    v = tp[j];
-    t0 = v.x - v.y / t0 - c0;
-    t1 = v.x - v.y / t1 - c1;
-    if (t0 <= pivmin) { k0++; t0 = fmin(t0, -pivmin); }
-    if (t1 <= pivmin) { k1++; t1 = fmin(t1, -pivmin); }
-  }
-  *cnt0 = k0;
-  *cnt1 = k1;
-}
-
-// dv_bisect_one for two eigenvalues j0, j1 of the same T at once: while both
-// intervals are open their counts share a pass (dv_count_bisect2); each
-// interval's sequence of points, tests and results is dv_bisect_one's.
-struct BisIv {
-  double a, b;
-  int na, nb, it, j;
-};
-static __device__ __noinline__ void dv_bisect_two(int n, const double2 *__restrict__ tp,
-                                           double pivmin, double abstol, double reltol,
-                                           int itmax, BisIv *x, BisIv *y) {
-  double cx = 0.5 * (x->a + x->b), cy = 0.5 * (y->a + y->b);
-  bool gx = x->it + 1 <= itmax, gy = y->it + 1 <= itmax;
-  const double tol0 = fmax(abstol, pivmin);
-  while (gx || gy) {
-    int kx = 0, ky = 0;
-    if (gx && gy) dv_count_bisect2(n, tp, pivmin, cx, cy, &kx, &ky);
-    else if (gx) kx = dv_count_bisect(n, tp, pivmin, cx);
-    else ky = dv_count_bisect(n, tp, pivmin, cy);
-    if (gx) {
-      const int it = x->it + 1;
-      const int cnt = d_imin(x->nb, d_imax(x->na, kx));
-      if (x->j <= cnt) { x->b = cx; x->nb = cnt; } else { x->a = cx; x->na = cnt; }
-      const double w = fabs(x->b - x->a), t = fmax(fabs(x->b), fabs(x->a));
-      x->it = it;
-      if (w < fmax(tol0, reltol * t) || x->na >= x->nb || it + 1 > itmax) gx = false;
-      else cx = 0.5 * (x->a + x->b);
-    }
-    if (gy) {
-      const int it = y->it + 1;
-      const int cnt = d_imin(y->nb, d_imax(y->na, ky));
-      if (y->j <= cnt) { y->b = cy; y->nb = cnt; } else { y->a = cy; y->na = cnt; }
-      const double w = fabs(y->b - y->a), t = fmax(fabs(y->b), fabs(y->a));
-      y->it = it;
-      if (w < fmax(tol0, reltol * t) || y->na >= y->nb || it + 1 > itmax) gy = false;
-      else cy = 0.5 * (y->a + y->b);
-    }
-  }
-}
-
 // dv_bisect_one by a group of L lanes (L = 4..32; groups independent): the
 // midpoints of the next log2(L) steps form a binary tree that follows from
 // the current interval; lane t of the group counts at node max(t,1) (its

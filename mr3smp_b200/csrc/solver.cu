@@ -804,64 +804,28 @@ k_bis_scatter(const BisNode *in, const int *n_in_dev, const ProbDev *probs, cons
     }
 }
 
-// The single eigenvalues that left the tree, continued with dv_bisect_one
-// from their state: a thread each, or (PAIR) a thread for two neighbouring
-// slots, whose counts share a pass over the rows when both belong to one
-// block (dv_bisect_two: the same intervals, two division chains in flight).
-__device__ __forceinline__ bool bis_cont_load(int g, int N, const BlockDev *blocks,
-                                              const int *blk_of_row, const double *Wt,
-                                              const double *Et, const BisState *st,
-                                              const BlockDev **Bo, BisIv *v, int *it0) {
-  if (g >= N) return false;
-  const BisState q = st[g];
-  if (q.it < 0) return false;
-  const BlockDev *B = &blocks[blk_of_row[g]];
-  *Bo = B;
-  v->a = Wt[g]; v->b = Et[g]; v->na = q.na; v->nb = q.nb; v->it = q.it;
-  v->j = B->nab1 + 1 + (g - B->ibgn);
-  *it0 = q.it;
-  return true;
-}
-
-__device__ __forceinline__ unsigned long long bis_cont_store(int g, const BlockDev *B,
-                                                             const BisIv &v, int it0, double *Wt,
-                                                             double *Et, int *It) {
-  Wt[g] = 0.5 * (v.a + v.b);
-  Et[g] = 0.5 * fabs(v.a - v.b);
-  It[g] = v.j;
-  return (unsigned long long)(v.it - it0) * (unsigned long long)B->nbl;
-}
-
-template <bool PAIR>
+// The single eigenvalues that left the tree, a thread each, continued with
+// dv_bisect_one from their state.
 __global__ void LB_BIS
 k_bisect_cont(int N, const ProbDev *probs, const BlockDev *blocks, const int *blk_of_row,
               const double2 *TP, double *Wt, double *Et, int *It, const BisState *st, Tol tol,
               unsigned long long *stats) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long work = 0;
-  const int g0 = PAIR ? 2 * t : t;
-  const BlockDev *B0 = nullptr, *B1 = nullptr;
-  BisIv x, y;
-  int i0 = 0, i1 = 0;
-  const bool h0 = bis_cont_load(g0, N, blocks, blk_of_row, Wt, Et, st, &B0, &x, &i0);
-  const bool h1 = PAIR && bis_cont_load(g0 + 1, N, blocks, blk_of_row, Wt, Et, st, &B1, &y, &i1);
-  if (h0 && h1 && B0 == B1) {
-    const ProbDev *p = &probs[B0->prob];
-    dv_bisect_two(B0->nbl, TP + B0->ibgn, p->pivmin, B0->atoli, tol.bsrtol, B0->itmax2, &x, &y);
-    work += bis_cont_store(g0, B0, x, i0, Wt, Et, It);
-    work += bis_cont_store(g0 + 1, B1, y, i1, Wt, Et, It);
-  } else {
-    if (h0) {
-      const ProbDev *p = &probs[B0->prob];
-      dv_bisect_one(B0->nbl, TP + B0->ibgn, p->pivmin, B0->atoli, tol.bsrtol, B0->itmax2, x.j,
-                    &x.a, &x.b, x.na, x.nb, &x.it, i0);
-      work += bis_cont_store(g0, B0, x, i0, Wt, Et, It);
-    }
-    if (h1) {
-      const ProbDev *p = &probs[B1->prob];
-      dv_bisect_one(B1->nbl, TP + B1->ibgn, p->pivmin, B1->atoli, tol.bsrtol, B1->itmax2, y.j,
-                    &y.a, &y.b, y.na, y.nb, &y.it, i1);
-      work += bis_cont_store(g0 + 1, B1, y, i1, Wt, Et, It);
+  if (g < N) {
+    const BisState q = st[g];
+    if (q.it >= 0) {
+      const BlockDev *B = &blocks[blk_of_row[g]];
+      const ProbDev *p = &probs[B->prob];
+      const int j = B->nab1 + 1 + (g - B->ibgn);
+      double a = Wt[g], b = Et[g];
+      int it = q.it;
+      dv_bisect_one(B->nbl, TP + B->ibgn, p->pivmin, B->atoli, tol.bsrtol, B->itmax2, j, &a, &b,
+                    q.na, q.nb, &it, q.it);
+      Wt[g] = 0.5 * (a + b);
+      Et[g] = 0.5 * fabs(a - b);
+      It[g] = j;
+      work = (unsigned long long)(it - q.it) * (unsigned long long)B->nbl;
     }
   }
   stat_add(stats, KID_BISECT * 4 + 0, work);
@@ -3589,14 +3553,8 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
                c->bis_st);
         cur ^= 1;
       }
-      // MR3_BIS_PAIR=0: a thread per eigenvalue instead of per pair
-      static const bool pair = !getenv("MR3_BIS_PAIR") || atoi(getenv("MR3_BIS_PAIR")) != 0;
-      if (pair)
-        LAUNCH(k_bisect_cont<true>, (NN / 2 + 1 + 127) / 128, 128, NN, c->probs, c->blocks,
-               c->blk_of_row, c->TP, c->Wt, c->Et, c->It, c->bis_st, tol, stats);
-      else
-        LAUNCH(k_bisect_cont<false>, gN128, 128, NN, c->probs, c->blocks, c->blk_of_row, c->TP,
-               c->Wt, c->Et, c->It, c->bis_st, tol, stats);
+      LAUNCH(k_bisect_cont, gN128, 128, NN, c->probs, c->blocks, c->blk_of_row, c->TP, c->Wt,
+             c->Et, c->It, c->bis_st, tol, stats);
     } else
       LAUNCH(k_bisect<true>, (int)(((long long)NN * Lb + 127) / 128), 128, NN, Lb, c->probs,
              c->blocks, c->blk_of_row, c->TP, c->Wt, c->Et, c->It, tol, stats);

@@ -774,12 +774,15 @@ def main():
         achieved = per_launch / (avg_ms * 1e-3) * 1e-9
         traffic = None
         if tname == "k_sng_round":
-            # DRAM bytes per dlar1v row of the round kernels, measured with ncu
-            # (dram__bytes_read.sum + dram__bytes_write.sum) on a 256-problem
-            # mixed batch (n <= 1024), scaled by this run's dlar1v rows
-            traffic = {"bytes_per_launch": 25.5 * ctr[4][2] / max(tcnt, 1),
-                       "source": "ncu on a 256-problem mixed batch: 25.5 B per dlar1v row, "
-                                 "scaled by the live dlar1v-row counter"}
+            # DRAM bytes per dlar1v row of the singleton kernels, measured with
+            # ncu (dram__bytes_read.sum + dram__bytes_write.sum) on a
+            # 256-problem mixed batch (n <= 4096), scaled by this run's rows
+            traffic = {"bytes_per_launch": 48.4 * ctr[4][2] / max(tcnt, 1),
+                       "algorithmic_bytes_per_launch": zbytes / max(tcnt, 1),   # the Z write
+                       "source": "ncu on a 256-problem mixed batch (n <= 4096): 48.4 B per "
+                                 "dlar1v row (checkpoints and child representations; the "
+                                 "Z write is about 3 B per row), scaled by the live "
+                                 "dlar1v-row counter"}
         roof = {"bound": "fp64-div", "kernel": tname, "achieved": achieved,
                 "peak": div_gops, "unit": "Gdiv/s",
                 "frac": (achieved / div_gops) if div_gops else None,

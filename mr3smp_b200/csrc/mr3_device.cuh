@@ -2305,6 +2305,16 @@ struct r1s_buf {
   double *SI, *LP, *PA, *UM, *ZV;
 };
 
+// Rows the split form's sweeping lanes prefetch ahead of their arithmetic
+// (0: none).  A lane sweeps alone, so nothing else hides the latency of its
+// loads; the child representations live in DRAM.
+#ifndef MR3_R1S_PF
+#define MR3_R1S_PF 32
+#endif
+static __device__ __forceinline__ void pf_l2(const void *p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 static __device__ __noinline__ void dv_r1s_call(int n, double lambda, const double2 *__restrict__ P,
                                          const double2 *__restrict__ Q, int ps, double pivmin,
                                          bool wantnc, int r_in, double gaptol, r1s_buf b,
@@ -2327,6 +2337,10 @@ static __device__ __noinline__ void dv_r1s_call(int n, double lambda, const doub
       sr1 = 0.0;
 #pragma unroll 4
       for (int i = 1; i <= r2 - 1; i++) {
+        if (MR3_R1S_PF && i + MR3_R1S_PF <= r2 - 1) {
+          pf_l2(&P[(size_t)(i + MR3_R1S_PF - 1) * ps]);
+          pf_l2(&Q[(size_t)(i + MR3_R1S_PF - 1) * ps]);
+        }
         const double2 pp = P[(size_t)(i - 1) * ps], q = Q[(size_t)(i - 1) * ps];
         double dplus = pp.x + s;
         if (SLOW && fabs(dplus) < pivmin) dplus = -pivmin;
@@ -2355,6 +2369,10 @@ static __device__ __noinline__ void dv_r1s_call(int n, double lambda, const doub
       neg2 = 0;
 #pragma unroll 4
       for (int i = n - 1; i >= r1; i--) {
+        if (MR3_R1S_PF && i - MR3_R1S_PF >= r1) {
+          pf_l2(&P[(size_t)(i - MR3_R1S_PF - 1) * ps]);
+          pf_l2(&Q[(size_t)(i - MR3_R1S_PF - 1) * ps]);
+        }
         const double2 pp = P[(size_t)(i - 1) * ps];
         double dminus = pp.y + p;
         if (SLOW && fabs(dminus) < pivmin) dminus = -pivmin;
@@ -2409,6 +2427,10 @@ static __device__ __noinline__ void dv_r1s_call(int n, double lambda, const doub
     b.ZV[r] = 1.0;
     double zp = 1.0, zpp = 0.0;
     for (int i = r - 1; i >= 1; i--) {
+      if (MR3_R1S_PF && i - 16 >= 1) {   // the rows ahead into L1
+        pf_l1(&Q[(size_t)(i - 17) * ps]);
+        pf_l1(&b.LP[i - 16]);
+      }
       const double ldi = Q[(size_t)(i - 1) * ps].y;
       double zi;
       if (!slow) zi = -(b.LP[i] * zp);
@@ -2423,6 +2445,10 @@ static __device__ __noinline__ void dv_r1s_call(int n, double lambda, const doub
   } else if (lane == 1) {
     double zc = 1.0, zcp = 0.0;
     for (int i = r; i <= n - 1; i++) {
+      if (MR3_R1S_PF && i + 16 <= n - 1) {
+        pf_l1(&Q[(size_t)(i + 15) * ps]);
+        pf_l1(&b.UM[i + 16]);
+      }
       const double ldi = Q[(size_t)(i - 1) * ps].y;
       double zn;
       if (!slow) zn = -(b.UM[i] * zc);

@@ -358,20 +358,12 @@ def run_serving(M, wl, rates, count: int, seed: int, budget: int):
                 for t in ts:
                     S.poll(t, wait=True)
                 pool.put(n * c, z)
-        # the lanes' workspaces now hold their largest sizes: the eigenvector
-        # budget is what the device has left beside them (at most the
-        # configured budget), with 6 GB of headroom for growing work arrays
-        with pool.cv:
-            pool._drop_idle(None)
-        torch.cuda.empty_cache()
-        free_b = int(torch.cuda.mem_get_info()[0])
-        pool.budget = max(1 << 30, min(budget, free_b - (6 << 30)))
-        for rate in rates:
+        def stream(arrivals, count):
+            """Requests 0..count-1 of the mix, submitted at the given arrival
+            times (seconds from the start); one record."""
             Dt.copy_(D0t)
             Et.copy_(E0t)
             torch.cuda.synchronize()
-            arrivals = np.cumsum(np.random.default_rng(seed + int(rate)).exponential(1.0 / rate,
-                                                                                   size=count))
             reqs = []
             for k in range(count):
                 n, o = int(ns[k]), int(offs[k])
@@ -436,8 +428,7 @@ def run_serving(M, wl, rates, count: int, seed: int, budget: int):
             th.join()
             done_n = count if error is None else stop[1]
             if done_n == 0:
-                out.append({"rate_per_s": rate, "error": error})
-                continue
+                return {"error": error}
             lat, qwait, done_t = lat[:done_n], qwait[:done_n], done_t[:done_n]
             el = float(done_t.max() - t0)
             b1 = S.stats()
@@ -450,7 +441,7 @@ def run_serving(M, wl, rates, count: int, seed: int, budget: int):
                                     "p50_ms": round(float(np.percentile(sel, 50)), 3),
                                     "p99_ms": round(float(np.percentile(sel, 99)), 3)}
             nb = b1["batches"] - b0["batches"]
-            rec = {"rate_per_s": rate, "requests": done_n,
+            rec = {"requests": done_n,
                    "p50_ms": round(float(np.percentile(lat, 50)), 3),
                    "p99_ms": round(float(np.percentile(lat, 99)), 3),
                    "queue_p50_ms": round(float(np.percentile(qwait, 50)), 3),
@@ -462,7 +453,26 @@ def run_serving(M, wl, rates, count: int, seed: int, budget: int):
                    "by_n": by_n}
             if error:
                 rec["error"] = error
-            out.append(rec)
+            return rec
+
+        # a burst of the mix before the timed streams: every lane meets its
+        # largest batches (work arrays at their steady-state sizes) before
+        # the budget for eigenvectors is fixed and the streams are timed
+        nburst = min(count, 2000)
+        stream(np.zeros(nburst), nburst)
+        # the lanes' workspaces now hold their largest sizes: the eigenvector
+        # budget is what the device has left beside them (at most the
+        # configured budget), with 6 GB of headroom for growing work arrays
+        with pool.cv:
+            pool._drop_idle(None)
+        torch.cuda.empty_cache()
+        free_b = int(torch.cuda.mem_get_info()[0])
+        pool.budget = max(1 << 30, min(budget, free_b - (6 << 30)))
+        for rate in rates:
+            arrivals = np.cumsum(np.random.default_rng(seed + int(rate)).exponential(1.0 / rate,
+                                                                                   size=count))
+            rec = stream(arrivals, count)
+            out.append({"rate_per_s": rate, **rec})
         lanes = S.stats()["lanes"]
     finally:
         S.close()

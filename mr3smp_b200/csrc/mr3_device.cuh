@@ -2535,6 +2535,14 @@ static __device__ __forceinline__ double rrf_sweep(int n, const double2 *__restr
 // Parent rows: d = P[i].x, l = Q[i].x, ld = Q[i].y.  w/wgap/werr point at the
 // cluster's first eigenvalue (CLSTRT = 1, CLEND = clend).  dplus, lplus: out;
 // work: 2n scratch.  Returns the shift sigma.
+// PAIR: two lanes (an even lane and the next odd one) per cluster, with the
+// same arguments; the even lane sweeps the left shift while the odd one
+// sweeps the right shift, so that a try costs one sweep's time instead of
+// two when the left shift fails.  The right sweep is run even when the left
+// one is accepted; its output (the work array) is then not used, so the
+// result -- the shift and the representation in dplus/lplus -- is the
+// sequential one bit for bit.  Both lanes return the shift.
+template <bool PAIR>
 static __device__ __noinline__ double dv_dlarrf(int n, const double2 *__restrict__ P,
                                          const double2 *__restrict__ Q, int ps, int clend,
                                          const double *w, const double *wgap, const double *werr,
@@ -2570,13 +2578,32 @@ static __device__ __noinline__ double dv_dlarrf(int n, const double2 *__restrict
     bool sawnan1 = false, sawnan2 = false;
     ldelta = fmin(ldmax, ldelta);
     rdelta = fmin(rdmax, rdelta);
-    max1 = rrf_sweep(n, P, Q, ps, lsigma, pivmin, dp_, lp_, os, &sawnan1);
-    sawnan1 = sawnan1 || isnan(max1);
-    if (forcer || (max1 <= growthbound && !sawnan1)) { sigma = lsigma; shift = 1; break; }
+    if (PAIR) {
+      const unsigned pm = 3u << ((threadIdx.x & 31) & ~1);   // this lane pair
+      const bool right = (threadIdx.x & 1) != 0;
+      bool sn = false;
+      const double mx = right ? rrf_sweep(n, P, Q, ps, rsigma, pivmin, wk_, wk_ + (size_t)n * os,
+                                          os, &sn)
+                              : rrf_sweep(n, P, Q, ps, lsigma, pivmin, dp_, lp_, os, &sn);
+      const int src = (threadIdx.x & 31) & ~1;
+      max1 = __shfl_sync(pm, mx, src);
+      sawnan1 = __shfl_sync(pm, (int)sn, src) != 0;
+      max2 = __shfl_sync(pm, mx, src + 1);
+      sawnan2 = __shfl_sync(pm, (int)sn, src + 1) != 0;
+      __syncwarp(pm);   // both sweeps' stores visible to both lanes
+      sawnan1 = sawnan1 || isnan(max1);
+      if (forcer || (max1 <= growthbound && !sawnan1)) { sigma = lsigma; shift = 1; break; }
+      sawnan2 = sawnan2 || isnan(max2);
+      if (forcer || (max2 <= growthbound && !sawnan2)) { sigma = rsigma; shift = 2; break; }
+    } else {
+      max1 = rrf_sweep(n, P, Q, ps, lsigma, pivmin, dp_, lp_, os, &sawnan1);
+      sawnan1 = sawnan1 || isnan(max1);
+      if (forcer || (max1 <= growthbound && !sawnan1)) { sigma = lsigma; shift = 1; break; }
 
-    max2 = rrf_sweep(n, P, Q, ps, rsigma, pivmin, wk_, wk_ + (size_t)n * os, os, &sawnan2);
-    sawnan2 = sawnan2 || isnan(max2);
-    if (forcer || (max2 <= growthbound && !sawnan2)) { sigma = rsigma; shift = 2; break; }
+      max2 = rrf_sweep(n, P, Q, ps, rsigma, pivmin, wk_, wk_ + (size_t)n * os, os, &sawnan2);
+      sawnan2 = sawnan2 || isnan(max2);
+      if (forcer || (max2 <= growthbound && !sawnan2)) { sigma = rsigma; shift = 2; break; }
+    }
 
     if (!(sawnan1 && sawnan2)) {
       if (!sawnan1) {
@@ -2633,8 +2660,11 @@ static __device__ __noinline__ double dv_dlarrf(int n, const double2 *__restrict
     forcer = true;
   }
   if (shift == 2) {
-    for (int i = 0; i < n; i++) dplus(i) = work(i);
-    for (int i = 0; i < n - 1; i++) lplus(i) = work(n + i);
+    // PAIR: the even lane copies DPLUS, the odd one LPLUS
+    if (!PAIR || (threadIdx.x & 1) == 0)
+      for (int i = 0; i < n; i++) dplus(i) = work(i);
+    if (!PAIR || (threadIdx.x & 1) != 0)
+      for (int i = 0; i < n - 1; i++) lplus(i) = work(n + i);
   }
   return sigma;
 #undef dplus

@@ -1576,11 +1576,17 @@ k_cl_ext(int ncl, int L, const ClusterDev *cl, const ProbDev *probs, const Block
 // thread per cluster, after storing the refined extremes and the gap right of
 // the first eigenvalue (computed against its neighbour's value before the
 // second extreme was refined).
+// PAIR (launches with few clusters, where each cluster's sweeps are the
+// cost): two lanes per cluster, the left and right shifts of each try swept
+// at once (dv_dlarrf<true>); the even lane writes the results.
+template <bool PAIR>
 __global__ void LB_RRF
 k_cl_rrf(int ncl, ClusterDev *cl, const ProbDev *probs, const BlockDev *blocks, const double2 *RP,
          const double2 *RQ, const double *arena_prev, double *arena_cur, const double *xw,
          const double *xe, double *Wsh, double *Werr, double *Wgap, unsigned long long *stats) {
-  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int w = PAIR ? gt >> 1 : gt;
+  const bool lead = !PAIR || (gt & 1) == 0;
   unsigned long long work = 0;
   if (w < ncl) {
     const ClusterDev C = cl[w];
@@ -1595,14 +1601,21 @@ k_cl_rrf(int ncl, ClusterDev *cl, const ProbDev *probs, const BlockDev *blocks, 
     double *dplus = grp + 4 * nG + C.g, *lplus = grp + 5 * nG + C.g, *wk = grp + 6 * nG + C.g;
     const double w0 = xw[2 * w], e0 = xe[2 * w], w1 = xw[2 * w + 1], e1 = xe[2 * w + 1];
     const double nw_ = Wsh[cb + 1], ne_ = Werr[cb + 1];
-    Wgap[cb] = fmax(0.0, (nw_ - ne_) - (w0 + e0));
-    Wsh[cb] = w0; Werr[cb] = e0;
-    Wsh[ce] = w1; Werr[ce] = e1;
-    const double tau = dv_dlarrf(nb, Pp, Qp, ps, ce - cb + 1, Wsh + cb, Wgap + cb, Werr + cb,
-                                 C.bl_spdiam, C.lgap, Wgap[ce], p->pivmin, dplus, lplus, wk, C.G);
-    cl[w].tau = tau;
-    cl[w].sigma = C.par_sigma + tau;
-    work = 2ull * nb;
+    if (PAIR) __syncwarp(3u << ((threadIdx.x & 31) & ~1));   // both lanes read nw_, ne_ first
+    if (lead) {
+      Wgap[cb] = fmax(0.0, (nw_ - ne_) - (w0 + e0));
+      Wsh[cb] = w0; Werr[cb] = e0;
+      Wsh[ce] = w1; Werr[ce] = e1;
+    }
+    if (PAIR) __syncwarp(3u << ((threadIdx.x & 31) & ~1));
+    const double tau = dv_dlarrf<PAIR>(nb, Pp, Qp, ps, ce - cb + 1, Wsh + cb, Wgap + cb,
+                                       Werr + cb, C.bl_spdiam, C.lgap, Wgap[ce], p->pivmin, dplus,
+                                       lplus, wk, C.G);
+    if (lead) {
+      cl[w].tau = tau;
+      cl[w].sigma = C.par_sigma + tau;
+      work = 2ull * nb;
+    }
   }
   stat_add(stats, KID_NEWRRR * 4 + 3, work);
 }
@@ -3626,8 +3639,15 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
           LAUNCH(k_cl_ext<true>, (int)((2LL * ncl * Lx + 127) / 128), 128, ncl, Lx, c->cl[cur],
                  c->probs, c->blocks, c->RP, c->RQ, c->arena[nxt], c->Wsh, c->Werr, c->Windex, c->Wt,
                  c->Et, tol, stats);
-        LAUNCH(k_cl_rrf, (ncl + 127) / 128, 128, ncl, c->cl[cur], c->probs, c->blocks, c->RP, c->RQ,
-               c->arena[nxt], c->arena[cur], c->Wt, c->Et, c->Wsh, c->Werr, c->Wgap, stats);
+        // two lanes per cluster when the clusters leave lanes idle
+        if (2LL * ncl <= lanes)
+          LAUNCH(k_cl_rrf<true>, (int)((2LL * ncl + 127) / 128), 128, ncl, c->cl[cur], c->probs,
+                 c->blocks, c->RP, c->RQ, c->arena[nxt], c->arena[cur], c->Wt, c->Et, c->Wsh,
+                 c->Werr, c->Wgap, stats);
+        else
+          LAUNCH(k_cl_rrf<false>, (ncl + 127) / 128, 128, ncl, c->cl[cur], c->probs, c->blocks,
+                 c->RP, c->RQ, c->arena[nxt], c->arena[cur], c->Wt, c->Et, c->Wsh, c->Werr,
+                 c->Wgap, stats);
         CK(cudaMemsetAsync(c->rl_n, 0, sizeof(int), st), "rl_n");
         LAUNCH(k_cl_pack, std::min(ncl, 65535 * 16), 256, ncl, c->cl[cur], c->blocks, c->arena[cur],
                c->Wsh, c->Werr, c->cl_of_slot, c->lvl_of_slot, level, c->rl_n);

@@ -591,6 +591,20 @@ def run_single(M, wl, which: str, hbm_gbs):
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1) * 1e-3)
     sec = times[-1]
+    # one more solve with per-kernel events, streams serialised (for the
+    # detail file: where a single large solve spends its time)
+    Dd.copy_(D0)
+    Ed.copy_(E0)
+    torch.cuda.synchronize()
+    S.profile(2)
+    S.solve(rec, st.cuda_stream)
+    torch.cuda.synchronize()
+    kern, ctr = S.profile_read()
+    S.profile(False)
+    prof = {"kernels_ms": {k: round(v[0], 2) for k, v in
+                           sorted(kern.items(), key=lambda kv: -kv[1][0])},
+            "launches": {k: v[1] for k, v in kern.items()},
+            "work_counters": dict(zip(M.Solver.KERNEL_GROUPS, ctr))}
     from mr3smp_b200.workloads import residual_orth_torch
     ok = rec[0].info == 0 and rec[0].m == m
     res, orth = residual_orth_torch(D, E, W[:m].cpu().numpy(), Z.view(m, n).T)
@@ -602,7 +616,8 @@ def run_single(M, wl, which: str, hbm_gbs):
            "resid": res, "orth": orth, "z_bytes": zb,
            "z_write_gbs": zb / sec * 1e-9,
            "z_write_frac_of_hbm": (zb / sec * 1e-9 / hbm_gbs) if hbm_gbs else None,
-           "api": "mr3_cuda_solve, arrays resident in HBM, CUDA events"}
+           "api": "mr3_cuda_solve, arrays resident in HBM, CUDA events",
+           "_profile": prof}
     S.close()
     del Z, W
     torch.cuda.empty_cache()
@@ -927,6 +942,8 @@ def main():
               "how": "one step after the timed region, every launch bracketed by CUDA events, "
                      "the singleton rounds on the solve's stream (no overlap with the next "
                      "level's cluster kernels)"}
+    if large:   # the large solves' per-kernel profiles go to the file only
+        detail["large_profiles"] = {k: v.pop("_profile", None) for k, v in large.items()}
     detail_path = args.detail_out or os.path.join(tempfile.gettempdir(), "mr3_bench_detail.json")
     with open(detail_path, "w") as f:
         json.dump(detail, f, indent=1)

@@ -65,15 +65,6 @@ static __device__ __forceinline__ int dv_itmax(double a, double b) {
 #define MR3_U 4     // rows per chunk of the software-pipelined sweeps
 #endif
 
-// Prefetch the L1 (L2) line holding *p (PTX prefetch.global.L1 / .L2).  Only
-// issued for addresses inside the arrays being read.
-static __device__ __forceinline__ void pf_l1(const void *p) {
-  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
-}
-static __device__ __forceinline__ void pf_l2(const void *p) {
-  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
-}
-
 // Sturm count of T - x, IJOB=1 rule of dlaebz (SRC/LAPACK/odebz.f:255-270).
 // tp[j] = (d[j], e2[j-1]); tp[0].y unused.  The threads of a warp count the
 // same matrix, so every load is a broadcast that L1 serves; the plain loop
@@ -195,9 +186,7 @@ static __device__ __noinline__ int dv_bisect_tree(int L, int n, const double2 *_
 // groups in the level arenas); the NaN re-run of a 128-row block reads its
 // rows again.  U == 1: the plain row loop, best when a warp's threads all
 // read the same rows (a block's root representation), which L1 serves.
-// PF > 0 (the tree bisection, whose few lanes sweep alone): each chunk also
-// prefetches the rows PF ahead into L2.
-template <int U, int PF = 0>
+template <int U>
 static __device__ __noinline__ int dv_dlaneg(int n, const double2 *__restrict__ P, int ps, double sigma,
                                       int r) {
   static_assert(128 % U == 0, "chunks must not straddle the 128-row blocks");
@@ -272,11 +261,6 @@ static __device__ __noinline__ int dv_dlaneg(int n, const double2 *__restrict__ 
       for (int j0 = bj; j0 <= jend; j0 += U) {
 #pragma unroll
         for (int u = 0; u < U; u++) nx[u] = P[(size_t)(d_imin(j0 + U + u, last) - 1) * ps];
-        if (PF > 0) {
-#pragma unroll
-          for (int u = 0; u < U; u++)
-            if (j0 + u + PF <= last) pf_l2(&P[(size_t)(j0 + u + PF - 1) * ps]);
-        }
 #pragma unroll
         for (int u = 0; u < U; u++) {
           if (j0 + u <= jend) {
@@ -316,11 +300,6 @@ static __device__ __noinline__ int dv_dlaneg(int n, const double2 *__restrict__ 
       for (int j0 = bj; j0 >= jend; j0 -= U) {
 #pragma unroll
         for (int u = 0; u < U; u++) nx[u] = P[(size_t)(d_imax(j0 - U - u, r) - 1) * ps];
-        if (PF > 0) {
-#pragma unroll
-          for (int u = 0; u < U; u++)
-            if (j0 - u - PF >= r) pf_l2(&P[(size_t)(j0 - u - PF - 1) * ps]);
-        }
 #pragma unroll
         for (int u = 0; u < U; u++) {
           if (j0 - u >= jend) {
@@ -352,10 +331,6 @@ static __device__ __noinline__ int dv_dlaneg(int n, const double2 *__restrict__ 
   if (gamma < 0.0) negcnt++;
   return negcnt;
 }
-
-#ifndef MR3_TREE_PF
-#define MR3_TREE_PF 32   // rows the tree bisection's counts prefetch ahead (0: none)
-#endif
 
 // One interval of dlarrb (SRC/LAPACK/odrrb.f:136-293).  Intervals of one
 // dlarrb call never read each other's state: the convergence test reads the
@@ -452,7 +427,7 @@ static __device__ __noinline__ int dv_dlarrb_tree(int L, int n, const double2 *_
       for (int j = 0; j < k; j++) { x = side ? x + back : x - back; back = 2.0 * back; }
       const bool mine = side ? need1 : need0;
       int cnt = 0;
-      if (mine) cnt = dv_dlaneg<MR3_U, MR3_TREE_PF>(n, R, ps, x, r);
+      if (mine) cnt = dv_dlaneg<MR3_U>(n, R, ps, x, r);
       const bool ok = mine && (side ? (cnt >= i) : (cnt <= i - 1));
       const unsigned gb = (__ballot_sync(full, ok) >> g0) & gbits;
       for (int sd = 0; sd < 2; sd++) {
@@ -495,7 +470,7 @@ static __device__ __noinline__ int dv_dlarrb_tree(int L, int n, const double2 *_
       if ((node_t >> b) & 1) l = m; else rr = m;
     }
     int cnt = 0;
-    if (!done) cnt = dv_dlaneg<MR3_U, MR3_TREE_PF>(n, R, ps, 0.5 * (l + rr), r);
+    if (!done) cnt = dv_dlaneg<MR3_U>(n, R, ps, 0.5 * (l + rr), r);
     int node = 1;
     for (int d = 0; d < depth; d++) {
       const int c = __shfl_sync(full, cnt, g0 + node);
@@ -1274,6 +1249,11 @@ static __device__ __forceinline__ double dv_lcg_uniform(uint64_t seed, uint64_t 
   return 2.0 * ((double)s * 3.5527136788005009e-15) - 1.0;   // 2^-48
 }
 
+// Prefetch the L1 line holding *p (PTX prefetch.global.L1).  Only issued for
+// addresses inside the arrays being read.
+static __device__ __forceinline__ void pf_l1(const void *p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
 
 #ifndef MR3_PF
 #define MR3_PF 16   // L1 prefetch distance in rows (0: none)
@@ -2331,7 +2311,9 @@ struct r1s_buf {
 #ifndef MR3_R1S_PF
 #define MR3_R1S_PF 32
 #endif
-
+static __device__ __forceinline__ void pf_l2(const void *p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
 
 static __device__ __noinline__ void dv_r1s_call(int n, double lambda, const double2 *__restrict__ P,
                                          const double2 *__restrict__ Q, int ps, double pivmin,
@@ -2502,9 +2484,6 @@ static __device__ __noinline__ void dv_r1s_call(int n, double lambda, const doub
 // -pivmin.  The running pivot stays in a register (it is written out, never
 // read back) and the rows are read in chunks of MR3_U issued one chunk
 // ahead of the arithmetic.
-#ifndef MR3_RRF_PF
-#define MR3_RRF_PF 32
-#endif
 static __device__ __forceinline__ double rrf_sweep(int n, const double2 *__restrict__ P,
                                                    const double2 *__restrict__ Q, int ps,
                                                    double sig, double pivmin, double *dp,
@@ -2531,12 +2510,6 @@ static __device__ __forceinline__ double rrf_sweep(int n, const double2 *__restr
         const int i = d_imin(i0 + U + u, last);
         nq[u] = Q[(size_t)i * ps];
         np_[u] = P[(size_t)(i + 1) * ps].x;
-        // rows MR3_RRF_PF ahead into L2: a cluster's sweep is a lone
-        // thread's dependent chain when clusters are few
-        if (MR3_RRF_PF && i0 + u + MR3_RRF_PF <= last) {
-          pf_l2(&Q[(size_t)(i0 + u + MR3_RRF_PF) * ps]);
-          pf_l2(&P[(size_t)(i0 + u + MR3_RRF_PF + 1) * ps]);
-        }
       }
 #pragma unroll
       for (int u = 0; u < U; u++) {

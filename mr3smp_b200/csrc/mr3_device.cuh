@@ -114,6 +114,63 @@ static __device__ __noinline__ void dv_ijob3(int n, const double2 *__restrict__ 
   }
 }
 
+// dv_ijob3 by a group of L lanes (L = 2..32, a power of two; every lane of
+// the group passes the same arguments and gets the same results).  The
+// first count is at the given point c, as in the loop; after it the points
+// are midpoints, and the midpoints of the next log2(L) steps form a binary
+// tree that follows from the current interval: lane t of the group counts
+// at node max(t,1) (heap numbering; its interval computed along the node's
+// path with the loop's operations), then the group walks the tree applying
+// the loop's updates and tests after each step.  A count equal to nval
+// closes the interval (a = b = c), which the width test then stops.  The
+// same points, counts and results as dv_ijob3; log2(L) steps per count.
+static __device__ __noinline__ void dv_ijob3_tree(int L, int n, const double2 *__restrict__ tp,
+                                           double pivmin, double abstol, double reltol,
+                                           int nitmax, int nval, double c, double *a_,
+                                           double *b_, int *na_, int *nb_) {
+  const int lane = threadIdx.x & 31;
+  const int t = lane & (L - 1), g0 = lane - t, depth = 31 - __clz(L);
+  const unsigned gm = ((L == 32) ? 0xffffffffu : ((1u << L) - 1u)) << g0;
+  const int node_t = t == 0 ? 1 : t;
+  const double tol0 = fmax(abstol, pivmin);
+  double a = *a_, b = *b_;
+  int na = *na_, nb = *nb_, it = 0;
+  bool done = nitmax < 1;
+  if (!done) {   // the first step, at the given point
+    const int cnt = dv_count_bisect(n, tp, pivmin, c);
+    if (cnt <= nval) { a = c; na = cnt; }
+    if (cnt >= nval) { b = c; nb = cnt; }
+    it = 1;
+    const double w = fabs(b - a), tt = fmax(fabs(b), fabs(a));
+    if (w < fmax(tol0, reltol * tt) || na >= nb || it >= nitmax) done = true;
+  }
+  while (!done) {
+    double l = a, r = b;
+    for (int k = 30 - __clz(node_t); k >= 0; k--) {
+      const double m = 0.5 * (l + r);
+      if ((node_t >> k) & 1) l = m; else r = m;
+    }
+    const int raw = dv_count_bisect(n, tp, pivmin, 0.5 * (l + r));
+    int node = 1;
+    for (int d = 0; d < depth; d++) {
+      const int cv = __shfl_sync(gm, raw, g0 + node);
+      if (!done) {
+        const double cm = 0.5 * (a + b);
+        if (cv <= nval) { a = cm; na = cv; }
+        if (cv >= nval) { b = cm; nb = cv; }
+        node = (cv < nval) ? 2 * node + 1 : 2 * node;
+        it++;
+        const double w = fabs(b - a), tt = fmax(fabs(b), fabs(a));
+        if (w < fmax(tol0, reltol * tt) || na >= nb || it >= nitmax) done = true;
+      }
+    }
+  }
+  *a_ = a;
+  *b_ = b;
+  *na_ = na;
+  *nb_ = nb;
+}
+
 // The interval of eigenvalue j under dlaebz IJOB=2 started from [a,b] with
 // counts (na,nb): midpoint bisection of that one interval (odebz.f 90-120).
 // it0 > 0 continues a bisection whose first it0 steps ended in [a,b].

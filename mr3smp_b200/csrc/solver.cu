@@ -441,18 +441,21 @@ k_prologue(ProbDev *probs, BlockDev *blocks, int *blk_of_row, double *D, double 
     if (irange == MR3_RANGE_A) { p->wl = p->gl; p->wu = p->gu; p->vl_out = p->gl; p->vu_out = p->gu; }
   }
   if (p->jobz == MR3_JOB_C) return;
-  // ---- range I: the interval holding eigenvalues il..iu (SRC/mrrr_val.c:295-319)
-  if (irange == MR3_RANGE_I && (tid == 0 || tid == 32)) {
+  // ---- range I: the interval holding eigenvalues il..iu (SRC/mrrr_val.c:295-319),
+  // the two searches by warps 0 and 1, each with the tree form
+  if (irange == MR3_RANGE_I && tid < 64) {
     int itmax = (int)((dv_log(p->tnorm + pivmin) - dv_log(pivmin)) / dv_log(2.0) + 2);
     double atoli = 2 * (2 * MR3_SAFMIN + 2 * pivmin);
     double a = p->gl, bq = p->gu;
     int na = -1, nb = n + 1;
-    if (tid == 0) {
-      dv_ijob3(n, TP + off, pivmin, atoli, tol.rqtol, itmax, p->il - 1, p->gl, &a, &bq, &na, &nb);
-      p->wl = a; p->wlu = bq; p->nwl = na; p->vl_out = a;
+    if (tid < 32) {
+      dv_ijob3_tree(32, n, TP + off, pivmin, atoli, tol.rqtol, itmax, p->il - 1, p->gl, &a, &bq,
+                    &na, &nb);
+      if (tid == 0) { p->wl = a; p->wlu = bq; p->nwl = na; p->vl_out = a; }
     } else {
-      dv_ijob3(n, TP + off, pivmin, atoli, tol.rqtol, itmax, p->iu, p->gu, &a, &bq, &na, &nb);
-      p->wul = a; p->wu = bq; p->nwu = nb; p->vu_out = bq;
+      dv_ijob3_tree(32, n, TP + off, pivmin, atoli, tol.rqtol, itmax, p->iu, p->gu, &a, &bq, &na,
+                    &nb);
+      if (tid == 32) { p->wul = a; p->wu = bq; p->nwu = nb; p->vu_out = bq; }
     }
   }
 }
@@ -524,14 +527,16 @@ k_blocks(ProbDev *probs, BlockDev *blocks, const double *D, double *E, const dou
       int itmax = dv_itmax(tnb + pivmin, pivmin);
       double a = gl2, bq = gu2;
       int na = -1, nb = nbl + 1;
-      if (lane == 0) {
-        dv_ijob3(nbl, TP + ibgn, pivmin, atoli, tol.bsrtol, itmax, ilow - 1, gl2, &a, &bq, &na, &nb);
-      } else if (lane == 1) {
-        dv_ijob3(nbl, TP + ibgn, pivmin, atoli, tol.bsrtol, itmax, iupp, gu2, &a, &bq, &na, &nb);
-      }
+      // the two searches by half-warps, each with the tree form
+      if (lane < 16)
+        dv_ijob3_tree(16, nbl, TP + ibgn, pivmin, atoli, tol.bsrtol, itmax, ilow - 1, gl2, &a, &bq,
+                      &na, &nb);
+      else
+        dv_ijob3_tree(16, nbl, TP + ibgn, pivmin, atoli, tol.bsrtol, itmax, iupp, gu2, &a, &bq,
+                      &na, &nb);
       double a0 = __shfl_sync(0xffffffffu, a, 0), b0 = __shfl_sync(0xffffffffu, bq, 0);
-      double a1 = __shfl_sync(0xffffffffu, a, 1), b1 = __shfl_sync(0xffffffffu, bq, 1);
-      int nwl = __shfl_sync(0xffffffffu, na, 0), nwu = __shfl_sync(0xffffffffu, nb, 1);
+      double a1 = __shfl_sync(0xffffffffu, a, 16), b1 = __shfl_sync(0xffffffffu, bq, 16);
+      int nwl = __shfl_sync(0xffffffffu, na, 0), nwu = __shfl_sync(0xffffffffu, nb, 16);
       wlb = a0; wlub = b0; wulb = a1; wub = b1;
       if (nwl < 0 || nwl >= nbl || nwu < 1 || nwu > nbl) bad = 1;
     }

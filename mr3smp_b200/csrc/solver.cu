@@ -1698,23 +1698,15 @@ __device__ __forceinline__ unsigned long long refine_cl_body(
   return (unsigned long long)nc * (unsigned long long)B.nbl;
 }
 
-// Lanes per interval for a launch of `items` independent bisection
-// intervals, with `lanes` the threads the kernel keeps resident on the GPU:
-// a thread each (one step per count), or groups of L = 4..32 lanes running
-// the tree bisection (the same intervals, log2 L steps per count).  Items x
-// L threads take ceil(items L / lanes) waves, so the choice maximises the
-// steps per count over the waves (ties: fewer lanes).
+// Lanes per interval for a launch of `items` independent dlarrb intervals:
+// a thread each when they fill the GPU, else groups of 4..32 lanes running
+// the tree bisection (the same intervals, fewer sequential sweeps).
 __host__ __device__ __forceinline__ int tree_lanes(long long items, long long lanes,
                                                    int maxL = 32) {
-  if (items <= 0 || lanes <= 0) return 1;
-  int best = 1;
-  double score = 1.0 / (double)((items + lanes - 1) / lanes);
-  const int top = maxL > 32 ? 32 : maxL;
-  for (int L = 4, lg = 2; L <= top; L <<= 1, lg++) {
-    const double sc = (double)lg / (double)((items * L + lanes - 1) / lanes);
-    if (sc > score) { score = sc; best = L; }
-  }
-  return best;
+  if (maxL < 4) return 1;
+  int L = maxL > 32 ? 32 : maxL;
+  while (L > 4 && items * L > lanes) L >>= 1;
+  return items * L > lanes ? 1 : L;
 }
 
 template <bool TREE>
@@ -2855,10 +2847,6 @@ __global__ void k_perm_zsupp2(int N, const ProbDev *probs, const int *prob_of_sl
 struct mr3_cuda_ctx {
   int device = 0, nsm = 148;
   int sng_ctas_per_sm = 2;                  // resident k_sng_round CTAs per SM
-  // threads the tree-bisection kernels keep resident (occupancy at 128
-  // threads per block), and the resident k_sng_bisect blocks
-  long long res_bis = 0, res_ref = 0, res_ext = 0, res_rcl = 0, res_rrf = 0;
-  int sbis_ctas = 0;
   cudaStream_t own = nullptr;
   cudaStream_t aux = nullptr;               // copies that overlap the solves
   cudaStream_t rnd = nullptr;               // a level's singleton rounds
@@ -3115,18 +3103,6 @@ extern "C" int mr3_cuda_ctx_create_prio(int device, int high, mr3_cuda_ctx **out
                                                     SNG_TILE_BYTES) == cudaSuccess &&
       nb > 0)
     c->sng_ctas_per_sm = nb;
-  auto resident = [&](const void *k, int threads) -> long long {
-    int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, threads, 0) != cudaSuccess || b < 1)
-      b = 1;
-    return (long long)c->nsm * b * threads;
-  };
-  c->res_bis = resident((const void *)k_bisect<true>, 128);
-  c->res_ref = resident((const void *)k_refine_root<true>, 128);
-  c->res_ext = resident((const void *)k_cl_ext<true>, 128);
-  c->res_rcl = resident((const void *)k_refine_cl<true>, 128);
-  c->res_rrf = resident((const void *)k_cl_rrf<true>, 128);
-  c->sbis_ctas = (int)(resident((const void *)k_sng_bisect, 256) / 256);
   c->h_const[0] = 1.0;
   c->h_iconst[0] = 1;
   c->h_iconst[1] = 1;
@@ -3573,7 +3549,7 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
   LAUNCH(k_blocks, L, MR3_THREADS, c->probs, c->blocks, c->D, c->E, c->gers, c->TP, tol);
   unsigned long long *stats = c->prof ? c->stats : nullptr;
   {
-    const int Lb = tree_lanes(NN, c->res_bis, tree_max);
+    const int Lb = tree_lanes(NN, (long long)c->nsm * 2048, tree_max);
     if (Lb == 1) {
       // shared intervals breadth-first, then a thread per eigenvalue
       CK(cudaMemsetAsync(c->bis_st, 0xff, N * sizeof(BisState), st), "bis st");
@@ -3607,7 +3583,7 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
   LAUNCH(k_root, L, MR3_THREADS, c->probs, c->blocks, c->D, c->E, c->TP, c->Dt, c->Lt, c->W,
          c->Werr, c->Wgap, c->RP, c->RQ);
   {
-    const int Lr = tree_lanes(NN, c->res_ref, tree_max);
+    const int Lr = tree_lanes(NN, (long long)c->nsm * 2048, tree_max);
     if (Lr == 1)
       LAUNCH(k_refine_root<false>, gN128, 128, NN, 1, c->probs, c->blocks, c->iblk, c->RP, c->W,
              c->Werr, c->Wgap, tol, stats);
@@ -3652,13 +3628,14 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
     const int DEPTH_CAP = 512;
     ClsScratch xs;
     xs.ns = c->cls_ns; xs.soff = c->cls_soff; xs.cbase = c->cls_cbase; xs.abase = c->cls_abase;
+    const long long lanes = (long long)c->nsm * 2048;   // lanes a launch can keep busy
     bool rounds_pending = false;
     for (int level = 0; ncl > 0; level++) {
       if (level >= DEPTH_CAP) { snprintf(c->err, sizeof(c->err), "representation tree too deep"); return MR3_EMISC; }
       const int cur = level & 1, nxt = cur ^ 1;
       const int gW = (ncl * 32 + MR3_THREADS - 1) / MR3_THREADS;
       if (level > 0) {
-        const int Lx = tree_lanes(2LL * ncl, c->res_ext, tree_max);
+        const int Lx = tree_lanes(2LL * ncl, lanes, tree_max);
         if (Lx == 1)
           LAUNCH(k_cl_ext<false>, (int)((2LL * ncl + 127) / 128), 128, ncl, 1, c->cl[cur], c->probs,
                  c->blocks, c->RP, c->RQ, c->arena[nxt], c->Wsh, c->Werr, c->Windex, c->Wt, c->Et,
@@ -3667,8 +3644,8 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
           LAUNCH(k_cl_ext<true>, (int)((2LL * ncl * Lx + 127) / 128), 128, ncl, Lx, c->cl[cur],
                  c->probs, c->blocks, c->RP, c->RQ, c->arena[nxt], c->Wsh, c->Werr, c->Windex, c->Wt,
                  c->Et, tol, stats);
-        // two lanes per cluster when that still fits one wave of the kernel
-        if (2LL * ncl <= c->res_rrf)
+        // two lanes per cluster when the clusters leave lanes idle
+        if (2LL * ncl <= lanes)
           LAUNCH(k_cl_rrf<true>, (int)((2LL * ncl + 127) / 128), 128, ncl, c->cl[cur], c->probs,
                  c->blocks, c->RP, c->RQ, c->arena[nxt], c->arena[cur], c->Wt, c->Et, c->Wsh,
                  c->Werr, c->Wgap, stats);
@@ -3689,10 +3666,10 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
         // length returns at once (the length is known on the device only)
         LAUNCH(k_refine_cl<false>, gN128, 128, c->rl, c->rl_n, c->cl[cur], c->probs, c->blocks,
                c->arena[cur], c->Wsh, c->Werr, c->Wgap, c->Windex, c->cl_of_slot, c->lvl_of_slot,
-               level, tol, c->res_rcl, tree_max, stats);
-        LAUNCH(k_refine_cl<true>, (int)(c->res_rcl / 128), 128, c->rl, c->rl_n, c->cl[cur],
-               c->probs, c->blocks, c->arena[cur], c->Wsh, c->Werr, c->Wgap, c->Windex,
-               c->cl_of_slot, c->lvl_of_slot, level, tol, c->res_rcl, tree_max, stats);
+               level, tol, lanes, tree_max, stats);
+        LAUNCH(k_refine_cl<true>, (int)(lanes / 128), 128, c->rl, c->rl_n, c->cl[cur], c->probs,
+               c->blocks, c->arena[cur], c->Wsh, c->Werr, c->Wgap, c->Windex, c->cl_of_slot,
+               c->lvl_of_slot, level, tol, lanes, tree_max, stats);
         LAUNCH(k_gaps_cl, gN, 256, NN, c->cl[cur], c->Wsh, c->Werr, c->Wgap, c->W, c->cl_of_slot,
                c->lvl_of_slot, level);
       }
@@ -3732,7 +3709,7 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
         const int ctas_all = (int)(nwarps / SNG_WARPS);
         const int ctas_first = std::min(ctas_all, (nsng + 32 * SNG_WARPS - 1) / (32 * SNG_WARPS));
         const size_t smem = SNG_TILE_BYTES;
-        const int bis_ctas = c->sbis_ctas;
+        const int bis_ctas = c->nsm * 4;
         const int nblk = (nsng + LIST_T - 1) / LIST_T;
         // a list of at most this many singletons (four per persistent warp)
         // is finished in one launch (k_sng_finish), a warp each in turn;

@@ -1698,6 +1698,13 @@ __device__ __forceinline__ unsigned long long refine_cl_body(
   return (unsigned long long)nc * (unsigned long long)B.nbl;
 }
 
+// Threads per SM that the tree forms may fill (a launch of few intervals
+// gets as many lanes per interval as fit; more than the resident threads
+// run in waves, which the tree's steps per count outweigh)
+#ifndef MR3_TREE_BUDGET
+#define MR3_TREE_BUDGET 2048
+#endif
+
 // Lanes per interval for a launch of `items` independent dlarrb intervals:
 // a thread each when they fill the GPU, else groups of 4..32 lanes running
 // the tree bisection (the same intervals, fewer sequential sweeps).
@@ -3549,7 +3556,7 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
   LAUNCH(k_blocks, L, MR3_THREADS, c->probs, c->blocks, c->D, c->E, c->gers, c->TP, tol);
   unsigned long long *stats = c->prof ? c->stats : nullptr;
   {
-    const int Lb = tree_lanes(NN, (long long)c->nsm * 2048, tree_max);
+    const int Lb = tree_lanes(NN, (long long)c->nsm * MR3_TREE_BUDGET, tree_max);
     if (Lb == 1) {
       // shared intervals breadth-first, then a thread per eigenvalue
       CK(cudaMemsetAsync(c->bis_st, 0xff, N * sizeof(BisState), st), "bis st");
@@ -3583,7 +3590,7 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
   LAUNCH(k_root, L, MR3_THREADS, c->probs, c->blocks, c->D, c->E, c->TP, c->Dt, c->Lt, c->W,
          c->Werr, c->Wgap, c->RP, c->RQ);
   {
-    const int Lr = tree_lanes(NN, (long long)c->nsm * 2048, tree_max);
+    const int Lr = tree_lanes(NN, (long long)c->nsm * MR3_TREE_BUDGET, tree_max);
     if (Lr == 1)
       LAUNCH(k_refine_root<false>, gN128, 128, NN, 1, c->probs, c->blocks, c->iblk, c->RP, c->W,
              c->Werr, c->Wgap, tol, stats);
@@ -3628,7 +3635,7 @@ extern "C" int mr3_cuda_solve_cb(mr3_cuda_ctx *c, int P, mr3_cuda_prob *pr, void
     const int DEPTH_CAP = 512;
     ClsScratch xs;
     xs.ns = c->cls_ns; xs.soff = c->cls_soff; xs.cbase = c->cls_cbase; xs.abase = c->cls_abase;
-    const long long lanes = (long long)c->nsm * 2048;   // lanes a launch can keep busy
+    const long long lanes = (long long)c->nsm * MR3_TREE_BUDGET;   // lanes a launch can keep busy
     bool rounds_pending = false;
     for (int level = 0; ncl > 0; level++) {
       if (level >= DEPTH_CAP) { snprintf(c->err, sizeof(c->err), "representation tree too deep"); return MR3_EMISC; }

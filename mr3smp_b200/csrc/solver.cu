@@ -2064,9 +2064,11 @@ __global__ void k_bucket_scan(int *bk) {
 // lanes sweep the blocks by absolute index, so a checkpoint access is one
 // coalesced 256-byte row.  Consecutive records of a list mostly share a
 // block; a warp whose lanes hold blocks of different sizes sweeps the
-// largest.  An accepted eigenvector is recomputed once more and written by
-// its lane straight to its column of Z; the warp zeroes the rows outside the
-// support in coalesced rows.
+// largest.  A call after a singleton's first writes z of its support to the
+// lane's column of Z as it goes; when the vector is accepted the warp scales
+// the support and zeroes the rows outside it in coalesced rows.  (A first
+// call, practically never accepted, writes nothing; if it is accepted the
+// next round repeats it and writes.)
 // ------------------------------------------------------------------------
 #define SNG_WARPS 8
 #ifndef SNG_MINB
@@ -2569,10 +2571,11 @@ k_sng_bisect(int out, const SngDev *sng, const ClusterDev *cl, const ProbDev *pr
 }
 
 // The rest of a level's singletons when few are left (SngCounters.mode 1):
-// one warp per singleton runs its remaining Rayleigh-quotient loop
-// (SRC/process_singleton.c:159-292) to the end in one launch -- dlar1v on
-// lane 0 (the warp's lane-0 checkpoints), a bisection by all 32 lanes with
-// the tree bisection -- instead of one call per round with a launch
+// a warp per singleton (the warps take them in turn) runs its remaining
+// Rayleigh-quotient loop (SRC/process_singleton.c:159-292) to the end in one
+// launch -- each dlar1v on lanes 0 and 1 (SPLIT, the default) or on lane 0
+// with its checkpoints, a bisection by all 32 lanes with the tree
+// bisection -- instead of one call per round with a launch
 // sequence (round, compaction, bisection, sort) between calls.  Every call
 // and every state update is the one the rounds make, so the results are the
 // same bits.  The last block to finish empties the list (mode 2).
